@@ -1,0 +1,94 @@
+"""Orthonormal bases for the DLR substeps (oracle).
+
+The reference takes left singular vectors from ``svd!(K)`` (LAPACK gesdd) and
+Householder Q factors from ``numpy.linalg.qr`` (``SolverCSD.jl:149-153``). Every
+downstream use is covariant under a change of orthonormal basis of the same
+column space, so only the SPAN of these factors is observable -- except where
+the input is (numerically) rank deficient, where LAPACK completes the basis
+with directions fixed by rounding noise. This module offers:
+
+* ``mode="lapack"``: the reference's calls verbatim;
+* ``mode="det"``: a deterministic, rank-revealing rule that the CUDA path
+  implements too. The numerical range of A is the span of the left singular
+  vectors with sigma_j > tol * ||A||_2; missing directions are completed by
+  canonical vectors e_c taken in increasing c, each accepted when its residual
+  after two Gram-Schmidt passes against the basis so far exceeds 1/2.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RANK_TOL = 1e-13
+
+
+def svd_full(A: np.ndarray):
+    """Julia ``svd!(A)`` -> (U, S, V), thin, V not transposed."""
+    U, s, Vt = np.linalg.svd(A, full_matrices=False)
+    return U, s, Vt.T
+
+
+def _complete(B: np.ndarray, need: int, n: int, order=None) -> np.ndarray:
+    cols = []
+    order = np.arange(n) if order is None else order
+    it = 0
+    while len(cols) < need:
+        if it >= len(order):
+            raise RuntimeError("basis completion ran out of canonical vectors")
+        c = order[it]
+        Bc = np.column_stack([B] + cols) if (B.shape[1] + len(cols)) else np.zeros((n, 0))
+        v = np.zeros(n)
+        v[c] = 1.0
+        for _ in range(2):
+            if Bc.shape[1]:
+                v = v - Bc @ (Bc.T @ v)
+        nv = np.linalg.norm(v)
+        if nv > 0.5:
+            cols.append(v / nv)
+        it += 1
+    return np.column_stack(cols) if cols else np.zeros((n, 0))
+
+
+def _range_basis(A: np.ndarray, scale: float, tol: float) -> np.ndarray:
+    if A.shape[1] == 0:
+        return np.zeros((A.shape[0], 0))
+    U, s, _ = np.linalg.svd(A, full_matrices=False)
+    rho = int(np.sum(s > tol * scale)) if scale > 0 else 0
+    return U[:, :rho]
+
+
+def orth(A: np.ndarray, mode: str = "lapack", tol: float | None = None, order=None) -> np.ndarray:
+    """Orthonormal n x k basis with the span of ``svd!(A).U``."""
+    if mode == "lapack":
+        U, _, _ = np.linalg.svd(A, full_matrices=False)
+        return U
+    tol = RANK_TOL if tol is None else tol
+    n, k = A.shape
+    scale = np.linalg.norm(A, 2) if A.size else 0.0
+    B = _range_basis(A, scale, tol)
+    if B.shape[1] < k:
+        B = np.column_stack([B, _complete(B, k - B.shape[1], n, order)])
+    return B
+
+
+def orth_augment(X: np.ndarray, K: np.ndarray, mode: str = "lapack", tol: float | None = None, order=None) -> np.ndarray:
+    """Q of ``py"qr"([X K])`` (``SolverCSD.jl:149-153``), n x (rX + rK).
+
+    Columns ``[:rX]`` span span(X) (completed if X is rank deficient), columns
+    ``[rX:]`` span span([X K]) minus span(X) (completed likewise).
+    """
+    if mode == "lapack":
+        Q, _ = np.linalg.qr(np.column_stack([X, K]))
+        return Q
+    tol = RANK_TOL if tol is None else tol
+    n = X.shape[0]
+    scale = np.linalg.norm(np.column_stack([X, K]), 2)
+    Q1 = _range_basis(X, scale, tol)
+    if Q1.shape[1] < X.shape[1]:
+        Q1 = np.column_stack([Q1, _complete(Q1, X.shape[1] - Q1.shape[1], n, order)])
+    Kp = K - Q1 @ (Q1.T @ K)
+    Kp = Kp - Q1 @ (Q1.T @ Kp)
+    Q2 = _range_basis(Kp, scale, tol)
+    base = np.column_stack([Q1, Q2])
+    if Q2.shape[1] < K.shape[1]:
+        base = np.column_stack([base, _complete(base, K.shape[1] - Q2.shape[1], n, order)])
+    return base

@@ -1,0 +1,309 @@
+"""``SolverCSD`` and the DLR energy loops (oracle restatement, FP64).
+
+Follows ``code/SolverCSD.jl``: constructor ``:63-146``, ``PsiBeam`` ``:240-276``,
+``solveFluxUpwind!`` ``:388-463``, fixed-rank ``SolveFirstCollisionSourceDLR``
+``:891-1120``, ``SolveFirstCollisionSourceDLRParallel`` ``:1726-2008``,
+``SolveFirstCollisionSourceDLRBUGRejection`` ``:2011-2374`` and ``truncate!``
+``:3369-3399``. Julia's in-place mutations (``X[bnd,:] .= 0``, ``S .= ...``) are
+kept as numpy in-place writes so that aliasing behaves the same.
+
+Index conventions: cell (i, j) (1-based in the reference) has row
+``(i-1)*ny + j``; here 0-based ``i*ny + j``. psi is stored as an (nx, ny, q)
+array; ``Mat2Vec(psi)`` is ``psi.reshape(nx*ny, q)``.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import linalg as la
+from . import pn as pnmod
+from . import quadrature as qd
+from .csd import CSD
+from .stencils import Stencils
+
+
+class SolverCSD:
+    """``mutable struct SolverCSD`` + constructor (``SolverCSD.jl:20-146``) at T = Float64."""
+
+    def __init__(self, settings, basis_mode: str = "lapack"):
+        s = settings
+        self.settings = s
+        self.basis_mode = basis_mode
+        self.x = s.x
+        self.y = s.y
+        self.gamma = np.array([2.0 / (2 * n + 1) for n in range(s.nPN + 1)])
+        self.csd = CSD(s)
+        Ax, _, Az = pnmod.setup_system_matrices(s.nPN)
+        self.Ax_dense, self.Az_dense = Ax, Az
+        Axs, _, Azs = pnmod.setup_system_matrices_sparse(s.nPN)
+        self.Ax, self.Az = Axs.tocsr(), Azs.tocsr()
+        self.AbsAx = pnmod.roe_abs(Ax).tocsr()
+        self.AbsAz = pnmod.roe_abs(Az).tocsr()
+        self.N = pnmod.n_moments(s.nPN)
+        self.density = s.density.astype(np.float64)
+        nx, ny = s.NCellsX, s.NCellsY
+        self.densityVec = self.density.reshape(nx * ny)
+        self.dose = np.zeros(nx * ny)
+        # boundary cells, SolverCSD.jl:108-131 (0-based rows, order kept)
+        bidx = []
+        for i in range(nx):
+            bidx.append(i * ny + 0)
+            bidx.append(i * ny + ny - 1)
+        for j in range(ny):
+            bidx.append(0 * ny + j)
+            bidx.append((nx - 1) * ny + j)
+        self.boundaryIdx = np.array(bidx, dtype=np.int64)
+        q = s.nPN + 1
+        self.Q_points, self.Q_weights = qd.standard_points(q)
+        self.O, self.M = qd.compute_trafo_matrices(q, s.nPN)
+        self.stencil = Stencils(s)
+        # Benchmark problems peak-normalise the angular Gaussian over the
+        # quadrature (no ordinate sits exactly on the beam direction).
+        self.psi_scale = s.psi_scale
+        if s.beam_peak_normalized:
+            pts = self.Q_points
+            ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - pts[:, 0]) ** 2) * np.exp(-s.sigmaO3Inv * (s.Omega3 - pts[:, 2]) ** 2)
+            self.psi_scale = s.psi_scale / ang.max()
+        # Completion candidates for rank-deficient bases (see oracle.linalg):
+        # boundary cells by ascending boundary-source amplitude, and odd (k < 0)
+        # moments before even ones.
+        bc_amp = np.exp(-s.sigmaXInv * (s.xMid[self.boundaryIdx // ny] - s.x0) ** 2) * \
+            np.exp(-s.sigmaYInv * (s.yMid[self.boundaryIdx % ny] - s.y0) ** 2)
+        cells, first = np.unique(self.boundaryIdx, return_index=True)
+        amp = bc_amp[first]
+        self.x_completion = cells[np.lexsort((cells, amp))]
+        ks = np.array([k for l in range(s.nPN + 1) for k in range(-l, l + 1)])
+        self.w_completion = np.concatenate([np.nonzero(ks < 0)[0], np.nonzero(ks >= 0)[0]])
+        self.qReduced = None
+        self.MReduced = None
+        self.OReduced = None
+        self.idxBeam = None
+
+    # -- boundary source --------------------------------------------------
+    def psi_beam(self, Omega, E, x, y, n):
+        """``PsiBeam(obj, Omega, E, x, y, n)`` generic branch (``SolverCSD.jl:275``).
+
+        ``n`` is the reference's 1-based energy index into ``csd.S``. Vectorised
+        over ``Omega`` rows and ``x``/``y`` arrays by broadcasting.
+        """
+        s = self.settings
+        E0 = s.eMax
+        Om = np.atleast_2d(Omega)
+        ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - Om[:, 0]) ** 2) * np.exp(-s.sigmaO3Inv * (s.Omega3 - Om[:, 2]) ** 2)
+        return (self.psi_scale * ang * math.exp(-s.sigmaEInv * (E0 - E) ** 2)
+                * np.exp(-s.sigmaXInv * (x - s.x0) ** 2) * np.exp(-s.sigmaYInv * (y - s.y0) ** 2)
+                * self.csd.S[n - 1] * s.densityMin)
+
+    def setup_directions(self):
+        """Direction reduction and psi initial condition (``SolverCSD.jl:910-925``)."""
+        s = self.settings
+        pts = self.Q_points
+        psiBeam = np.array([self.psi_beam(pts[k], s.eMax, s.x0, s.y0, 1)[0] for k in range(pts.shape[0])])
+        idx = np.nonzero(psiBeam > 1e-17 * psiBeam.max())[0]
+        self.idxBeam = idx
+        self.qReduced = pts[idx, :]
+        self.MReduced = self.M[:, idx]
+        self.OReduced = self.O[idx, :]
+        # SetupIC -> IC(...) is zero for the beam problems (settings.jl:341-347)
+        return np.zeros((s.NCellsX, s.NCellsY, idx.size))
+
+    def apply_bc(self, psi, E, n):
+        """Boundary inflow on the 4 boundary rows/cols for all ordinates (``:977-988``)."""
+        s = self.settings
+        xm, ym = s.xMid, s.yMid
+        Om = self.qReduced
+        # psi[j,1,k], psi[j,end,k] over j = 1..nx, then psi[1,j,k], psi[end,j,k] over j = 1..ny
+        psi[:, 0, :] = self.psi_beam(Om, E, xm[:, None], ym[0], n)
+        psi[:, -1, :] = self.psi_beam(Om, E, xm[:, None], ym[-1], n)
+        psi[0, :, :] = self.psi_beam(Om, E, xm[0], ym[:, None], n)
+        psi[-1, :, :] = self.psi_beam(Om, E, xm[-1], ym[:, None], n)
+
+    def flux_upwind(self, phi):
+        """``solveFluxUpwind!`` (``SolverCSD.jl:388-463``), interior cells only.
+
+        Returns flux with zeros on boundary cells (the reference's ``flux`` buffer
+        is allocated zero and only interior entries are ever written).
+        """
+        s = self.settings
+        flux = np.zeros_like(phi)
+        ox = self.qReduced[:, 0]
+        oz = self.qReduced[:, 2]
+        c = phi[1:-1, 1:-1, :]
+        xm = phi[:-2, 1:-1, :]
+        xp = phi[2:, 1:-1, :]
+        ym = phi[1:-1, :-2, :]
+        yp = phi[1:-1, 2:, :]
+        ew = np.where(ox >= 0.0, c - xm, xp - c)
+        ns = np.where(oz >= 0.0, c - ym, yp - c)
+        flux[1:-1, 1:-1, :] = (ox / s.dx) * ew + (oz / s.dy) * ns
+        return flux
+
+    def sweep(self, psi, dE, sigma0):
+        """Uncollided update ``:1000-1005`` incl. the boundary-slab quirk.
+
+        ``psi[boundaryIdx]`` linear-indexes the column-major (nx, ny, q) array, so
+        only q-slab 1 is restored, at (a, b) = ((L-1) % nx, (L-1) // nx).
+        """
+        s = self.settings
+        nx = s.NCellsX
+        flux = self.flux_upwind(psi / self.density[:, :, None])
+        L0 = self.boundaryIdx
+        a, b = L0 % nx, L0 // nx
+        psiBC = psi[a, b, 0].copy()
+        psi[...] = (psi - dE * flux) / (1 + dE * sigma0)
+        psi[a, b, 0] = psiBC
+
+    def dvec(self, sigma):
+        s = self.settings
+        Dv = np.zeros(self.N)
+        for l in range(s.nPN + 1):
+            for k in range(-l, l + 1):
+                Dv[pnmod.global_index(l, k)] = sigma[l]
+        return Dv
+
+    def dose_half(self, X, S, W, psi, dE, Sn):
+        """``dose += 0.5 dE (X S W[1,:] + uOUnc) S[n] ./ rho`` (``:990-997``)."""
+        nx, ny = self.settings.NCellsX, self.settings.NCellsY
+        uOUnc = psi.reshape(nx * ny, -1) @ self.MReduced[0, :]
+        self.dose += 0.5 * dE * (X @ (S @ W[0, :]) + uOUnc) * Sn / self.densityVec
+
+    # Grams used by the streaming substeps
+    def _w_grams(self, Wa, Wb):
+        return (Wa.T @ (self.Ax @ Wb), Wa.T @ (self.Az @ Wb), Wa.T @ (self.AbsAx @ Wb), Wa.T @ (self.AbsAz @ Wb))
+
+    def _x_grams(self, Xa, Xb):
+        st = self.stencil
+        return (Xa.T @ (st.L2x @ Xb), Xa.T @ (st.L2y @ Xb), Xa.T @ (st.L1x @ Xb), Xa.T @ (st.L1y @ Xb))
+
+    def _k_stream(self, K, WAxW, WAzW, WAbsAxW, WAbsAzW, dE):
+        st = self.stencil
+        return K - dE * ((st.L2x @ K) @ WAxW + (st.L2y @ K) @ WAzW + (st.L1x @ K) @ WAbsAxW + (st.L1y @ K) @ WAbsAzW)
+
+    def _l_stream(self, L, XL2xX, XL2yX, XL1xX, XL1yX, dE):
+        return L - dE * ((self.Ax @ L) @ XL2xX.T + (self.Az @ L) @ XL2yX.T
+                         + (self.AbsAx @ L) @ XL1xX.T + (self.AbsAz @ L) @ XL1yX.T)
+
+    def _s_stream(self, S, G, C, dE, sign=-1.0):
+        return S + sign * dE * (G[0] @ S @ C[0] + G[1] @ S @ C[1] + G[2] @ S @ C[2] + G[3] @ S @ C[3])
+
+    def truncate(self, X, S, W):
+        """``truncate!`` (``SolverCSD.jl:3369-3399``): l1 tail test, clamp [2, r]."""
+        s = self.settings
+        U, D, V = la.svd_full(S)
+        rMaxTotal = s.r
+        rMinTotal = 2
+        tol = s.theta * np.linalg.norm(D) ** s.thetaIndex
+        rmax = int(math.floor(D.size / 2))
+        for j in range(1, 2 * rmax + 1):
+            tmp = math.sqrt(np.sum(D[j - 1:2 * rmax]) ** 2)
+            if tmp < tol:
+                rmax = j
+                break
+        rmax = min(rmax, rMaxTotal)
+        rmax = max(rmax, rMinTotal)
+        return X @ U[:, :rmax], np.diag(D[:rmax]), W @ V[:, :rmax]
+
+    def outputs(self, X, S, W, psi):
+        U, Sig, V = la.svd_full(S)
+        return X @ U, 0.5 * math.sqrt(self.gamma[0]) * Sig, self.O @ (W @ V), W @ V, self.dose, psi
+
+
+def out_scatter_factor(L, mode, order=None):
+    """``W,S1,S2 = svd!(L); S = S2*Diagonal(S1)`` (``SolverCSD.jl:1071-1074``).
+
+    ``mode="det"`` returns W = orth(L) and S = L^T W, the same product W S^T = L.
+    """
+    if mode == "lapack":
+        W, S1, S2 = la.svd_full(L)
+        return W, S2 @ np.diag(S1)
+    W = la.orth(L, mode, order=order)
+    return W, L.T @ W
+
+
+def init_factors(solver, r):
+    """``svd!(zeros)`` factors (``SolverCSD.jl:931-938``): first r identity columns;
+    X's boundary rows are then zeroed (``:955``)."""
+    s = solver.settings
+    n = s.NCellsX * s.NCellsY
+    X = np.eye(n, r)
+    W = np.eye(solver.N, r)
+    S = np.zeros((r, r))
+    X[solver.boundaryIdx, :] = 0.0
+    return X, S, W
+
+
+def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None):
+    """``SolveFirstCollisionSourceDLR`` (``SolverCSD.jl:891-1120``).
+
+    Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, psi). ``max_steps``
+    stops after that many energy steps (a bounded sample of the sweep).
+    """
+    s = solver.settings
+    mode = solver.basis_mode
+    r = s.r
+    eTrafo = solver.csd.eTrafo
+    energy = solver.csd.eGrid
+    Scsd = solver.csd.S
+    psi = solver.setup_directions()
+    nx, ny = s.NCellsX, s.NCellsY
+    X, S, W = init_factors(solver, r)
+    bnd = solver.boundaryIdx
+    nE = eTrafo.size
+    dE = eTrafo[1] - eTrafo[0]
+    s.dE = dE
+    Mr = solver.MReduced
+    last = nE if max_steps is None else min(nE, 1 + max_steps)
+    for n in range(2, last + 1):
+        sigma = solver.csd.sigma_at_energy(energy[n - 1])
+        solver.apply_bc(psi, energy[n - 2], n - 1)
+        solver.dose_half(X, S, W, psi, dE, Scsd[n - 2])
+        solver.sweep(psi, dE, sigma[0])
+        Dvec = solver.dvec(sigma)
+        D = sigma[0] - Dvec
+        if n > 2:
+            # K-step
+            X[bnd, :] = 0.0
+            K = X @ S
+            C = solver._w_grams(W, W)
+            K = solver._k_stream(K, *C, dE)
+            XNew = la.orth(K, mode, order=solver.x_completion)
+            MUp = XNew.T @ X
+            # L-step
+            L = W @ S.T
+            G = solver._x_grams(X, X)
+            L = solver._l_stream(L, *G, dE)
+            WNew = la.orth(L, mode, order=solver.w_completion)
+            NUp = WNew.T @ W
+            W = WNew
+            X = XNew
+            # S-step
+            S = MUp @ S @ NUp.T
+            G = solver._x_grams(X, X)
+            C = solver._w_grams(W, W)
+            S = solver._s_stream(S, G, C, dE)
+        # out scattering
+        L = W @ S.T
+        L = L / (1.0 + dE * D)[:, None]
+        W, S = out_scatter_factor(L, mode, solver.w_completion)
+        # in scattering, K-step
+        X[bnd, :] = 0.0
+        K = X @ S
+        psiv = psi.reshape(nx * ny, -1)
+        K = K + dE * psiv @ (Mr.T @ (Dvec[:, None] * W))
+        K[bnd, :] = 0.0
+        XNew = la.orth(K, mode, order=solver.x_completion)
+        MUp = XNew.T @ X
+        # L-step
+        L = W @ S.T
+        L = L + dE * Dvec[:, None] * (Mr @ (psiv.T @ X))
+        WNew = la.orth(L, mode, order=solver.w_completion)
+        NUp = WNew.T @ W
+        W = WNew
+        X = XNew
+        # S-step
+        S = MUp @ S @ NUp.T
+        S = S + dE * (X.T @ psiv) @ Mr.T @ (Dvec[:, None] * W)
+        solver.dose_half(X, S, W, psi, dE, Scsd[n - 1])
+    return solver.outputs(X, S, W, psi)
