@@ -1,0 +1,143 @@
+/*
+ * titus.h -- C ABI of the B200-native CSD energy-step library (libtitus.so).
+ *
+ * Drop-in boundary for the dynamical-low-rank (DLR) energy loops of TITUS
+ * (CSMMLab/TITUS, code/SolverCSD.jl). The host keeps the reference's
+ * Settings / SolverCSD construction (grid, P_N matrices, quadrature, Roe
+ * matrices, CSD energy grid) and hands the assembled problem to this library;
+ * the energy loop runs on the GPU as one persistent kernel.
+ *
+ * Conventions: plain pointers and sizes, FP64, row-major matrices
+ * (X is n x r with row (i*ny + j) for cell (i, j), 0-based), int status
+ * returns (0 = success; titus_last_error() gives the message). No C++
+ * exceptions cross this boundary. A solver handle belongs to one host thread.
+ */
+#ifndef TITUS_H
+#define TITUS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TITUS_OK 0
+#define TITUS_ERR_ARG 1      /* invalid argument (sizes, null pointers) */
+#define TITUS_ERR_CUDA 2     /* CUDA runtime error */
+#define TITUS_ERR_DEVICE 3   /* device-side error flag (e.g. barrier timeout, breakdown) */
+#define TITUS_ERR_LIMIT 4    /* size beyond what this build supports */
+
+/* Integrators: SolverCSD.jl SolveFirstCollisionSourceDLR (:891-1120),
+ * SolveFirstCollisionSourceDLRParallel (:1726-2008),
+ * SolveFirstCollisionSourceDLRBUGRejection (:2011-2374). */
+#define TITUS_DLR_FIXED 0
+#define TITUS_PARALLEL_ADAPTIVE 1
+#define TITUS_BUG_ADAPTIVE 2
+
+/* Assembled problem. Replaces the fields of `SolverCSD{T}` that the energy
+ * loop reads (SolverCSD.jl:20-146) plus the per-step tables the loop derives
+ * from them (SigmaAtEnergy, PsiBeam). All arrays are host memory, copied by
+ * titus_create. */
+typedef struct titus_problem {
+    int32_t nx, ny;           /* NCellsX, NCellsY */
+    int32_t npn;              /* nPN; N = (nPN+1)^2 moments */
+    int32_t n_moments;        /* N */
+    int32_t n_ordinates;      /* q = number of reduced ordinates (idxBeam) */
+    int32_t n_energies;       /* nEnergies = length(csd.eTrafo) */
+    int32_t r;                /* settings.r */
+    double dx, dy;            /* settings.dx, settings.dy */
+    double theta;             /* settings.ϑ */
+    double theta_index;       /* settings.ϑIndex */
+    double c_eta;             /* settings.cη */
+    const double* density;    /* n: density at cell i*ny+j */
+    const double* e_trafo;    /* nE: csd.eTrafo */
+    const double* stopping;   /* nE: csd.S (dose weights) */
+    const double* bc_energy;  /* nE: PsiBeam energy factor at index k (scale*exp(-σE(E0-E_k)^2)*S[k]*ρmin) */
+    const double* sigma;      /* nE x (npn+1): SigmaAtEnergy(csd, eGrid[k]) */
+    const double* bc_space;   /* n: PsiBeam spatial factor at each cell (read on boundary cells) */
+    const double* bc_angle;   /* q: PsiBeam angular factor per reduced ordinate */
+    const double* omega;      /* q x 3: qReduced (Omega_x, Omega_y, Omega_z) */
+    const double* m_reduced;  /* N x q: MReduced (row-major) */
+    /* P_N operators as CSR (N x N): [0]=Ax, [1]=Az, [2]=|Ax|, [3]=|Az| */
+    const int32_t* op_rowptr[4];
+    const int32_t* op_col[4];
+    const double* op_val[4];
+    const int32_t* x_completion;   /* candidate cells for completing rank-deficient X bases */
+    int32_t n_x_completion;
+    const int32_t* w_completion;   /* candidate moments for completing rank-deficient W bases */
+    int32_t n_w_completion;
+    const int32_t* sweep_restore;  /* cells whose ordinate-0 value is restored after the sweep */
+    int32_t n_sweep_restore;
+} titus_problem_t;
+
+typedef struct titus_options {
+    int32_t team_ctas;     /* CTAs cooperating on one solve (0 = library default) */
+    int32_t max_steps;     /* stop after this many loop iterations (0 = full sweep) */
+    double rank_tol;       /* relative singular-value cut for numerical rank (0 = 1e-12) */
+} titus_options_t;
+
+/* Host result buffers (caller-owned). Factors are returned raw: X (n x r_cap),
+ * S (r_cap x r_cap), W (N x r_cap) in their leading `rank` columns; the
+ * caller forms svd(S) to build the reference's return tuple
+ * (X*U, 1/2 sqrt(gamma_0) Sigma, O*W*V, W*V, dose, psi). */
+typedef struct titus_result {
+    double* dose;          /* n */
+    double* X;             /* n x r_cap, row-major, leading dimension r_cap */
+    double* S;             /* r_cap x r_cap */
+    double* W;             /* N x r_cap */
+    double* psi;           /* n x q */
+    int32_t r_cap;         /* capacity (columns) of X, S, W */
+    int32_t rank;          /* out: rank of the returned factors */
+    int32_t steps_done;    /* out: loop iterations executed */
+    int32_t* rank_history; /* optional (nE): rank after each iteration, -1 if unused */
+    double* eta_history;   /* optional (nE): streaming eta (BUG), 0 otherwise */
+    double* bound_history; /* optional (nE): eta bound (BUG) */
+    double* time_history;  /* optional (nE): accumulated pseudo-time t (parallel) / energy (BUG) */
+} titus_result_t;
+
+typedef struct titus_solver titus_solver_t;
+
+/* Upload the problem and allocate device state (replaces the data that
+ * `SolverCSD(settings)` prepares, SolverCSD.jl:63-146). */
+int titus_create(const titus_problem_t* problem, titus_solver_t** out);
+
+/* Run one integrator over the energy grid on the device and copy the result
+ * to host buffers (replaces `Solve*(solver)` of SolverCSD.jl:891, 1726, 2011). */
+int titus_solve(titus_solver_t* solver, int32_t method, const titus_options_t* options,
+                titus_result_t* result);
+
+/* Same energy loop without the host copies: leaves the state on the device.
+ * `stream` is a cudaStream_t (NULL = legacy default stream). Used for
+ * device-resident timing; titus_fetch copies the state out afterwards. */
+int titus_solve_device(titus_solver_t* solver, int32_t method, const titus_options_t* options,
+                       void* stream);
+int titus_fetch(titus_solver_t* solver, titus_result_t* result);
+
+/* One-shot: create + solve + destroy with host buffers in and out. */
+int titus_solve_problem(const titus_problem_t* problem, int32_t method,
+                        const titus_options_t* options, titus_result_t* result);
+
+/* Checkpoint / resume: replace the device state (X, S, W of the given rank,
+ * psi, dose) and the next energy index `n_next` (1-based like the reference
+ * loop variable n), then titus_solve_from continues the loop from there. */
+int titus_set_state(titus_solver_t* solver, int32_t rank, const double* X, const double* S,
+                    const double* W, const double* psi, const double* dose, int32_t n_next);
+int titus_solve_from(titus_solver_t* solver, int32_t method, const titus_options_t* options,
+                     int32_t n_stop, titus_result_t* result);
+
+void titus_destroy(titus_solver_t* solver);
+
+/* Copy the last error message of this thread into buf (always terminated). */
+int titus_last_error(char* buf, size_t len);
+
+/* Build / capability queries. */
+int titus_max_rank(void);        /* largest basis width (columns) supported */
+int titus_max_ordinates(void);   /* largest q supported */
+const char* titus_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TITUS_H */

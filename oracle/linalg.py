@@ -11,14 +11,15 @@ with directions fixed by rounding noise. This module offers:
 * ``mode="det"``: a deterministic, rank-revealing rule that the CUDA path
   implements too. The numerical range of A is the span of the left singular
   vectors with sigma_j > tol * ||A||_2; missing directions are completed by
-  canonical vectors e_c taken in increasing c, each accepted when its residual
-  after two Gram-Schmidt passes against the basis so far exceeds 1/2.
+  canonical vectors e_c taken in the caller's candidate order (index order by
+  default, LAPACK's result for an exactly zero input), each accepted when its
+  residual after two Gram-Schmidt passes against the basis so far exceeds 1/2.
 """
 from __future__ import annotations
 
 import numpy as np
 
-RANK_TOL = 1e-13
+RANK_TOL = 1e-12
 
 
 def svd_full(A: np.ndarray):

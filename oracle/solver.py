@@ -27,7 +27,7 @@ from .stencils import Stencils
 class SolverCSD:
     """``mutable struct SolverCSD`` + constructor (``SolverCSD.jl:20-146``) at T = Float64."""
 
-    def __init__(self, settings, basis_mode: str = "lapack"):
+    def __init__(self, settings, basis_mode: str = "det"):
         s = settings
         self.settings = s
         self.basis_mode = basis_mode
@@ -66,16 +66,12 @@ class SolverCSD:
             pts = self.Q_points
             ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - pts[:, 0]) ** 2) * np.exp(-s.sigmaO3Inv * (s.Omega3 - pts[:, 2]) ** 2)
             self.psi_scale = s.psi_scale / ang.max()
-        # Completion candidates for rank-deficient bases (see oracle.linalg):
-        # boundary cells by ascending boundary-source amplitude, and odd (k < 0)
-        # moments before even ones.
-        bc_amp = np.exp(-s.sigmaXInv * (s.xMid[self.boundaryIdx // ny] - s.x0) ** 2) * \
-            np.exp(-s.sigmaYInv * (s.yMid[self.boundaryIdx % ny] - s.y0) ** 2)
-        cells, first = np.unique(self.boundaryIdx, return_index=True)
-        amp = bc_amp[first]
-        self.x_completion = cells[np.lexsort((cells, amp))]
-        ks = np.array([k for l in range(s.nPN + 1) for k in range(-l, l + 1)])
-        self.w_completion = np.concatenate([np.nonzero(ks < 0)[0], np.nonzero(ks >= 0)[0]])
+        # Completion candidates for rank-deficient bases (see oracle.linalg): the
+        # canonical vectors in index order, which is what LAPACK returns for an
+        # exactly zero input (identity columns). Spatial candidates are the
+        # boundary cells, whose rows are zero in every K the loop builds.
+        self.x_completion = np.unique(self.boundaryIdx)
+        self.w_completion = np.arange(self.N)
         self.qReduced = None
         self.MReduced = None
         self.OReduced = None
@@ -234,11 +230,14 @@ def init_factors(solver, r):
     return X, S, W
 
 
-def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None):
+def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
+                    n_begin: int = 2, return_state: bool = False):
     """``SolveFirstCollisionSourceDLR`` (``SolverCSD.jl:891-1120``).
 
     Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, psi). ``max_steps``
     stops after that many energy steps (a bounded sample of the sweep).
+    ``state`` (X, S, W, psi, dose after step ``n_begin - 1``) resumes the loop at
+    ``n_begin``; ``return_state`` returns that dict for the end of the run.
     """
     s = solver.settings
     mode = solver.basis_mode
@@ -249,13 +248,17 @@ def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None):
     psi = solver.setup_directions()
     nx, ny = s.NCellsX, s.NCellsY
     X, S, W = init_factors(solver, r)
+    if state is not None:
+        X, S, W = state["X"].copy(), state["S"].copy(), state["W"].copy()
+        psi = state["psi"].reshape(psi.shape).copy()
+        solver.dose = state["dose"].copy()
     bnd = solver.boundaryIdx
     nE = eTrafo.size
     dE = eTrafo[1] - eTrafo[0]
     s.dE = dE
     Mr = solver.MReduced
-    last = nE if max_steps is None else min(nE, 1 + max_steps)
-    for n in range(2, last + 1):
+    last = nE if max_steps is None else min(nE, n_begin - 1 + max_steps)
+    for n in range(n_begin, last + 1):
         sigma = solver.csd.sigma_at_energy(energy[n - 1])
         solver.apply_bc(psi, energy[n - 2], n - 1)
         solver.dose_half(X, S, W, psi, dE, Scsd[n - 2])
@@ -306,4 +309,229 @@ def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None):
         S = MUp @ S @ NUp.T
         S = S + dE * (X.T @ psiv) @ Mr.T @ (Dvec[:, None] * W)
         solver.dose_half(X, S, W, psi, dE, Scsd[n - 1])
+    if return_state:
+        return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), n_next=last + 1)
     return solver.outputs(X, S, W, psi)
+
+
+def _augment_tilde(solver, A_old, A_new, side):
+    """``Xtmp,_ = py"qr"([X K]); X1Tilde = Xtmp[:, (r+1):end]`` and the full Q.
+
+    Returns (Q, tilde) with Q the n x (r + r') factor and tilde = Q[:, r:].
+    """
+    order = solver.x_completion if side == "x" else solver.w_completion
+    Q = la.orth_augment(A_old, A_new, solver.basis_mode, order=order)
+    return Q, Q[:, A_old.shape[1]:]
+
+
+def _step_prologue(solver, psi, X, S, W, n, dE):
+    """BC, first dose half-step, uncollided sweep; returns (sigma, Dvec, D)."""
+    energy = solver.csd.eGrid
+    sigma = solver.csd.sigma_at_energy(energy[n - 1])
+    solver.apply_bc(psi, energy[n - 2], n - 1)
+    solver.dose_half(X, S, W, psi, dE, solver.csd.S[n - 2])
+    solver.sweep(psi, dE, sigma[0])
+    Dvec = solver.dvec(sigma)
+    return sigma, Dvec, sigma[0] - Dvec
+
+
+def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None):
+    """``SolveFirstCollisionSourceDLRParallel`` (``SolverCSD.jl:1726-2008``).
+
+    Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, rVec, psi) with
+    rVec (2 x nEnergies): row 0 the accumulated pseudo-time t, row 1 the rank.
+    """
+    s = solver.settings
+    mode = solver.basis_mode
+    r = int(math.floor(s.r / 2))
+    eTrafo = solver.csd.eTrafo
+    psi = solver.setup_directions()
+    nx, ny = s.NCellsX, s.NCellsY
+    X, S, W = init_factors(solver, r)
+    bnd = solver.boundaryIdx
+    nE = eTrafo.size
+    dE = eTrafo[1] - eTrafo[0]
+    s.dE = dE
+    Mr = solver.MReduced
+    rVec = r * np.ones((2, nE))
+    t = 0.0
+    last = nE if max_steps is None else min(nE, 1 + max_steps)
+    for n in range(2, last + 1):
+        sigma, Dvec, D = _step_prologue(solver, psi, X, S, W, n, dE)
+        if n > 2:
+            G = solver._x_grams(X, X)  # before X[bnd] = 0 (:1856-1859)
+            C = solver._w_grams(W, W)
+            X[bnd, :] = 0.0
+            K = X @ S
+            K = solver._k_stream(K, *C, dE)
+            _, X1T = _augment_tilde(solver, X, K, "x")
+            L = W @ S.T
+            L = solver._l_stream(L, *G, dE)
+            _, W1T = _augment_tilde(solver, W, L, "w")
+            S[...] = solver._s_stream(S, G, C, dE)  # S .= S .- dE ...
+            SNew = np.zeros((2 * r, 2 * r))
+            SNew[:r, :r] = S
+            SNew[r:, :r] = X1T.T @ K
+            SNew[:r, r:] = L.T @ W1T
+            X, S, W = solver.truncate(np.column_stack([X, X1T]), SNew, np.column_stack([W, W1T]))
+            r = S.shape[0]
+        # out scattering
+        L = W @ S.T
+        L = L / (1.0 + dE * D)[:, None]
+        W, Snew = out_scatter_factor(L, mode, solver.w_completion)
+        S[...] = Snew  # S .= S2 * Diagonal(S1)
+        # in scattering
+        MtDW = Mr.T @ (Dvec[:, None] * W)
+        psiv = psi.reshape(nx * ny, -1)
+        Xtpsi = X.T @ psiv  # before X[bnd] = 0 (:1904)
+        X[bnd, :] = 0.0
+        K = X @ S
+        K = K + dE * psiv @ MtDW
+        K[bnd, :] = 0.0
+        _, X1T = _augment_tilde(solver, X, K, "x")
+        L = W @ S.T
+        L = L + dE * Dvec[:, None] * (Mr @ Xtpsi.T)
+        _, W1T = _augment_tilde(solver, W, L, "w")
+        S[...] = S + dE * Xtpsi @ MtDW
+        SNew = np.zeros((2 * r, 2 * r))
+        SNew[:r, :r] = S
+        SNew[r:, :r] = X1T.T @ K
+        SNew[:r, r:] = L.T @ W1T
+        solver.dose_half(X, S, W, psi, dE, solver.csd.S[n - 1])
+        X, S, W = solver.truncate(np.column_stack([X, X1T]), SNew, np.column_stack([W, W1T]))
+        r = S.shape[0]
+        rVec[0, n - 1] = t
+        rVec[1, n - 1] = r
+        t += dE
+    U, Sig, V = la.svd_full(S)
+    return X @ U, 0.5 * math.sqrt(solver.gamma[0]) * Sig, solver.O @ (W @ V), W @ V, solver.dose, rVec, psi
+
+
+def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None):
+    """``SolveFirstCollisionSourceDLRBUGRejection`` (``SolverCSD.jl:2011-2374``).
+
+    The undefined name ``rmax`` (``:2205, :2295``) is read as ``settings.r``,
+    the bound the neighbouring branches use (``:2227, :2283``). Rejected steps
+    repeat with the doubled basis exactly as the reference does, including the
+    psi sweep and first dose half-step already applied (``n = n-1; continue``).
+    ``max_steps`` bounds the number of loop iterations.
+
+    Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, [E rank]^T,
+    [E eta], [E bound], psi).
+    """
+    s = solver.settings
+    mode = solver.basis_mode
+    rmax = s.r
+    r = int(math.floor(s.r / 2))
+    eTrafo = solver.csd.eTrafo
+    energy = solver.csd.eGrid
+    psi = solver.setup_directions()
+    nx, ny = s.NCellsX, s.NCellsY
+    X, S, W = init_factors(solver, r)
+    bnd = solver.boundaryIdx
+    nE = eTrafo.size
+    dE = eTrafo[1] - eTrafo[0]
+    s.dE = dE
+    Mr = solver.MReduced
+    t = 0.0
+    n = 1
+    timeVec, rankInTime, etaVec, etaVecTime, etaBoundVec = [], [], [], [], []
+    iters = 0
+    while t < nE * dE:
+        n += 1
+        if n == nE:
+            break
+        if max_steps is not None and iters >= max_steps:
+            break
+        iters += 1
+        timeVec.append(energy[n - 1])
+        rankInTime.append(r)
+        sigma, Dvec, D = _step_prologue(solver, psi, X, S, W, n, dE)
+        if n > 2:
+            G = solver._x_grams(X, X)
+            C = solver._w_grams(W, W)
+            X[bnd, :] = 0.0
+            K = X @ S
+            K = solver._k_stream(K, *C, dE)
+            X1, X1T = _augment_tilde(solver, X, K, "x")
+            Mu = X1.T @ X
+            L = W @ S.T
+            L = solver._l_stream(L, *G, dE)
+            W1, W1T = _augment_tilde(solver, W, L, "w")
+            Nu = W1.T @ W
+            W = W1
+            X = X1
+            S = Mu @ S @ Nu.T
+            G = solver._x_grams(X, X)
+            C = solver._w_grams(W, W)
+            Sup = solver._s_stream(S, G, C, dE)
+            XUP, SUP, WUP = solver.truncate(X, Sup, W)
+            if SUP.shape[0] == 2 * r and 2 * r < rmax:
+                r = 2 * r
+                n = n - 1
+            else:
+                Gt = solver._x_grams(X1T, X)
+                Ct = solver._w_grams(W, W1T)
+                eta = np.linalg.norm(Gt[0] @ S @ Ct[0] + Gt[1] @ S @ Ct[1] + Gt[2] @ S @ Ct[2] + Gt[3] @ S @ Ct[3])
+                etaVec.append(eta)
+                etaVecTime.append(energy[n - 1])
+                bound = s.c_eta * s.theta * max(1e-7, np.linalg.norm(Sup) ** s.thetaIndex) / dE
+                etaBoundVec.append(bound)
+                if eta > bound and 2 * r < s.r:
+                    r = 2 * r
+                    n = n - 1
+                    continue
+            S = SUP
+            X = XUP
+            W = WUP
+            r = S.shape[0]
+        # out scattering
+        L = W @ S.T
+        L = L / (1.0 + dE * D)[:, None]
+        W, Snew = out_scatter_factor(L, mode, solver.w_completion)
+        S[...] = Snew
+        # in scattering
+        MtDW = Mr.T @ (Dvec[:, None] * W)
+        psiv = psi.reshape(nx * ny, -1)
+        Xtpsi = X.T @ psiv
+        X[bnd, :] = 0.0
+        K = X @ S
+        K = K + dE * psiv @ MtDW
+        K[bnd, :] = 0.0
+        X1, X1T = _augment_tilde(solver, X, K, "x")
+        Mu = X1.T @ X
+        L = W @ S.T
+        L = L + dE * Dvec[:, None] * (Mr @ Xtpsi.T)
+        W1, W1T = _augment_tilde(solver, W, L, "w")
+        Nu = W1.T @ W
+        W = W1
+        X = X1
+        S = Mu @ S @ Nu.T
+        MtDW = Mr.T @ (Dvec[:, None] * W)
+        Xtpsi = X.T @ psiv
+        Sup = S + dE * Xtpsi @ MtDW
+        XUP, SUP, WUP = solver.truncate(X, Sup, W)
+        if SUP.shape[0] == 2 * r and 2 * r < s.r:
+            r = 2 * r
+            n = n - 1
+        else:
+            MtDWt = Mr.T @ (Dvec[:, None] * W1T)
+            Xtpsit = X1T.T @ psiv
+            eta = np.linalg.norm(Xtpsit @ MtDWt)
+            bound = s.c_eta * s.theta * max(1e-7, np.linalg.norm(SUP) ** s.thetaIndex) / dE
+            if eta > bound and 2 * r < rmax:
+                r = 2 * r
+                n = n - 1
+                continue
+        S = SUP
+        X = XUP
+        W = WUP
+        r = S.shape[0]
+        solver.dose_half(X, S, W, psi, dE, solver.csd.S[n - 1])
+        t += dE
+    U, Sig, V = la.svd_full(S)
+    rank_hist = np.array([timeVec, rankInTime], dtype=float)
+    eta_hist = np.array([etaVecTime, etaVec], dtype=float).T
+    bound_hist = np.array([etaVecTime, etaBoundVec], dtype=float).T
+    return (X @ U, 0.5 * math.sqrt(solver.gamma[0]) * Sig, solver.O @ (W @ V), W @ V, solver.dose,
+            rank_hist, eta_hist, bound_hist, psi)

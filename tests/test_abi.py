@@ -1,0 +1,42 @@
+"""The C ABI library loads and exports every symbol that include/titus.h declares."""
+import os
+import re
+
+import pytest
+
+from titus_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "titus.h")).read()
+    return sorted(set(re.findall(r"\b(titus_[a-z_]+)\s*\(", txt)))
+
+
+def test_header_matches_binding():
+    names = {n for n, _, _ in _lib.SIGNATURES}
+    assert set(declared_symbols()) == names
+
+
+def test_library_exports():
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libtitus.so not built (run titus_b200.build)")
+    lib = _lib.load()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert lib.titus_max_rank() >= 20
+    assert lib.titus_version().startswith(b"titus-b200")
+
+
+def test_invalid_problem_is_rejected_without_gpu():
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libtitus.so not built")
+    import ctypes as C
+    lib = _lib.load()
+    p = _lib.Problem()
+    p.nx = 2  # too small: rejected by validation before any CUDA call
+    h = C.c_void_p()
+    rc = lib.titus_create(C.byref(p), C.byref(h))
+    assert rc == 1
+    assert "nx" in _lib.last_error()

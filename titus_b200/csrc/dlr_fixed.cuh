@@ -1,0 +1,522 @@
+// Fixed-rank DLR energy loop (SolverCSD.jl SolveFirstCollisionSourceDLR :891-1120)
+// as phases of one persistent kernel. See dlr_kernel.cuh for the phase map.
+#pragma once
+#include "dlr_kernel.cuh"
+
+namespace titus {
+
+// ---- phase A: (pending) second dose half-step, boundary inflow, first dose
+// half-step, X[bnd,:] = 0.  Own cells only; no reduction.
+__device__ void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc) {
+    const DevProblem& P = x.P;
+    SmemLayout* sm = x.sm;
+    const int k = x.k;
+    const double* S = sm->slot[SL_S];
+    double* v = sm->vec;  // S W[0,:]^T
+    double* w0 = sm->vec + KM;
+    for (int j = threadIdx.x; j < k; j += NT) w0[j] = ldcg(x.st.W + j);
+    __syncthreads();
+    for (int i = threadIdx.x; i < k; i += NT) {
+        double s = 0.0;
+        for (int j = 0; j < k; ++j) s = fma(S[i * KM + j], w0[j], s);
+        v[i] = s;
+    }
+    __syncthreads();
+    const double dE = P.dE;
+    // dose half-steps use csd.S at 1-based n-1 for both the pending second
+    // half of step n-1 and the first half of step n (0-based index n-2)
+    const double sd = P.stopping[n - 2];
+    const double bce = P.bc_energy[n - 2];
+    for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT) {
+        double xv = 0.0;
+        for (int j = 0; j < k; ++j) xv = fma(x.st.X[(size_t)c * KM + j], v[j], xv);
+        double* pr = x.psi_in + (size_t)c * QM;
+        double dose = x.st.dose[c];
+        if (dose2_pending) {
+            double u = 0.0;
+            for (int kq = 0; kq < P.q; ++kq) u = fma(pr[kq], P.mred[kq], u);
+            dose += 0.5 * dE * (xv + u) * sd * P.rinv[c];
+        }
+        bool bnd = is_bnd(P, c);
+        if (do_bc) {
+            if (bnd) {
+                double bs = bce * P.bc_space[c];
+                for (int kq = 0; kq < P.q; ++kq) pr[kq] = bs * P.bc_angle[kq];
+            }
+            double u = 0.0;
+            for (int kq = 0; kq < P.q; ++kq) u = fma(pr[kq], P.mred[kq], u);
+            dose += 0.5 * dE * (xv + u) * sd * P.rinv[c];
+            if (bnd)
+                for (int j = 0; j < k; ++j) x.st.X[(size_t)c * KM + j] = 0.0;
+        }
+        x.st.dose[c] = dose;
+    }
+}
+
+// ---- uncollided sweep for own cells (psi_in -> psi_out)
+__device__ void sweep_cells(Ctx& x, double sigma0) {
+    const DevProblem& P = x.P;
+    const double dE = P.dE;
+    const double den = 1.0 + dE * sigma0;
+    const int q = P.q;
+    for (int e = threadIdx.x; e < (x.c1 - x.c0) * q; e += NT) {
+        int c = x.c0 + e / q, kq = e - (e / q) * q;
+        double pc = ldcg(x.psi_in + (size_t)c * QM + kq);
+        double flux = 0.0;
+        if (!is_bnd(P, c)) {
+            double ox = P.omega[kq * 3 + 0], oz = P.omega[kq * 3 + 2];
+            double f0 = pc * P.rinv[c];
+            double ew, ns;
+            if (ox >= 0.0) ew = f0 - ldcg(x.psi_in + (size_t)(c - P.ny) * QM + kq) * P.rinv[c - P.ny];
+            else ew = ldcg(x.psi_in + (size_t)(c + P.ny) * QM + kq) * P.rinv[c + P.ny] - f0;
+            if (oz >= 0.0) ns = f0 - ldcg(x.psi_in + (size_t)(c - 1) * QM + kq) * P.rinv[c - 1];
+            else ns = ldcg(x.psi_in + (size_t)(c + 1) * QM + kq) * P.rinv[c + 1] - f0;
+            flux = (ox / P.dx) * ew + (oz / P.dy) * ns;
+        }
+        double out = (pc - dE * flux) / den;
+        if (kq == 0 && P.restore[c]) out = pc;
+        x.psi_out[(size_t)c * QM + kq] = out;
+    }
+}
+
+// ---- streaming Grams X^T L_d X (own cells) and W^T A_d W (own moments):
+// partial layout [G_0..G_3 | C_0..C_3], each k x k.
+__device__ void stream_grams_partial(Ctx& x) {
+    SmemLayout* sm = x.sm;
+    const int k = x.k;
+    for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+        int nr = min(TR, x.c1 - r0);
+        load_rows(sm->tA, x.st.X, r0, nr, k);
+        stencil_tile(x, x.st.X, r0, nr, k, sm->tL);
+        __syncthreads();
+        for (int d = 0; d < 4; ++d) gram_acc(sm->acc, d * k * k, sm->tA, KM, k, sm->tL[d], KM, k, nr);
+        __syncthreads();
+    }
+    for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+        int nr = min(TR, x.m1 - r0);
+        load_rows(sm->tA, x.st.W, r0, nr, k);
+        spmm_tile(x, x.st.W, r0, nr, k, sm->tL);
+        __syncthreads();
+        for (int d = 0; d < 4; ++d) gram_acc(sm->acc, (4 + d) * k * k, sm->tA, KM, k, sm->tL[d], KM, k, nr);
+        __syncthreads();
+    }
+}
+
+// ---- range finder pass 1 (G1 = (A V)^T (A V)) on one side; A is n x k in global
+__device__ void rf_pass_b(Ctx& x, const double* A, int r0b, int r1b, const double* V, int k, int off) {
+    SmemLayout* sm = x.sm;
+    for (int r0 = r0b; r0 < r1b; r0 += TR) {
+        int nr = min(TR, r1b - r0);
+        load_rows(sm->tA, A, r0, nr, k);
+        __syncthreads();
+        tile_mm(sm->tO, sm->tA, V, nr, k, k);
+        __syncthreads();
+        gram_acc(sm->acc, off, sm->tO, KM, k, sm->tO, KM, k, nr);
+        __syncthreads();
+    }
+}
+// ---- range finder pass 2: C = A T1 (written to Cbuf), G2 = C^T C
+__device__ void rf_pass_c(Ctx& x, const double* A, double* Cbuf, int r0b, int r1b, const double* T1, int k,
+                          int rho, int off) {
+    SmemLayout* sm = x.sm;
+    for (int r0 = r0b; r0 < r1b; r0 += TR) {
+        int nr = min(TR, r1b - r0);
+        load_rows(sm->tA, A, r0, nr, k);
+        __syncthreads();
+        tile_mm(sm->tO, sm->tA, T1, nr, k, rho);
+        __syncthreads();
+        store_rows(Cbuf, sm->tO, r0, nr, rho);
+        gram_acc(sm->acc, off, sm->tO, KM, rho, sm->tO, KM, rho, nr);
+        __syncthreads();
+    }
+}
+
+// Range-finder tail shared by all orthonormalisations of one phase group:
+// after G0 for the X side (off gx) and/or W side (off gw) is published and the
+// team barrier passed, run the two remaining passes. On return slots
+// SL_RIK/SL_RIL hold R^{-1} of the CholQR, CX/CW hold C, x.rhoK/x.rhoL the
+// numerical ranks, and the W completion is prepared.
+// Returns false if the team aborted.
+__device__ bool range_finder(Ctx& x, const double* AX, const double* AW, bool doX, bool doW, int k) {
+    SmemLayout* sm = x.sm;
+    const double tol = x.P.rank_tol;
+    // eig of G0 (reduced into ja by the caller's reduce): X side first
+    if (doX) {
+        reduce_into(x, 0, k, k, sm->ja);
+        rf_eig0(x, sm->slot[SL_VK], sm->lamK, k);
+    }
+    if (doW) {
+        reduce_into(x, doX ? k * k : 0, k, k, sm->ja);
+        rf_eig0(x, sm->slot[SL_VL], sm->lamL, k);
+    }
+    // pass B
+    acc_zero(x, 2 * k * k);
+    if (doX) rf_pass_b(x, AX, x.c0, x.c1, sm->slot[SL_VK], k, 0);
+    if (doW) rf_pass_b(x, AW, x.m0, x.m1, sm->slot[SL_VL], k, k * k);
+    acc_publish(x, 2 * k * k);
+    if (!team_sync(x.st.bar, x.st.status, x.G)) return false;
+    if (doX) {
+        reduce_into(x, 0, k, k, sm->ja);
+        x.rhoK = rf_eig1(x, sm->slot[SL_VK], sm->slot[SL_TK], k, tol);
+    }
+    if (doW) {
+        reduce_into(x, k * k, k, k, sm->ja);
+        x.rhoL = rf_eig1(x, sm->slot[SL_VL], sm->slot[SL_TL], k, tol);
+    }
+    // pass C
+    acc_zero(x, 2 * k * k);
+    if (doX) rf_pass_c(x, AX, x.CX, x.c0, x.c1, sm->slot[SL_TK], k, x.rhoK, 0);
+    if (doW) rf_pass_c(x, AW, x.CW, x.m0, x.m1, sm->slot[SL_TL], k, x.rhoL, k * k);
+    acc_publish(x, 2 * k * k);
+    if (!team_sync(x.st.bar, x.st.status, x.G)) return false;
+    if (doX) {
+        reduce_into(x, 0, x.rhoK, x.rhoK, sm->ja);
+        chol_inv(sm->ja, sm->slot[SL_RK], sm->slot[SL_RIK], x.rhoK, x.st.status);
+        if (k - x.rhoK > x.P.nxcomp && threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+    }
+    if (doW) {
+        reduce_into(x, k * k, x.rhoL, x.rhoL, sm->ja);
+        chol_inv(sm->ja, sm->slot[SL_RL], sm->slot[SL_RIL], x.rhoL, x.st.status);
+        w_complete(x, x.rhoL, k - x.rhoL);
+    }
+    __syncthreads();
+    return true;
+}
+
+// small: D = A S B^T (k x k) with scratch
+__device__ void sm_asbt(double* D, const double* A, const double* S, const double* B, double* tmp, int k) {
+    sm_mm(tmp, A, S, k, k, k);
+    sm_mmt(D, tmp, B, k, k, k);
+}
+
+template <int METHOD>
+__global__ void __launch_bounds__(NT, 1)
+dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int dose2_pending_in) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SmemLayout* sm = reinterpret_cast<SmemLayout*>(smem_raw);
+    Ctx x;
+    x.P = P;
+    x.G = G;
+    x.b = blockIdx.x % G;
+    x.st = states[blockIdx.x / G];
+    x.sm = sm;
+    x.c0 = (int)((long long)x.b * P.n / G);
+    x.c1 = (int)((long long)(x.b + 1) * P.n / G);
+    x.m0 = (int)((long long)x.b * P.N / G);
+    x.m1 = (int)((long long)(x.b + 1) * P.N / G);
+    x.CX = x.st.K;          // C of the X-side range finder reuses K after K is consumed
+    x.CW = x.st.L + (size_t)P.N * KM;  // W side: second half of the L allocation
+    const int k = ldcg(x.st.info + 0);
+    x.k = k;
+    int psi_idx = ldcg(x.st.info + 2);
+    for (int e = threadIdx.x; e < KK; e += NT) sm->slot[SL_S][e] = ldcg(x.st.S + e);
+    __syncthreads();
+    bool pending = dose2_pending_in != 0;
+    int steps = 0;
+    double* Sm = sm->slot[SL_S];
+    for (int n = n_begin; n <= n_end; ++n) {
+        x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
+        x.psi_out = psi_idx ? x.st.psi0 : x.st.psi1;
+        const double* sig = P.sigma + (size_t)(n - 1) * (P.npn + 1);
+        const double dE = P.dE;
+        // ---------------- phase A
+        phase_bc_dose(x, n, pending, true);
+        pending = false;
+        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        // ---------------- phase B: sweep + streaming Grams
+        sweep_cells(x, sig[0]);
+        const bool stream = (n > 2);
+        if (stream) {
+            acc_zero(x, 8 * k * k);
+            stream_grams_partial(x);
+            acc_publish(x, 8 * k * k);
+        }
+        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        psi_idx ^= 1;
+        x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;  // swept psi
+        if (stream) {
+            for (int d = 0; d < 4; ++d) {
+                reduce_into(x, d * k * k, k, k, sm->slot[SL_G0 + d]);
+                reduce_into(x, (4 + d) * k * k, k, k, sm->slot[SL_C0 + d]);
+            }
+            // SC_d = S C_d -> slot C_d ; SG_d = S^T G_d^T -> slot G_d
+            for (int d = 0; d < 4; ++d) {
+                sm_mm(sm->slot[SL_P0], Sm, sm->slot[SL_C0 + d], k, k, k);
+                sm_copy(sm->slot[SL_C0 + d], sm->slot[SL_P0], k, k);
+                // (S^T G^T)[i][j] = sum_l S[l][i] G[j][l]
+                for (int e = threadIdx.x; e < k * k; e += NT) {
+                    int i = e / k, j = e % k;
+                    double s = 0.0;
+                    for (int l = 0; l < k; ++l) s = fma(Sm[l * KM + i], sm->slot[SL_G0 + d][j * KM + l], s);
+                    sm->slot[SL_P0][i * KM + j] = s;
+                }
+                __syncthreads();
+                sm_copy(sm->slot[SL_G0 + d], sm->slot[SL_P0], k, k);
+            }
+            // ---------------- phase C: K and L streaming updates
+            acc_zero(x, 2 * k * k);
+            for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+                int nr = min(TR, x.c1 - r0);
+                load_rows(sm->tA, x.st.X, r0, nr, k);
+                stencil_tile(x, x.st.X, r0, nr, k, sm->tL);
+                __syncthreads();
+                for (int e = threadIdx.x; e < nr * k; e += NT) {
+                    int r = e / k, j = e % k;
+                    double s = 0.0;
+                    for (int l = 0; l < k; ++l) s = fma(sm->tA[r * KM + l], Sm[l * KM + j], s);
+                    double t = 0.0;
+                    for (int d = 0; d < 4; ++d)
+                        for (int l = 0; l < k; ++l) t = fma(sm->tL[d][r * KM + l], sm->slot[SL_C0 + d][l * KM + j], t);
+                    sm->tO[r * KM + j] = s - dE * t;
+                }
+                __syncthreads();
+                store_rows(x.st.K, sm->tO, r0, nr, k);
+                gram_acc(sm->acc, 0, sm->tO, KM, k, sm->tO, KM, k, nr);
+                __syncthreads();
+            }
+            for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+                int nr = min(TR, x.m1 - r0);
+                load_rows(sm->tA, x.st.W, r0, nr, k);
+                spmm_tile(x, x.st.W, r0, nr, k, sm->tL);
+                __syncthreads();
+                for (int e = threadIdx.x; e < nr * k; e += NT) {
+                    int r = e / k, j = e % k;
+                    double s = 0.0;  // (W S^T)[r][j] = sum_l W[r][l] S[j][l]
+                    for (int l = 0; l < k; ++l) s = fma(sm->tA[r * KM + l], Sm[j * KM + l], s);
+                    double t = 0.0;
+                    for (int d = 0; d < 4; ++d)
+                        for (int l = 0; l < k; ++l) t = fma(sm->tL[d][r * KM + l], sm->slot[SL_G0 + d][l * KM + j], t);
+                    sm->tO[r * KM + j] = s - dE * t;
+                }
+                __syncthreads();
+                store_rows(x.st.L, sm->tO, r0, nr, k);
+                gram_acc(sm->acc, k * k, sm->tO, KM, k, sm->tO, KM, k, nr);
+                __syncthreads();
+            }
+            acc_publish(x, 2 * k * k);
+            if (!team_sync(x.st.bar, x.st.status, G)) return;
+            // ---------------- phases D, E: range finders of K and L
+            if (!range_finder(x, x.st.K, x.st.L, true, true, k)) return;
+            // ---------------- phase F: new bases, MUp = XNew^T X, NUp = WNew^T W
+            acc_zero(x, 2 * k * k);
+            for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+                int nr = min(TR, x.c1 - r0);
+                x_basis_tile(x, r0, nr, x.rhoK, k, sm->tO);
+                load_rows(sm->tA, x.st.X, r0, nr, k);
+                __syncthreads();
+                gram_acc(sm->acc, 0, sm->tO, KM, k, sm->tA, KM, k, nr);
+                __syncthreads();
+                store_rows(x.st.X, sm->tO, r0, nr, k);
+                __syncthreads();
+            }
+            for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+                int nr = min(TR, x.m1 - r0);
+                w_basis_tile(x, r0, nr, x.rhoL, k - x.rhoL, sm->tO);
+                load_rows(sm->tA, x.st.W, r0, nr, k);
+                __syncthreads();
+                gram_acc(sm->acc, k * k, sm->tO, KM, k, sm->tA, KM, k, nr);
+                __syncthreads();
+                store_rows(x.st.W, sm->tO, r0, nr, k);
+                __syncthreads();
+            }
+            acc_publish(x, 2 * k * k);
+            if (!team_sync(x.st.bar, x.st.status, G)) return;
+            reduce_into(x, 0, k, k, sm->slot[SL_M]);
+            reduce_into(x, k * k, k, k, sm->slot[SL_N]);
+            // S1 = MUp S NUp^T -> slot S
+            sm_asbt(sm->slot[SL_P0 + 1], sm->slot[SL_M], Sm, sm->slot[SL_N], sm->slot[SL_P0], k);
+            sm_copy(Sm, sm->slot[SL_P0 + 1], k, k);
+            // ---------------- phase G: S-step Grams with the new X, W
+            acc_zero(x, 8 * k * k);
+            stream_grams_partial(x);
+            acc_publish(x, 8 * k * k);
+            if (!team_sync(x.st.bar, x.st.status, G)) return;
+            for (int d = 0; d < 4; ++d) {
+                reduce_into(x, d * k * k, k, k, sm->slot[SL_G0 + d]);
+                reduce_into(x, (4 + d) * k * k, k, k, sm->slot[SL_C0 + d]);
+            }
+            // S = S1 - dE sum_d G_d S1 C_d
+            sm_zero(sm->slot[SL_P0 + 2], k, k);
+            for (int d = 0; d < 4; ++d) {
+                sm_mm(sm->slot[SL_P0], sm->slot[SL_G0 + d], Sm, k, k, k);
+                sm_mm(sm->slot[SL_P0 + 1], sm->slot[SL_P0], sm->slot[SL_C0 + d], k, k, k);
+                for (int e = threadIdx.x; e < k * k; e += NT)
+                    sm->slot[SL_P0 + 2][(e / k) * KM + e % k] += sm->slot[SL_P0 + 1][(e / k) * KM + e % k];
+                __syncthreads();
+            }
+            for (int e = threadIdx.x; e < k * k; e += NT) Sm[(e / k) * KM + e % k] -= dE * sm->slot[SL_P0 + 2][(e / k) * KM + e % k];
+            __syncthreads();
+        }
+        // ---------------- phase H: out-scattering L (W side); P = psi^T X (X side, X[bnd]=0)
+        acc_zero(x, k * k + P.q * k);
+        for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT)
+            if (is_bnd(P, c))
+                for (int j = 0; j < k; ++j) x.st.X[(size_t)c * KM + j] = 0.0;
+        __syncthreads();
+        for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+            int nr = min(TR, x.m1 - r0);
+            load_rows(sm->tA, x.st.W, r0, nr, k);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nr * k; e += NT) {
+                int r = e / k, j = e % k;
+                double s = 0.0;
+                for (int l = 0; l < k; ++l) s = fma(sm->tA[r * KM + l], Sm[j * KM + l], s);
+                int m = r0 + r;
+                double D = sig[0] - sig[P.lof[m]];
+                sm->tO[r * KM + j] = s / (1.0 + dE * D);
+            }
+            __syncthreads();
+            store_rows(x.st.L, sm->tO, r0, nr, k);
+            gram_acc(sm->acc, 0, sm->tO, KM, k, sm->tO, KM, k, nr);
+            __syncthreads();
+        }
+        for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+            int nr = min(TR, x.c1 - r0);
+            load_rows(sm->tA, x.st.X, r0, nr, k);
+            for (int e = threadIdx.x; e < nr * P.q; e += NT)
+                sm->tP[(e / P.q) * QM + e % P.q] = ldcg(x.psi_in + (size_t)(r0 + e / P.q) * QM + e % P.q);
+            __syncthreads();
+            gram_acc(sm->acc, k * k, sm->tP, QM, P.q, sm->tA, KM, k, nr);
+            __syncthreads();
+        }
+        acc_publish(x, k * k + P.q * k);
+        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        // keep P = psi^T X (q x k) in slot P0+3 ; G0 of L into ja via range_finder
+        reduce_into(x, k * k, P.q, k, sm->slot[SL_P0 + 3]);
+        // range finder expects G0 of the W side at partial offset 0 when doX is false
+        if (!range_finder(x, nullptr, x.st.L, false, true, k)) return;
+        // ---------------- phase K: W = basis(L); S = L^T W ; Bk = MRed^T diag(Dvec) W
+        acc_zero(x, k * k + P.q * k);
+        for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+            int nr = min(TR, x.m1 - r0);
+            w_basis_tile(x, r0, nr, x.rhoL, k - x.rhoL, sm->tO);
+            load_rows(sm->tA, x.st.L, r0, nr, k);
+            for (int e = threadIdx.x; e < nr * P.q; e += NT) {
+                int r = e / P.q, kq = e % P.q;
+                int m = r0 + r;
+                sm->tP[r * QM + kq] = P.mred[(size_t)m * P.q + kq] * sig[P.lof[m]];
+            }
+            __syncthreads();
+            gram_acc(sm->acc, 0, sm->tA, KM, k, sm->tO, KM, k, nr);
+            gram_acc(sm->acc, k * k, sm->tP, QM, P.q, sm->tO, KM, k, nr);
+            __syncthreads();
+            store_rows(x.st.W, sm->tO, r0, nr, k);
+            __syncthreads();
+        }
+        acc_publish(x, k * k + P.q * k);
+        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        reduce_into(x, 0, k, k, Sm);
+        reduce_into(x, k * k, P.q, k, sm->slot[SL_P0 + 2]);  // Bk (q x k)
+        // ---------------- phase L: in-scattering K (X side) and L (W side)
+        acc_zero(x, 2 * k * k);
+        for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+            int nr = min(TR, x.c1 - r0);
+            load_rows(sm->tA, x.st.X, r0, nr, k);
+            for (int e = threadIdx.x; e < nr * P.q; e += NT)
+                sm->tP[(e / P.q) * QM + e % P.q] = ldcg(x.psi_in + (size_t)(r0 + e / P.q) * QM + e % P.q);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nr * k; e += NT) {
+                int r = e / k, j = e % k;
+                double s = 0.0;
+                if (!is_bnd(P, r0 + r)) {
+                    for (int l = 0; l < k; ++l) s = fma(sm->tA[r * KM + l], Sm[l * KM + j], s);
+                    double t = 0.0;
+                    for (int kq = 0; kq < P.q; ++kq) t = fma(sm->tP[r * QM + kq], sm->slot[SL_P0 + 2][kq * KM + j], t);
+                    s += dE * t;
+                }
+                sm->tO[r * KM + j] = s;
+            }
+            __syncthreads();
+            store_rows(x.st.K, sm->tO, r0, nr, k);
+            gram_acc(sm->acc, 0, sm->tO, KM, k, sm->tO, KM, k, nr);
+            __syncthreads();
+        }
+        for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+            int nr = min(TR, x.m1 - r0);
+            load_rows(sm->tA, x.st.W, r0, nr, k);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nr * k; e += NT) {
+                int r = e / k, j = e % k;
+                int m = r0 + r;
+                double s = 0.0;
+                for (int l = 0; l < k; ++l) s = fma(sm->tA[r * KM + l], Sm[j * KM + l], s);
+                double t = 0.0;  // (MRed P)[m][j]
+                for (int kq = 0; kq < P.q; ++kq) t = fma(P.mred[(size_t)m * P.q + kq], sm->slot[SL_P0 + 3][kq * KM + j], t);
+                sm->tO[r * KM + j] = s + dE * sig[P.lof[m]] * t;
+            }
+            __syncthreads();
+            store_rows(x.st.L, sm->tO, r0, nr, k);
+            gram_acc(sm->acc, k * k, sm->tO, KM, k, sm->tO, KM, k, nr);
+            __syncthreads();
+        }
+        acc_publish(x, 2 * k * k);
+        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        if (!range_finder(x, x.st.K, x.st.L, true, true, k)) return;
+        // ---------------- phase O: new bases; MUp, X^T psi, NUp, MRed^T D W
+        const int offM = 0, offXp = k * k, offN = k * k + k * P.q, offB = 2 * k * k + k * P.q;
+        acc_zero(x, 2 * k * k + 2 * k * P.q);
+        for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+            int nr = min(TR, x.c1 - r0);
+            x_basis_tile(x, r0, nr, x.rhoK, k, sm->tO);
+            load_rows(sm->tA, x.st.X, r0, nr, k);
+            for (int e = threadIdx.x; e < nr * P.q; e += NT)
+                sm->tP[(e / P.q) * QM + e % P.q] = ldcg(x.psi_in + (size_t)(r0 + e / P.q) * QM + e % P.q);
+            __syncthreads();
+            gram_acc(sm->acc, offM, sm->tO, KM, k, sm->tA, KM, k, nr);
+            gram_acc(sm->acc, offXp, sm->tO, KM, k, sm->tP, QM, P.q, nr);
+            __syncthreads();
+            store_rows(x.st.X, sm->tO, r0, nr, k);
+            __syncthreads();
+        }
+        for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+            int nr = min(TR, x.m1 - r0);
+            w_basis_tile(x, r0, nr, x.rhoL, k - x.rhoL, sm->tO);
+            load_rows(sm->tA, x.st.W, r0, nr, k);
+            for (int e = threadIdx.x; e < nr * P.q; e += NT) {
+                int r = e / P.q, kq = e % P.q;
+                int m = r0 + r;
+                sm->tP[r * QM + kq] = P.mred[(size_t)m * P.q + kq] * sig[P.lof[m]];
+            }
+            __syncthreads();
+            gram_acc(sm->acc, offN, sm->tO, KM, k, sm->tA, KM, k, nr);
+            gram_acc(sm->acc, offB, sm->tP, QM, P.q, sm->tO, KM, k, nr);
+            __syncthreads();
+            store_rows(x.st.W, sm->tO, r0, nr, k);
+            __syncthreads();
+        }
+        acc_publish(x, 2 * k * k + 2 * k * P.q);
+        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        reduce_into(x, offM, k, k, sm->slot[SL_M]);
+        reduce_into(x, offXp, k, P.q, sm->slot[SL_P0 + 3]);   // XNew^T psi (k x q)
+        reduce_into(x, offN, k, k, sm->slot[SL_N]);
+        reduce_into(x, offB, P.q, k, sm->slot[SL_P0 + 2]);    // MRed^T D WNew (q x k)
+        // S = MUp S NUp^T + dE (X^T psi)(MRed^T D W)
+        sm_asbt(sm->slot[SL_P0 + 1], sm->slot[SL_M], Sm, sm->slot[SL_N], sm->slot[SL_P0], k);
+        sm_mm(sm->slot[SL_P0], sm->slot[SL_P0 + 3], sm->slot[SL_P0 + 2], k, P.q, k);
+        for (int e = threadIdx.x; e < k * k; e += NT) {
+            int i = e / k, j = e % k;
+            Sm[i * KM + j] = sm->slot[SL_P0 + 1][i * KM + j] + dE * sm->slot[SL_P0][i * KM + j];
+        }
+        __syncthreads();
+        pending = true;
+        ++steps;
+        if (x.b == 0 && threadIdx.x == 0 && x.st.rank_hist) x.st.rank_hist[n - 1] = k;
+    }
+    // final second dose half-step of the last step (phase A without inflow)
+    if (pending && n_end >= n_begin) {
+        x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
+        // the last step's index is n_end: its dose weight is csd.S[n_end] (1-based)
+        phase_bc_dose(x, n_end + 1, true, false);
+    }
+    if (x.b == 0) {
+        for (int e = threadIdx.x; e < KK; e += NT) x.st.S[e] = Sm[e];
+        if (threadIdx.x == 0) {
+            x.st.info[0] = k;
+            x.st.info[1] = steps;
+            x.st.info[2] = psi_idx;
+            x.st.info[3] = n_end + 1;
+        }
+    }
+}
+
+}  // namespace titus

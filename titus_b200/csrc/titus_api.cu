@@ -1,0 +1,407 @@
+// C ABI of libtitus (include/titus.h): problem upload, device state, launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/titus.h"
+#include "dlr_fixed.cuh"
+
+using namespace titus;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(TITUS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int upload(T** dptr, const T* host, size_t count) {
+    *dptr = nullptr;
+    if (count == 0) return TITUS_OK;
+    CK(cudaMalloc((void**)dptr, count * sizeof(T)));
+    if (host) CK(cudaMemcpy(*dptr, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    return TITUS_OK;
+}
+
+}  // namespace
+
+struct titus_solver {
+    DevProblem P{};
+    int n = 0, N = 0, q = 0, nE = 0;
+    std::vector<void*> allocs;
+    // single-team state
+    TeamState st{};
+    TeamState* d_st = nullptr;
+    int team_ctas = 0;
+    int device = 0;
+    int num_sms = 0;
+    int r = 0;
+    int last_method = -1;
+
+    template <class T>
+    int alloc(T** p, size_t count, const T* host = nullptr) {
+        int rc = upload(p, host, count);
+        if (rc == TITUS_OK && *p) allocs.push_back((void*)*p);
+        return rc;
+    }
+    ~titus_solver() {
+        for (void* p : allocs) cudaFree(p);
+    }
+};
+
+static int validate(const titus_problem_t* pb) {
+    if (!pb) return fail(TITUS_ERR_ARG, "problem is NULL");
+    if (pb->nx < 3 || pb->ny < 3) return fail(TITUS_ERR_ARG, "need nx, ny >= 3 (got %d, %d)", pb->nx, pb->ny);
+    if (pb->npn < 0) return fail(TITUS_ERR_ARG, "npn < 0");
+    if (pb->n_moments != (pb->npn + 1) * (pb->npn + 1))
+        return fail(TITUS_ERR_ARG, "n_moments %d != (npn+1)^2", pb->n_moments);
+    if (pb->n_ordinates < 1) return fail(TITUS_ERR_ARG, "n_ordinates < 1");
+    if (pb->n_ordinates > QM) return fail(TITUS_ERR_LIMIT, "n_ordinates %d > %d supported", pb->n_ordinates, QM);
+    if (pb->n_energies < 2) return fail(TITUS_ERR_ARG, "n_energies < 2");
+    if (pb->r < 1) return fail(TITUS_ERR_ARG, "r < 1");
+    if (pb->r > KM) return fail(TITUS_ERR_LIMIT, "rank %d > %d supported by this build", pb->r, KM);
+    if (pb->r > pb->n_moments) return fail(TITUS_ERR_ARG, "r %d > n_moments %d", pb->r, pb->n_moments);
+    if (!(pb->dx > 0) || !(pb->dy > 0)) return fail(TITUS_ERR_ARG, "dx, dy must be > 0");
+    const void* req[] = {pb->density, pb->e_trafo, pb->stopping, pb->bc_energy, pb->sigma,
+                         pb->bc_space, pb->bc_angle, pb->omega, pb->m_reduced};
+    for (const void* p : req)
+        if (!p) return fail(TITUS_ERR_ARG, "a required problem array is NULL");
+    for (int d = 0; d < 4; ++d)
+        if (!pb->op_rowptr[d] || (!pb->op_col[d] && pb->op_rowptr[d][pb->n_moments] > 0) ||
+            (!pb->op_val[d] && pb->op_rowptr[d][pb->n_moments] > 0))
+            return fail(TITUS_ERR_ARG, "operator %d CSR arrays missing", d);
+    if (pb->n_x_completion < 0 || pb->n_w_completion < 0 || pb->n_sweep_restore < 0)
+        return fail(TITUS_ERR_ARG, "negative list length");
+    const int n = pb->nx * pb->ny;
+    for (int i = 0; i < n; ++i)
+        if (!(pb->density[i] > 0)) return fail(TITUS_ERR_ARG, "density must be > 0 (cell %d)", i);
+    for (int i = 0; i < pb->n_x_completion; ++i)
+        if (pb->x_completion[i] < 0 || pb->x_completion[i] >= n) return fail(TITUS_ERR_ARG, "x_completion out of range");
+    for (int i = 0; i < pb->n_w_completion; ++i)
+        if (pb->w_completion[i] < 0 || pb->w_completion[i] >= pb->n_moments)
+            return fail(TITUS_ERR_ARG, "w_completion out of range");
+    for (int i = 0; i < pb->n_sweep_restore; ++i)
+        if (pb->sweep_restore[i] < 0 || pb->sweep_restore[i] >= n) return fail(TITUS_ERR_ARG, "sweep_restore out of range");
+    for (int d = 0; d < 4; ++d) {
+        const int32_t* rp = pb->op_rowptr[d];
+        if (rp[0] != 0) return fail(TITUS_ERR_ARG, "operator %d rowptr[0] != 0", d);
+        for (int m = 0; m < pb->n_moments; ++m)
+            if (rp[m + 1] < rp[m]) return fail(TITUS_ERR_ARG, "operator %d rowptr not monotone", d);
+        for (int p = 0; p < rp[pb->n_moments]; ++p)
+            if (pb->op_col[d][p] < 0 || pb->op_col[d][p] >= pb->n_moments)
+                return fail(TITUS_ERR_ARG, "operator %d column index out of range", d);
+    }
+    return TITUS_OK;
+}
+
+extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
+    if (!out) return fail(TITUS_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = validate(pb);
+    if (rc) return rc;
+    auto* s = new titus_solver();
+    auto cleanup = [&](int code) {
+        delete s;
+        return code;
+    };
+    CK(cudaGetDevice(&s->device));
+    CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
+    int coop = 0;
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device));
+    if (!coop) return cleanup(fail(TITUS_ERR_CUDA, "device does not support cooperative launch"));
+    const int n = pb->nx * pb->ny, N = pb->n_moments, q = pb->n_ordinates, nE = pb->n_energies;
+    s->n = n;
+    s->N = N;
+    s->q = q;
+    s->nE = nE;
+    s->r = pb->r;
+    DevProblem& P = s->P;
+    P.nx = pb->nx;
+    P.ny = pb->ny;
+    P.n = n;
+    P.N = N;
+    P.npn = pb->npn;
+    P.q = q;
+    P.nE = nE;
+    P.r = pb->r;
+    P.dx = pb->dx;
+    P.dy = pb->dy;
+    P.dE = pb->e_trafo[1] - pb->e_trafo[0];
+    P.theta = pb->theta;
+    P.theta_index = pb->theta_index;
+    P.c_eta = pb->c_eta;
+    P.rank_tol = 1e-12;
+    std::vector<double> rinv(n);
+    for (int i = 0; i < n; ++i) rinv[i] = 1.0 / pb->density[i];
+    std::vector<int32_t> lof(N);
+    for (int l = 0; l <= pb->npn; ++l)
+        for (int kk = -l; kk <= l; ++kk) lof[l * l + kk + l] = l;
+    std::vector<uint8_t> restore(n, 0);
+    for (int i = 0; i < pb->n_sweep_restore; ++i) restore[pb->sweep_restore[i]] = 1;
+    double* d_rinv;
+    double* d_stop;
+    double* d_bce;
+    double* d_sig;
+    double* d_bcs;
+    double* d_bca;
+    double* d_om;
+    double* d_mr;
+    int32_t* d_lof;
+    uint8_t* d_res;
+    int32_t* d_xc = nullptr;
+    int32_t* d_wc = nullptr;
+    if ((rc = s->alloc(&d_rinv, n, rinv.data())) || (rc = s->alloc(&d_stop, nE, pb->stopping)) ||
+        (rc = s->alloc(&d_bce, nE, pb->bc_energy)) ||
+        (rc = s->alloc(&d_sig, (size_t)nE * (pb->npn + 1), pb->sigma)) || (rc = s->alloc(&d_bcs, n, pb->bc_space)) ||
+        (rc = s->alloc(&d_bca, q, pb->bc_angle)) || (rc = s->alloc(&d_om, (size_t)q * 3, pb->omega)) ||
+        (rc = s->alloc(&d_mr, (size_t)N * q, pb->m_reduced)) || (rc = s->alloc(&d_lof, N, lof.data())) ||
+        (rc = s->alloc(&d_res, n, restore.data())) ||
+        (rc = s->alloc(&d_xc, pb->n_x_completion, pb->x_completion)) ||
+        (rc = s->alloc(&d_wc, pb->n_w_completion, pb->w_completion)))
+        return cleanup(rc);
+    P.rinv = d_rinv;
+    P.stopping = d_stop;
+    P.bc_energy = d_bce;
+    P.sigma = d_sig;
+    P.bc_space = d_bcs;
+    P.bc_angle = d_bca;
+    P.omega = d_om;
+    P.mred = d_mr;
+    P.lof = d_lof;
+    P.restore = d_res;
+    P.xcomp = d_xc;
+    P.nxcomp = pb->n_x_completion;
+    P.wcomp = d_wc;
+    P.nwcomp = pb->n_w_completion;
+    for (int d = 0; d < 4; ++d) {
+        const int nnz = pb->op_rowptr[d][N];
+        int32_t* rp;
+        int32_t* ci = nullptr;
+        double* v = nullptr;
+        if ((rc = s->alloc(&rp, N + 1, pb->op_rowptr[d])) || (rc = s->alloc(&ci, nnz, pb->op_col[d])) ||
+            (rc = s->alloc(&v, nnz, pb->op_val[d])))
+            return cleanup(rc);
+        P.op[d].rowptr = rp;
+        P.op[d].col = ci;
+        P.op[d].val = v;
+    }
+    // team state (one team); partial buffer sized for the largest team
+    s->team_ctas = std::min(s->num_sms, 32);
+    TeamState& st = s->st;
+    const size_t nK = (size_t)n * KM, NK = (size_t)N * KM;
+    unsigned* bar;
+    int* info;
+    if ((rc = s->alloc(&st.X, nK)) || (rc = s->alloc(&st.K, nK)) || (rc = s->alloc(&st.W, NK)) ||
+        (rc = s->alloc(&st.L, 2 * NK)) || (rc = s->alloc(&st.psi0, (size_t)n * QM)) ||
+        (rc = s->alloc(&st.psi1, (size_t)n * QM)) || (rc = s->alloc(&st.dose, n)) ||
+        (rc = s->alloc(&st.S, KK)) || (rc = s->alloc(&st.part, (size_t)s->num_sms * PMAX)) ||
+        (rc = s->alloc(&bar, 2)) || (rc = s->alloc(&st.status, 1)) || (rc = s->alloc(&info, 4)) ||
+        (rc = s->alloc(&st.rank_hist, nE)))
+        return cleanup(rc);
+    st.bar = bar;
+    st.info = info;
+    st.eta_hist = st.bound_hist = st.time_hist = nullptr;
+    if ((rc = s->alloc(&s->d_st, 1))) return cleanup(rc);
+    CK(cudaMemcpy(s->d_st, &st, sizeof(TeamState), cudaMemcpyHostToDevice));
+    CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(SmemLayout)));
+    *out = s;
+    return TITUS_OK;
+}
+
+// Initial factors of SolverCSD.jl:931-955: X = first r identity columns with
+// boundary rows zeroed, W = first r identity columns, S = 0; psi = 0, dose = 0.
+static int init_state(titus_solver* s, int r, cudaStream_t stream) {
+    const int n = s->n, N = s->N;
+    TeamState& st = s->st;
+    std::vector<double> X((size_t)n * KM, 0.0), W((size_t)N * KM, 0.0);
+    const int nx = s->P.nx, ny = s->P.ny;
+    for (int j = 0; j < r && j < n; ++j) {
+        int i = j / ny, jj = j % ny;
+        bool bnd = (i == 0 || jj == 0 || i == nx - 1 || jj == ny - 1);
+        X[(size_t)j * KM + j] = bnd ? 0.0 : 1.0;
+    }
+    for (int j = 0; j < r && j < N; ++j) W[(size_t)j * KM + j] = 1.0;
+    CK(cudaMemcpyAsync(st.X, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(st.W, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(st.S, 0, KK * sizeof(double), stream));
+    CK(cudaMemsetAsync(st.psi0, 0, (size_t)n * QM * sizeof(double), stream));
+    CK(cudaMemsetAsync(st.psi1, 0, (size_t)n * QM * sizeof(double), stream));
+    CK(cudaMemsetAsync(st.dose, 0, (size_t)n * sizeof(double), stream));
+    int info[4] = {r, 0, 0, 2};
+    CK(cudaMemcpyAsync(st.info, info, sizeof(info), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(st.rank_hist, 0xff, s->nE * sizeof(int), stream));
+    CK(cudaStreamSynchronize(stream));
+    return TITUS_OK;
+}
+
+static int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin, int n_end, int dose2_pending,
+                  cudaStream_t stream) {
+    if (method != TITUS_DLR_FIXED)
+        return fail(TITUS_ERR_ARG, "method %d is not available in this build (fixed-rank only)", method);
+    int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : s->team_ctas;
+    G = std::min(G, s->num_sms);
+    G = std::max(G, 1);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dlr_kernel<TITUS_DLR_FIXED>, NT, sizeof(SmemLayout)));
+    if (per_sm < 1) return fail(TITUS_ERR_CUDA, "kernel does not fit on an SM (smem %zu)", sizeof(SmemLayout));
+    if (G > per_sm * s->num_sms) G = per_sm * s->num_sms;
+    DevProblem P = s->P;
+    if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
+    CK(cudaMemsetAsync(s->st.bar, 0, 2 * sizeof(unsigned), stream));
+    CK(cudaMemsetAsync(s->st.status, 0, sizeof(int), stream));
+    TeamState* dst = s->d_st;
+    void* args[] = {&P, &dst, &G, &n_begin, &n_end, &dose2_pending};
+    CK(cudaLaunchCooperativeKernel((void*)dlr_kernel<TITUS_DLR_FIXED>, dim3(G), dim3(NT), args, sizeof(SmemLayout),
+                                   stream));
+    s->last_method = method;
+    return TITUS_OK;
+}
+
+static int check_status(titus_solver* s, cudaStream_t stream) {
+    CK(cudaStreamSynchronize(stream));
+    int status = 0;
+    CK(cudaMemcpy(&status, s->st.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) {
+        const char* what = status == ST_BARRIER_TIMEOUT ? "team barrier timeout"
+                           : status == ST_CHOL_BREAKDOWN ? "Cholesky breakdown in the range finder"
+                           : status == ST_COMPLETION      ? "basis completion ran out of candidates"
+                                                          : "device error";
+        return fail(TITUS_ERR_DEVICE, "device status %d: %s", status, what);
+    }
+    return TITUS_OK;
+}
+
+static int end_index(const titus_solver* s, const titus_options_t* opt, int n_begin) {
+    int n_end = s->nE;
+    if (opt && opt->max_steps > 0) n_end = std::min(n_end, n_begin + opt->max_steps - 1);
+    return n_end;
+}
+
+extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus_options_t* opt, void* stream_) {
+    if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    int rc = init_state(s, s->r, stream);
+    if (rc) return rc;
+    return launch(s, method, opt, 2, end_index(s, opt, 2), 0, stream);
+}
+
+extern "C" int titus_fetch(titus_solver_t* s, titus_result_t* res) {
+    if (!s || !res) return fail(TITUS_ERR_ARG, "NULL argument");
+    int rc = check_status(s, 0);
+    if (rc) return rc;
+    int info[4];
+    CK(cudaMemcpy(info, s->st.info, sizeof(info), cudaMemcpyDeviceToHost));
+    const int k = info[0];
+    res->rank = k;
+    res->steps_done = info[1];
+    if (res->dose) CK(cudaMemcpy(res->dose, s->st.dose, s->n * sizeof(double), cudaMemcpyDeviceToHost));
+    const int rc_cap = res->r_cap;
+    if ((res->X || res->S || res->W) && rc_cap < k) return fail(TITUS_ERR_ARG, "r_cap %d < rank %d", rc_cap, k);
+    if (res->X)
+        CK(cudaMemcpy2D(res->X, rc_cap * sizeof(double), s->st.X, KM * sizeof(double), k * sizeof(double), s->n,
+                        cudaMemcpyDeviceToHost));
+    if (res->W)
+        CK(cudaMemcpy2D(res->W, rc_cap * sizeof(double), s->st.W, KM * sizeof(double), k * sizeof(double), s->N,
+                        cudaMemcpyDeviceToHost));
+    if (res->S)
+        CK(cudaMemcpy2D(res->S, rc_cap * sizeof(double), s->st.S, KM * sizeof(double), k * sizeof(double), k,
+                        cudaMemcpyDeviceToHost));
+    if (res->psi) {
+        double* src = info[2] ? s->st.psi1 : s->st.psi0;
+        CK(cudaMemcpy2D(res->psi, s->q * sizeof(double), src, QM * sizeof(double), s->q * sizeof(double), s->n,
+                        cudaMemcpyDeviceToHost));
+    }
+    if (res->rank_history) CK(cudaMemcpy(res->rank_history, s->st.rank_hist, s->nE * sizeof(int), cudaMemcpyDeviceToHost));
+    if (res->eta_history) memset(res->eta_history, 0, s->nE * sizeof(double));
+    if (res->bound_history) memset(res->bound_history, 0, s->nE * sizeof(double));
+    if (res->time_history) memset(res->time_history, 0, s->nE * sizeof(double));
+    return TITUS_OK;
+}
+
+extern "C" int titus_solve(titus_solver_t* s, int32_t method, const titus_options_t* opt, titus_result_t* res) {
+    int rc = titus_solve_device(s, method, opt, nullptr);
+    if (rc) return rc;
+    return titus_fetch(s, res);
+}
+
+extern "C" int titus_solve_problem(const titus_problem_t* pb, int32_t method, const titus_options_t* opt,
+                                   titus_result_t* res) {
+    titus_solver_t* s = nullptr;
+    int rc = titus_create(pb, &s);
+    if (rc) return rc;
+    rc = titus_solve(s, method, opt, res);
+    titus_destroy(s);
+    return rc;
+}
+
+extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X, const double* S, const double* W,
+                               const double* psi, const double* dose, int32_t n_next) {
+    if (!s || !X || !S || !W || !psi || !dose) return fail(TITUS_ERR_ARG, "NULL argument");
+    if (rank < 1 || rank > KM) return fail(TITUS_ERR_LIMIT, "rank %d outside [1, %d]", rank, KM);
+    if (n_next < 2 || n_next > s->nE + 1) return fail(TITUS_ERR_ARG, "n_next %d outside [2, nE+1]", n_next);
+    TeamState& st = s->st;
+    CK(cudaMemset(st.X, 0, (size_t)s->n * KM * sizeof(double)));
+    CK(cudaMemset(st.W, 0, (size_t)s->N * KM * sizeof(double)));
+    CK(cudaMemset(st.S, 0, KK * sizeof(double)));
+    CK(cudaMemcpy2D(st.X, KM * sizeof(double), X, rank * sizeof(double), rank * sizeof(double), s->n,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemcpy2D(st.W, KM * sizeof(double), W, rank * sizeof(double), rank * sizeof(double), s->N,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemcpy2D(st.S, KM * sizeof(double), S, rank * sizeof(double), rank * sizeof(double), rank,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemset(st.psi0, 0, (size_t)s->n * QM * sizeof(double)));
+    CK(cudaMemcpy2D(st.psi0, QM * sizeof(double), psi, s->q * sizeof(double), s->q * sizeof(double), s->n,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(st.dose, dose, s->n * sizeof(double), cudaMemcpyHostToDevice));
+    int info[4] = {rank, 0, 0, n_next};
+    CK(cudaMemcpy(st.info, info, sizeof(info), cudaMemcpyHostToDevice));
+    CK(cudaMemset(st.rank_hist, 0xff, s->nE * sizeof(int)));
+    return TITUS_OK;
+}
+
+extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t n_stop,
+                                titus_result_t* res) {
+    if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    int info[4];
+    CK(cudaMemcpy(info, s->st.info, sizeof(info), cudaMemcpyDeviceToHost));
+    const int n_begin = info[3];
+    int n_end = std::min(n_stop, end_index(s, opt, n_begin));
+    if (n_end < n_begin) return fail(TITUS_ERR_ARG, "nothing to run (n_begin %d, n_stop %d)", n_begin, n_stop);
+    // The state handed over by titus_set_state is taken after the second dose
+    // half-step of step n_begin-1, so no dose half-step is pending.
+    int rc = launch(s, method, opt, n_begin, n_end, 0, nullptr);
+    if (rc) return rc;
+    return titus_fetch(s, res);
+}
+
+extern "C" void titus_destroy(titus_solver_t* s) { delete s; }
+
+extern "C" int titus_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return TITUS_ERR_ARG;
+    snprintf(buf, len, "%s", g_last_error.c_str());
+    return TITUS_OK;
+}
+
+extern "C" int titus_max_rank(void) { return KM; }
+extern "C" int titus_max_ordinates(void) { return QM; }
+extern "C" const char* titus_version(void) { return "titus-b200 0.1 (sm_100a, FP64)"; }

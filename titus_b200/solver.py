@@ -1,0 +1,215 @@
+"""``SolverCSD`` and the ``Solve*`` entry points, running on the B200 through libtitus.
+
+Mirrors the reference API (``code/SolverCSD.jl``):
+
+* ``SolverCSD(settings)`` -- builds the solver data (``:63-146``) on the host
+  and uploads it to the device once (``titus_create``);
+* ``SolveFirstCollisionSourceDLR(solver)`` -- fixed-rank integrator
+  (``:891-1120``), returns ``(X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, psi)``.
+
+The energy loop itself always runs on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from . import physics as ph
+
+
+class SolverCSD:
+    def __init__(self, settings, team_ctas: int = 0):
+        s = settings
+        self.settings = s
+        self.team_ctas = team_ctas
+        nx, ny = s.NCellsX, s.NCellsY
+        self.n = nx * ny
+        npn = s.nPN
+        self.N = (npn + 1) ** 2
+        self.gamma = np.array([2.0 / (2 * l + 1) for l in range(npn + 1)])
+        Ax, Az = ph.flux_matrices(npn)
+        self.ops = [ph.to_csr(A) for A in (Ax, Az, ph.roe(Ax), ph.roe(Az))]
+        q = npn + 1
+        self.Q_points, self.Q_weights, self.O, self.M = ph.quadrature(q, npn)
+        self.eGrid, self.eTrafo, self.S = ph.energy_grid(s)
+        self.nE = self.eTrafo.size
+        # separable PsiBeam (SolverCSD.jl:275): angular x spatial x energy factors
+        ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - self.Q_points[:, 0]) ** 2) * \
+            np.exp(-s.sigmaO3Inv * (s.Omega3 - self.Q_points[:, 2]) ** 2)
+        scale = s.psi_scale / ang.max() if s.beam_peak_normalized else s.psi_scale
+        # direction reduction, SolverCSD.jl:912-925 (PsiBeam at eMax, x0, y0, n=1)
+        e0 = scale * math.exp(-s.sigmaEInv * (s.eMax - s.eMax) ** 2) * self.S[0] * s.densityMin
+        beam = ang * e0 * math.exp(-s.sigmaXInv * (s.x0 - s.x0) ** 2) * math.exp(-s.sigmaYInv * (s.y0 - s.y0) ** 2)
+        self.idxBeam = np.nonzero(beam > 1e-17 * beam.max())[0]
+        self.qReduced = self.Q_points[self.idxBeam]
+        self.MReduced = np.ascontiguousarray(self.M[:, self.idxBeam])
+        self.OReduced = self.O[self.idxBeam]
+        self.q = self.idxBeam.size
+        self.bc_angle = np.ascontiguousarray(ang[self.idxBeam])
+        self.bc_energy = scale * np.exp(-s.sigmaEInv * (s.eMax - self.eGrid) ** 2) * self.S * s.densityMin
+        xm = s.xMid[np.arange(self.n) // ny]
+        ym = s.yMid[np.arange(self.n) % ny]
+        self.bc_space = np.exp(-s.sigmaXInv * (xm - s.x0) ** 2) * np.exp(-s.sigmaYInv * (ym - s.y0) ** 2)
+        sig = np.array([s.sigmaT_hg * s.hg_g**l for l in range(npn + 1)])
+        self.sigma = np.ascontiguousarray(np.tile(sig, (self.nE, 1)))
+        self.density = np.ascontiguousarray(s.density.reshape(self.n), dtype=np.float64)
+        # boundary cells in the reference's order (SolverCSD.jl:108-131)
+        bidx = []
+        for i in range(nx):
+            bidx += [i * ny, i * ny + ny - 1]
+        for j in range(ny):
+            bidx += [j, (nx - 1) * ny + j]
+        self.boundaryIdx = np.array(bidx, dtype=np.int64)
+        # psi[boundaryIdx] linear-indexes the column-major (nx, ny, q) array:
+        # ordinate-0 value of cell (L % nx, L // nx) survives the sweep
+        Lb = self.boundaryIdx
+        self.sweep_restore = np.unique((Lb % nx) * ny + Lb // nx).astype(np.int32)
+        # completion candidates for rank-deficient bases: canonical vectors in
+        # index order (LAPACK's identity columns for a zero input); spatial
+        # candidates are boundary cells, whose rows are zero in every K
+        self.x_completion = np.unique(self.boundaryIdx).astype(np.int32)
+        self.w_completion = np.arange(self.N, dtype=np.int32)
+        self.dose = np.zeros(self.n)
+        self._handle = None
+        self._keep = None
+
+    # -------------------------------------------------------------- device
+    def problem_struct(self):
+        s = self.settings
+        p = _lib.Problem()
+        keep = []
+
+        def dp(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return _lib.as_dp(a)
+
+        def ip(a):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            keep.append(a)
+            return _lib.as_ip(a)
+
+        p.nx, p.ny, p.npn, p.n_moments = s.NCellsX, s.NCellsY, s.nPN, self.N
+        p.n_ordinates, p.n_energies, p.r = self.q, self.nE, s.r
+        p.dx, p.dy = s.dx, s.dy
+        p.theta, p.theta_index, p.c_eta = s.theta, s.thetaIndex, s.c_eta
+        p.density = dp(self.density)
+        p.e_trafo = dp(self.eTrafo)
+        p.stopping = dp(self.S)
+        p.bc_energy = dp(self.bc_energy)
+        p.sigma = dp(self.sigma)
+        p.bc_space = dp(self.bc_space)
+        p.bc_angle = dp(self.bc_angle)
+        p.omega = dp(self.qReduced)
+        p.m_reduced = dp(self.MReduced)
+        for d, (rp, ci, v) in enumerate(self.ops):
+            p.op_rowptr[d] = ip(rp)
+            p.op_col[d] = ip(ci)
+            p.op_val[d] = dp(v)
+        p.x_completion = ip(self.x_completion)
+        p.n_x_completion = self.x_completion.size
+        p.w_completion = ip(self.w_completion)
+        p.n_w_completion = self.w_completion.size
+        p.sweep_restore = ip(self.sweep_restore)
+        p.n_sweep_restore = self.sweep_restore.size
+        return p, keep
+
+    def handle(self):
+        if self._handle is None:
+            lib = _lib.load()
+            p, keep = self.problem_struct()
+            h = C.c_void_p()
+            _lib.check(lib.titus_create(C.byref(p), C.byref(h)), "titus_create")
+            self._handle = h
+        return self._handle
+
+    def close(self):
+        if self._handle is not None:
+            _lib.load().titus_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def options(self, max_steps=0, rank_tol=0.0):
+        o = _lib.Options()
+        o.team_ctas = self.team_ctas
+        o.max_steps = max_steps
+        o.rank_tol = rank_tol
+        return o
+
+    def _result(self, r_cap):
+        res = _lib.Result()
+        bufs = dict(
+            dose=np.zeros(self.n), X=np.zeros((self.n, r_cap)), S=np.zeros((r_cap, r_cap)),
+            W=np.zeros((self.N, r_cap)), psi=np.zeros((self.n, self.q)),
+            rank_history=np.zeros(self.nE, dtype=np.int32),
+        )
+        res.dose = _lib.as_dp(bufs["dose"])
+        res.X = _lib.as_dp(bufs["X"])
+        res.S = _lib.as_dp(bufs["S"])
+        res.W = _lib.as_dp(bufs["W"])
+        res.psi = _lib.as_dp(bufs["psi"])
+        res.rank_history = _lib.as_ip(bufs["rank_history"])
+        res.r_cap = r_cap
+        return res, bufs
+
+    def run(self, method: int, max_steps: int = 0, rank_tol: float = 0.0):
+        """Run one integrator on the device; returns raw factors and histories."""
+        lib = _lib.load()
+        h = self.handle()
+        r_cap = max(self.settings.r, 1)
+        res, bufs = self._result(r_cap)
+        opt = self.options(max_steps, rank_tol)
+        _lib.check(lib.titus_solve(h, method, C.byref(opt), C.byref(res)), "titus_solve")
+        k = res.rank
+        return dict(X=bufs["X"][:, :k], S=bufs["S"][:k, :k], W=bufs["W"][:, :k], dose=bufs["dose"],
+                    psi=bufs["psi"], rank=k, steps=res.steps_done, rank_history=bufs["rank_history"])
+
+    def run_from(self, method: int, state: dict, n_next: int, n_stop: int, rank_tol: float = 0.0):
+        """Resume the loop from a given state (checkpoint restart)."""
+        lib = _lib.load()
+        h = self.handle()
+        X = np.ascontiguousarray(state["X"], dtype=np.float64)
+        S = np.ascontiguousarray(state["S"], dtype=np.float64)
+        W = np.ascontiguousarray(state["W"], dtype=np.float64)
+        psi = np.ascontiguousarray(state["psi"], dtype=np.float64).reshape(self.n, self.q)
+        dose = np.ascontiguousarray(state["dose"], dtype=np.float64)
+        k = S.shape[0]
+        _lib.check(lib.titus_set_state(h, k, _lib.as_dp(X), _lib.as_dp(S), _lib.as_dp(W), _lib.as_dp(psi),
+                                       _lib.as_dp(dose), n_next), "titus_set_state")
+        r_cap = max(self.settings.r, k)
+        res, bufs = self._result(r_cap)
+        opt = self.options(0, rank_tol)
+        _lib.check(lib.titus_solve_from(h, method, C.byref(opt), n_stop, C.byref(res)), "titus_solve_from")
+        kk = res.rank
+        return dict(X=bufs["X"][:, :kk], S=bufs["S"][:kk, :kk], W=bufs["W"][:, :kk], dose=bufs["dose"],
+                    psi=bufs["psi"], rank=kk, steps=res.steps_done)
+
+    def outputs(self, out):
+        """The reference's return tuple from raw factors (``SolverCSD.jl:1116-1118``)."""
+        U, sig, Vt = np.linalg.svd(out["S"])
+        V = Vt.T
+        X, W = out["X"], out["W"]
+        nx, ny = self.settings.NCellsX, self.settings.NCellsY
+        psi = out["psi"].reshape(nx, ny, self.q)
+        return X @ U, 0.5 * math.sqrt(self.gamma[0]) * sig, self.O @ (W @ V), W @ V, out["dose"], psi
+
+
+def SolveFirstCollisionSourceDLR(solver: SolverCSD, max_steps: int = 0):
+    """Fixed-rank DLR (``SolverCSD.jl:891-1120``) on the GPU."""
+    out = solver.run(_lib.TITUS_DLR_FIXED, max_steps=max_steps)
+    res = solver.outputs(out)
+    solver.dose = res[4]
+    return res
+
+
+def scalar_flux(X, sigma, WV):
+    """``u = X diag(Sigma) W_mod[1,:]`` (``main.jl:73``), cell order i*ny + j."""
+    return X @ (sigma * WV[0, :])
