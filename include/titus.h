@@ -75,6 +75,7 @@ typedef struct titus_options {
     int32_t team_ctas;     /* CTAs cooperating on one solve (0 = library default) */
     int32_t max_steps;     /* stop after this many loop iterations (0 = full sweep) */
     double rank_tol;       /* relative singular-value cut for numerical rank (0 = 1e-12) */
+    int32_t profile;       /* 1 = record per-phase device timers (read with titus_profile) */
 } titus_options_t;
 
 /* Host result buffers (caller-owned). Factors are returned raw: X (n x r_cap),
@@ -130,6 +131,13 @@ void titus_destroy(titus_solver_t* solver);
 
 /* Copy the last error message of this thread into buf (always terminated). */
 int titus_last_error(char* buf, size_t len);
+
+/* Per-phase device timers of the last profiled solve (options.profile = 1),
+ * in nanoseconds at the nominal SM clock, recorded on the first CTA:
+ * [0] barrier waits, [1] reductions, [2] Jacobi eigensolves, [3] Cholesky,
+ * [4] basis completion, [5] (unused), [6] (unused), [7] range-finder passes,
+ * [8] (unused), [9] kernel total. Returns the number of entries written. */
+int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
 
 /* Build / capability queries. */
 int titus_max_rank(void);        /* largest basis width (columns) supported */

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libtitus.so")
 TITUS_DLR_FIXED = 0
 TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
+PROFILE_NAMES = ["barrier", "reduce", "jacobi", "cholesky", "completion", "-", "-", "rf_passes", "-", "total"]
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -38,7 +39,8 @@ class Problem(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("team_ctas", C.c_int32), ("max_steps", C.c_int32), ("rank_tol", C.c_double)]
+    _fields_ = [("team_ctas", C.c_int32), ("max_steps", C.c_int32), ("rank_tol", C.c_double),
+                ("profile", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -60,6 +62,7 @@ SIGNATURES = [
     ("titus_solve_from", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_int32, C.POINTER(Result)]),
     ("titus_destroy", None, [C.c_void_p]),
     ("titus_last_error", C.c_int, [C.c_char_p, C.c_size_t]),
+    ("titus_profile", C.c_int, [C.c_void_p, _dp, C.c_int32]),
     ("titus_max_rank", C.c_int, []),
     ("titus_max_ordinates", C.c_int, []),
     ("titus_version", C.c_char_p, []),

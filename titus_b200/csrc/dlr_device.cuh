@@ -15,7 +15,7 @@ namespace titus {
 constexpr int NT = 256;        // threads per CTA
 constexpr int KM = 24;         // max basis width handled by this build
 constexpr int QM = 32;         // max reduced ordinates
-constexpr int TR = 16;         // rows per staged tile
+constexpr int TR = 32;         // rows per staged tile
 constexpr int NOPS = 4;        // Ax, Az, |Ax|, |Az|
 constexpr int KK = KM * KM;
 constexpr int PMAX = 8 * KK;  // partial-reduction capacity (doubles); >= 2KK + 2 KM QM
@@ -51,6 +51,24 @@ struct DevProblem {
     const int32_t* xcomp; int nxcomp;
     const int32_t* wcomp; int nwcomp;
     const uint8_t* restore;   // n: 1 if ordinate-0 value is restored after the sweep
+    unsigned long long* prof; // optional phase timers (SM cycles), recorded by CTA 0 of team 0
+    int zero_smem;            // 1: clear the dynamic shared memory at kernel start
+};
+
+// Phase-timer categories (titus_profile reports them in this order).
+enum ProfCat { PF_BARRIER = 0, PF_REDUCE, PF_JACOBI, PF_CHOL, PF_COMPLETE, PF_ROWS_STREAM, PF_ROWS_SCATTER,
+               PF_RF_PASSES, PF_SMALL, PF_TOTAL, PF_COUNT };
+
+struct ProfScope {
+    unsigned long long* p;
+    int cat;
+    long long t0;
+    __device__ ProfScope(unsigned long long* p_, int c) : p(p_), cat(c), t0(0) {
+        if (p && threadIdx.x == 0) t0 = clock64();
+    }
+    __device__ ~ProfScope() {
+        if (p && threadIdx.x == 0) p[cat] += (unsigned long long)(clock64() - t0);
+    }
 };
 
 // Per-team device state.
@@ -63,10 +81,12 @@ struct TeamState {
     double* psi1;   // n x QM
     double* dose;   // n
     double* S;      // KM x KM (final S written back)
-    double* part;   // G x PMAX partial reductions
-    unsigned* bar;  // [0] = arrive count, [1] = generation
+    double* part;   // 2 x G x PMAX partial reductions (double-buffered)
+    double* red;    // PMAX: second-stage reduced entries (large teams)
+    unsigned* bar;  // [0, G): arrival generation per CTA; [G]: release generation
     int* status;    // device error flag
     int* info;      // [0]=rank, [1]=steps done, [2]=psi buffer index, [3]=next n
+    double* diag;   // 16: breakdown diagnostics (see record_breakdown)
     int* rank_hist; // nE
     double* eta_hist;
     double* bound_hist;
@@ -81,30 +101,61 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
-// Team barrier: arrive counter + generation, bounded spin. Returns false if the
-// team's status flag is set (by this or another CTA, e.g. after a timeout).
-__device__ bool team_sync(unsigned* bar, int* status, int G) {
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Team barrier without atomics: CTA b publishes its arrival generation in
+// flags[b]; CTA 0 polls all arrival flags (one thread per CTA) and then
+// publishes the release generation in flags[G]; the others poll that. Every
+// spin is bounded (about a second); on expiry the status flag is set and all
+// CTAs leave. Returns false if the team's status flag is set.
+__device__ bool team_sync(unsigned* flags, int* status, int G, int b, unsigned& gen, double* diag = nullptr) {
     __shared__ int s_ok;
+    constexpr long long kSpinLimit = 1ll << 21;
     __syncthreads();
+    ++gen;
     if (threadIdx.x == 0) {
-        unsigned gen = ld_acquire(bar + 1);
         __threadfence();
-        unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == (unsigned)(G - 1)) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
+        st_release(flags + b, gen);
+    }
+    if (b == 0) {
+        for (int t = threadIdx.x; t < G; t += NT) {
             long long it = 0;
-            while (ld_acquire(bar + 1) == gen) {
-                if (++it > (1ll << 24)) {  // ~1-2 s with the sleep below
-                    atomicExch(status, ST_BARRIER_TIMEOUT);
+            while (ld_acquire(flags + t) != gen) {
+                if (++it > kSpinLimit) {
+                    if (atomicCAS(status, 0, ST_BARRIER_TIMEOUT) == 0 && diag) {
+                        diag[8] = t;
+                        diag[9] = ld_acquire(flags + t);
+                        diag[10] = gen;
+                    }
                     break;
                 }
-                if (it > 64) __nanosleep(100);
-                if ((it & 1023) == 0 && ldcg(status) != 0) break;
+                if (it > 32) __nanosleep(200);
+                if ((it & 255) == 0 && ldcg(status) != 0) break;
             }
         }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release(flags + G, gen);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire(flags + G) != gen) {
+            if (++it > kSpinLimit) {
+                if (atomicCAS(status, 0, ST_BARRIER_TIMEOUT) == 0 && diag) {
+                    diag[8] = 1000 + b;
+                    diag[9] = ld_acquire(flags + G);
+                    diag[10] = gen;
+                }
+                break;
+            }
+            if (it > 32) __nanosleep(200);
+            if ((it & 255) == 0 && ldcg(status) != 0) break;
+        }
+    }
+    if (threadIdx.x == 0) {
         __threadfence();
         s_ok = (ldcg(status) == 0);
     }
@@ -179,7 +230,7 @@ __device__ __forceinline__ bool rr_pair(int m, int t, int s, int k, int& p, int&
 __device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* status) {
     __shared__ double rc[KM / 2 + 1], rs[KM / 2 + 1];
     __shared__ int rp[KM / 2 + 1], rq[KM / 2 + 1];
-    __shared__ int s_rot;
+    __shared__ int s_rot[2];  // per-sweep-parity flag: a reset never races a late reader
     __shared__ double s_lam[KM];
     __shared__ int s_perm[KM];
     for (int e = threadIdx.x; e < k * k; e += NT) V[(e / k) * KM + e % k] = ((e / k) == (e % k)) ? 1.0 : 0.0;
@@ -193,7 +244,8 @@ __device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* statu
     const int npairs = m / 2;
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
-        if (threadIdx.x == 0) s_rot = 0;
+        const int par = sweep & 1;
+        if (threadIdx.x == 0) s_rot[par] = 0;
         __syncthreads();
         for (int t = 0; t < m - 1; ++t) {
             if (threadIdx.x < npairs) {
@@ -210,7 +262,7 @@ __device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* statu
                         else t_ = copysign(1.0, theta) / (fabs(theta) + sqrt(theta * theta + 1.0));
                         c = 1.0 / sqrt(t_ * t_ + 1.0);
                         s = t_ * c;
-                        s_rot = 1;
+                        s_rot[par] = 1;
                     }
                 } else {
                     p = q = -1;
@@ -249,7 +301,7 @@ __device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* statu
             }
             __syncthreads();
         }
-        if (!s_rot) break;
+        if (!s_rot[par]) break;
     }
     (void)status;
     // sort descending (stable): rank of each eigenvalue
@@ -276,50 +328,145 @@ __device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* statu
     __syncthreads();
 }
 
-// Upper Cholesky R^T R = G (k x k), then Ri = R^{-1} (upper). G in smem (read),
-// R and Ri written (may alias nothing). Sets status on breakdown.
-__device__ void chol_inv(const double* G, double* R, double* Ri, int k, int* status) {
-    for (int e = threadIdx.x; e < k * k; e += NT) R[(e / k) * KM + e % k] = G[(e / k) * KM + e % k];
-    __syncthreads();
-    __shared__ double s_piv;
-    for (int j = 0; j < k; ++j) {
-        if (threadIdx.x == 0) {
-            double d = R[j * KM + j];
+// Upper Cholesky R^T R = G (k x k, k <= KM <= 32) and Ri = R^{-1} by ONE warp:
+// lane c keeps column c of R and of R^{-1} in registers (fully unrolled loops,
+// so all register indices are static), row entries travel by shuffles.
+// Returns ||R||_F ||R^{-1}||_F, or +inf on breakdown (non-positive pivot).
+__device__ double warp_chol_inv(const double* G, double* R, double* Ri, int k, int* bad_j = nullptr,
+                                double* bad_d = nullptr) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    double col[KM];
+    int first_bad = -1;
+    double first_d = 0.0;
+#pragma unroll
+    for (int a = 0; a < KM; ++a) col[a] = (lane < k && a < k && a <= lane) ? G[a * KM + lane] : 0.0;
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < KM; ++j) {
+        if (j < k) {
+            double d = __shfl_sync(FULL, col[j], j);
             if (!(d > 0.0)) {
-                set_status(status, ST_CHOL_BREAKDOWN);
+                if (ok) {
+                    first_bad = j;
+                    first_d = d;
+                }
+                ok = false;
                 d = 1.0;
             }
-            s_piv = sqrt(d);
-            R[j * KM + j] = s_piv;
-        }
-        __syncthreads();
-        for (int c = j + 1 + threadIdx.x; c < k; c += NT) R[j * KM + c] /= s_piv;
-        __syncthreads();
-        // trailing update on the upper triangle: R[a][b] -= R[j][a] R[j][b], a<=b
-        int m = k - j - 1;
-        for (int e = threadIdx.x; e < m * m; e += NT) {
-            int a = j + 1 + e / m, b = j + 1 + e % m;
-            if (b >= a) R[a * KM + b] -= R[j * KM + a] * R[j * KM + b];
-        }
-        __syncthreads();
-    }
-    for (int e = threadIdx.x; e < k * k; e += NT) {
-        int a = e / k, b = e % k;
-        if (b < a) R[a * KM + b] = 0.0;
-    }
-    __syncthreads();
-    // inverse of upper triangular R, column by column: Ri[:, c] solves R x = e_c
-    for (int c = threadIdx.x; c < k; c += NT) {
-        for (int a = k - 1; a >= 0; --a) {
-            double s = (a == c) ? 1.0 : 0.0;
-            if (a > c) s = 0.0;
-            else {
-                for (int b = a + 1; b <= c; ++b) s -= R[a * KM + b] * Ri[b * KM + c];
+            const double piv = sqrt(d);
+            const double ip = 1.0 / piv;
+            if (lane == j) col[j] = piv;
+            else if (lane > j) col[j] *= ip;
+#pragma unroll
+            for (int a = j + 1; a < KM; ++a) {
+                if (a < k) {
+                    const double rja = __shfl_sync(FULL, col[j], a);
+                    if (lane >= a) col[a] = fma(-rja, col[j], col[a]);
+                }
             }
-            Ri[a * KM + c] = (a > c) ? 0.0 : s / R[a * KM + a];
+        }
+    }
+    // R to shared memory (column lane), then R^{-1} column lane by back substitution
+    if (lane < k) {
+#pragma unroll
+        for (int a = 0; a < KM; ++a)
+            if (a < k) R[a * KM + lane] = (a <= lane) ? col[a] : 0.0;
+    }
+    __syncwarp();
+    double inv[KM];
+    double nr = 0.0, ni = 0.0;
+#pragma unroll
+    for (int a = KM - 1; a >= 0; --a) {
+        double v = 0.0;
+        if (a < k && lane < k && a <= lane) {
+            double t = (a == lane) ? 1.0 : 0.0;
+#pragma unroll
+            for (int b = a + 1; b < KM; ++b)
+                if (b <= lane && b < k) t = fma(-R[a * KM + b], inv[b], t);
+            v = t / R[a * KM + a];
+        }
+        inv[a] = v;
+    }
+    if (lane < k) {
+#pragma unroll
+        for (int a = 0; a < KM; ++a)
+            if (a < k) {
+                Ri[a * KM + lane] = inv[a];
+                nr = fma(col[a], col[a], nr);
+                ni = fma(inv[a], inv[a], ni);
+            }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        nr += __shfl_xor_sync(FULL, nr, o);
+        ni += __shfl_xor_sync(FULL, ni, o);
+    }
+    ok = __all_sync(FULL, ok);
+    if (bad_j) *bad_j = first_bad;
+    if (bad_d) *bad_d = first_d;
+    return ok ? sqrt(nr) * sqrt(ni) : INFINITY;
+}
+
+// Two independent Cholesky factorisations on warps 0 and 1 concurrently
+// (either may be skipped). Writes the condition estimates; sets the status
+// flag on breakdown when `flag` is set.
+// On breakdown with `flag`, the first CTA to fail records in diag:
+// [0] stage tag, [1] side (0 = X, 1 = W), [2] k, [3] first bad pivot index,
+// [4] its value, [5] G[0][0], [6] min diagonal of G, [7] energy index.
+__device__ void record_breakdown(double* diag, int* status, int tag, int side, int k, int bj, double bd,
+                                 const double* G, int n) {
+    if (atomicCAS(status, 0, ST_CHOL_BREAKDOWN) == 0 && diag) {
+        double mn = INFINITY;
+        for (int a = 0; a < k; ++a) mn = fmin(mn, G[a * KM + a]);
+        diag[0] = tag;
+        diag[1] = side;
+        diag[2] = k;
+        diag[3] = bj;
+        diag[4] = bd;
+        diag[5] = k > 0 ? G[0] : 0.0;
+        diag[6] = mn;
+        diag[7] = n;
+    }
+}
+
+__device__ void dual_chol(bool dx, const double* GX, double* RX, double* RiX, int kx, double* condX,
+                          bool dw, const double* GW, double* RW, double* RiW, int kw, double* condW,
+                          int* status, bool flag, double* diag = nullptr, int tag = 0, int n = 0) {
+    __shared__ double s_c[2];
+    const int w = threadIdx.x >> 5;
+    if (w == 0 && dx) {
+        int bj;
+        double bd;
+        double c = warp_chol_inv(GX, RX, RiX, kx, &bj, &bd);
+        if ((threadIdx.x & 31) == 0) {
+            s_c[0] = c;
+            if (flag && !(c < INFINITY)) record_breakdown(diag, status, tag, 0, kx, bj, bd, GX, n);
+        }
+    }
+    if (w == 1 && dw) {
+        int bj;
+        double bd;
+        double c = warp_chol_inv(GW, RW, RiW, kw, &bj, &bd);
+        if ((threadIdx.x & 31) == 0) {
+            s_c[1] = c;
+            if (flag && !(c < INFINITY)) record_breakdown(diag, status, tag, 1, kw, bj, bd, GW, n);
         }
     }
     __syncthreads();
+    if (condX) *condX = dx ? s_c[0] : 0.0;
+    if (condW) *condW = dw ? s_c[1] : 0.0;
+}
+
+// Row-wise triangular solve on a tile: Y[r,:] R = A[r,:] (R upper, k x k), in place.
+__device__ __forceinline__ void tile_rsolve(double* t, const double* R, const double* dinv_unused, int nr, int k) {
+    for (int r = threadIdx.x; r < nr; r += NT) {
+        double* row = t + r * KM;
+        for (int j = 0; j < k; ++j) {
+            double v = row[j];
+            for (int i = 0; i < j; ++i) v = fma(-row[i], R[i * KM + j], v);
+            row[j] = v / R[j * KM + j];
+        }
+    }
 }
 
 }  // namespace titus

@@ -5,6 +5,36 @@
 
 namespace titus {
 
+__device__ __forceinline__ bool tsync(Ctx& x) {
+    ProfScope ps(x.prof, PF_BARRIER);
+    return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag);
+}
+
+// Publish this CTA's partial reduction of `count` entries and synchronise the
+// team. Large teams add a second stage: CTA b sums slice b of the entries over
+// all partials into the team's reduced buffer, then a second barrier; small
+// teams let every CTA sum the partials directly (reduce_into).
+__device__ bool publish_sync(Ctx& x, int count) {
+    acc_publish(x, count);
+    if (!tsync(x)) return false;
+    if (x.G <= kDirectReduceMax) {
+        x.red_mode = 0;
+        return true;
+    }
+    {
+        ProfScope ps(x.prof, PF_REDUCE);
+        const int per = (count + x.G - 1) / x.G;
+        const int e0 = x.b * per, e1 = min(count, e0 + per);
+        for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+            double acc = 0.0;
+            for (int g = 0; g < x.G; ++g) acc += ldcg(part_base(x, g) + e);
+            x.st.red[e] = acc;
+        }
+    }
+    x.red_mode = 1;
+    return tsync(x);
+}
+
 // ---- phase A: (pending) second dose half-step, boundary inflow, first dose
 // half-step, X[bnd,:] = 0.  Own cells only; no reduction.
 __device__ void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc) {
@@ -131,54 +161,109 @@ __device__ void rf_pass_c(Ctx& x, const double* A, double* Cbuf, int r0b, int r1
     }
 }
 
-// Range-finder tail shared by all orthonormalisations of one phase group:
-// after G0 for the X side (off gx) and/or W side (off gw) is published and the
-// team barrier passed, run the two remaining passes. On return slots
-// SL_RIK/SL_RIL hold R^{-1} of the CholQR, CX/CW hold C, x.rhoK/x.rhoL the
-// numerical ranks, and the W completion is prepared.
+// Range-finder pass of the fast path: Y = A R^{-1} by row-wise triangular
+// solves (written to Cbuf), G = Y^T Y.
+// Rows are processed in chunks of kBigRows over the contiguous tile area
+// tA..tO (free during the range finder), one thread per row for the solve.
+__device__ void rf_pass_solve(Ctx& x, const double* A, double* Cbuf, int r0b, int r1b, const double* R, int k, int off) {
+    SmemLayout* sm = x.sm;
+    double* big = sm->tA;
+    for (int r0 = r0b; r0 < r1b; r0 += kBigRows) {
+        int nr = min(kBigRows, r1b - r0);
+        load_rows(big, A, r0, nr, k);
+        __syncthreads();
+        tile_rsolve(big, R, nullptr, nr, k);
+        __syncthreads();
+        store_rows(Cbuf, big, r0, nr, k);
+        gram_acc(sm->acc, off, big, KM, k, big, KM, k, nr);
+        __syncthreads();
+    }
+}
+
+// Orthonormal bases of the numerical ranges of A_X (own cells) and A_W (own
+// moments), after their Grams G0 were published at partial offsets 0 and
+// (doX ? k*k : 0) and the team barrier passed. On return CX/CW hold C and
+// slots SL_RIK/SL_RIL the inverse R of its CholQR, so that the basis is
+// C R^{-1} (rho columns) followed by the completion vectors.
+//  fast path: Cholesky of G0 with ||R||_F ||R^-1||_F < 1e5 certifies full
+//    numerical rank; C = A R0^{-1} (row solves), then CholQR of C.
+//  rank-revealing path: Jacobi eig of G0 -> V; Gram of A V -> Jacobi -> V2,
+//    nu; C = A V V2_J / nu_J with nu_j > tol nu_0; CholQR of C.
 // Returns false if the team aborted.
 __device__ bool range_finder(Ctx& x, const double* AX, const double* AW, bool doX, bool doW, int k) {
     SmemLayout* sm = x.sm;
     const double tol = x.P.rank_tol;
-    // eig of G0 (reduced into ja by the caller's reduce): X side first
-    if (doX) {
+    const double kCert = 1e5;
+    double cX = 0.0, cW = 0.0;
+    if (doX) reduce_into(x, 0, k, k, sm->ja);
+    if (doW) reduce_into(x, doX ? k * k : 0, k, k, sm->jv);
+    {
+        ProfScope ps(x.prof, PF_CHOL);
+        dual_chol(doX, sm->ja, sm->slot[SL_RK], sm->slot[SL_RIK], k, &cX, doW, sm->jv, sm->slot[SL_RL],
+                  sm->slot[SL_RIL], k, &cW, x.st.status, false);
+    }
+    const bool fastX = doX && cX < kCert, fastW = doW && cW < kCert;
+    const bool slowX = doX && !fastX, slowW = doW && !fastW;
+    if (slowX) {
         reduce_into(x, 0, k, k, sm->ja);
         rf_eig0(x, sm->slot[SL_VK], sm->lamK, k);
     }
-    if (doW) {
+    if (slowW) {
         reduce_into(x, doX ? k * k : 0, k, k, sm->ja);
         rf_eig0(x, sm->slot[SL_VL], sm->lamL, k);
     }
-    // pass B
-    acc_zero(x, 2 * k * k);
-    if (doX) rf_pass_b(x, AX, x.c0, x.c1, sm->slot[SL_VK], k, 0);
-    if (doW) rf_pass_b(x, AW, x.m0, x.m1, sm->slot[SL_VL], k, k * k);
-    acc_publish(x, 2 * k * k);
-    if (!team_sync(x.st.bar, x.st.status, x.G)) return false;
-    if (doX) {
+    // first pass
+    {
+        ProfScope ps(x.prof, PF_RF_PASSES);
+        acc_zero(x, 2 * k * k);
+        if (doX) {
+            if (fastX) rf_pass_solve(x, AX, x.CX, x.c0, x.c1, sm->slot[SL_RK], k, 0);
+            else rf_pass_b(x, AX, x.c0, x.c1, sm->slot[SL_VK], k, 0);
+        }
+        if (doW) {
+            if (fastW) rf_pass_solve(x, AW, x.CW, x.m0, x.m1, sm->slot[SL_RL], k, k * k);
+            else rf_pass_b(x, AW, x.m0, x.m1, sm->slot[SL_VL], k, k * k);
+        }
+    }
+    if (!publish_sync(x, 2 * k * k)) return false;
+    if (fastX) reduce_into(x, 0, k, k, sm->ja);
+    if (fastW) reduce_into(x, k * k, k, k, sm->jv);
+    if (fastX || fastW) {
+        ProfScope ps(x.prof, PF_CHOL);
+        dual_chol(fastX, sm->ja, sm->slot[SL_RK], sm->slot[SL_RIK], k, nullptr, fastW, sm->jv, sm->slot[SL_RL],
+                  sm->slot[SL_RIL], k, nullptr, x.st.status, true, x.st.diag, 2, x.cur_n);
+    }
+    if (fastX) x.rhoK = k;
+    if (fastW) x.rhoL = k;
+    if (slowX) {
         reduce_into(x, 0, k, k, sm->ja);
         x.rhoK = rf_eig1(x, sm->slot[SL_VK], sm->slot[SL_TK], k, tol);
     }
-    if (doW) {
+    if (slowW) {
         reduce_into(x, k * k, k, k, sm->ja);
         x.rhoL = rf_eig1(x, sm->slot[SL_VL], sm->slot[SL_TL], k, tol);
     }
-    // pass C
-    acc_zero(x, 2 * k * k);
-    if (doX) rf_pass_c(x, AX, x.CX, x.c0, x.c1, sm->slot[SL_TK], k, x.rhoK, 0);
-    if (doW) rf_pass_c(x, AW, x.CW, x.m0, x.m1, sm->slot[SL_TL], k, x.rhoL, k * k);
-    acc_publish(x, 2 * k * k);
-    if (!team_sync(x.st.bar, x.st.status, x.G)) return false;
-    if (doX) {
-        reduce_into(x, 0, x.rhoK, x.rhoK, sm->ja);
-        chol_inv(sm->ja, sm->slot[SL_RK], sm->slot[SL_RIK], x.rhoK, x.st.status);
-        if (k - x.rhoK > x.P.nxcomp && threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+    if (slowX || slowW) {
+        {
+            ProfScope ps(x.prof, PF_RF_PASSES);
+            acc_zero(x, 2 * k * k);
+            if (slowX) rf_pass_c(x, AX, x.CX, x.c0, x.c1, sm->slot[SL_TK], k, x.rhoK, 0);
+            if (slowW) rf_pass_c(x, AW, x.CW, x.m0, x.m1, sm->slot[SL_TL], k, x.rhoL, k * k);
+        }
+        if (!publish_sync(x, 2 * k * k)) return false;
+        if (slowX) reduce_into(x, 0, x.rhoK, x.rhoK, sm->ja);
+        if (slowW) reduce_into(x, k * k, x.rhoL, x.rhoL, sm->jv);
+        ProfScope ps(x.prof, PF_CHOL);
+        dual_chol(slowX, sm->ja, sm->slot[SL_RK], sm->slot[SL_RIK], x.rhoK, nullptr, slowW, sm->jv,
+                  sm->slot[SL_RL], sm->slot[SL_RIL], x.rhoL, nullptr, x.st.status, true, x.st.diag, 3, x.cur_n);
     }
-    if (doW) {
-        reduce_into(x, k * k, x.rhoL, x.rhoL, sm->ja);
-        chol_inv(sm->ja, sm->slot[SL_RL], sm->slot[SL_RIL], x.rhoL, x.st.status);
-        w_complete(x, x.rhoL, k - x.rhoL);
+    if (x.b == 0 && threadIdx.x == 0 && x.st.diag) {
+        x.st.diag[11] = (doX ? 1 : 0) + (fastX ? 2 : 0) + (doW ? 4 : 0) + (fastW ? 8 : 0);
+        x.st.diag[12] = x.rhoK;
+        x.st.diag[13] = x.rhoL;
     }
+    if (doX && k - x.rhoK > x.P.nxcomp && threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+    if (doW) w_complete(x, x.rhoL, k - x.rhoL);
     __syncthreads();
     return true;
 }
@@ -194,12 +279,24 @@ __global__ void __launch_bounds__(NT, 1)
 dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int dose2_pending_in) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SmemLayout* sm = reinterpret_cast<SmemLayout*>(smem_raw);
+    if (P.zero_smem) {
+        double* z = reinterpret_cast<double*>(smem_raw);
+        for (size_t e = threadIdx.x; e < sizeof(SmemLayout) / sizeof(double); e += NT) z[e] = 0.0;
+        __syncthreads();
+    }
     Ctx x;
     x.P = P;
     x.G = G;
     x.b = blockIdx.x % G;
     x.st = states[blockIdx.x / G];
     x.sm = sm;
+    x.prof = (blockIdx.x == 0) ? P.prof : nullptr;
+    x.red_mode = 0;
+    x.gen = 0;
+    x.parity = 0;
+    x.rhoK = x.rhoL = 0;
+    x.cur_n = 0;
+    ProfScope ps_total(x.prof, PF_TOTAL);
     x.c0 = (int)((long long)x.b * P.n / G);
     x.c1 = (int)((long long)(x.b + 1) * P.n / G);
     x.m0 = (int)((long long)x.b * P.N / G);
@@ -218,20 +315,22 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
         x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
         x.psi_out = psi_idx ? x.st.psi0 : x.st.psi1;
         const double* sig = P.sigma + (size_t)(n - 1) * (P.npn + 1);
+        x.cur_n = n;
         const double dE = P.dE;
         // ---------------- phase A
         phase_bc_dose(x, n, pending, true);
         pending = false;
-        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        if (!tsync(x)) return;
         // ---------------- phase B: sweep + streaming Grams
         sweep_cells(x, sig[0]);
         const bool stream = (n > 2);
         if (stream) {
             acc_zero(x, 8 * k * k);
             stream_grams_partial(x);
-            acc_publish(x, 8 * k * k);
+            if (!publish_sync(x, 8 * k * k)) return;
+        } else if (!tsync(x)) {
+            return;
         }
-        if (!team_sync(x.st.bar, x.st.status, G)) return;
         psi_idx ^= 1;
         x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;  // swept psi
         if (stream) {
@@ -293,8 +392,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
                 gram_acc(sm->acc, k * k, sm->tO, KM, k, sm->tO, KM, k, nr);
                 __syncthreads();
             }
-            acc_publish(x, 2 * k * k);
-            if (!team_sync(x.st.bar, x.st.status, G)) return;
+            if (!publish_sync(x, 2 * k * k)) return;
             // ---------------- phases D, E: range finders of K and L
             if (!range_finder(x, x.st.K, x.st.L, true, true, k)) return;
             // ---------------- phase F: new bases, MUp = XNew^T X, NUp = WNew^T W
@@ -319,8 +417,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
                 store_rows(x.st.W, sm->tO, r0, nr, k);
                 __syncthreads();
             }
-            acc_publish(x, 2 * k * k);
-            if (!team_sync(x.st.bar, x.st.status, G)) return;
+            if (!publish_sync(x, 2 * k * k)) return;
             reduce_into(x, 0, k, k, sm->slot[SL_M]);
             reduce_into(x, k * k, k, k, sm->slot[SL_N]);
             // S1 = MUp S NUp^T -> slot S
@@ -329,8 +426,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
             // ---------------- phase G: S-step Grams with the new X, W
             acc_zero(x, 8 * k * k);
             stream_grams_partial(x);
-            acc_publish(x, 8 * k * k);
-            if (!team_sync(x.st.bar, x.st.status, G)) return;
+            if (!publish_sync(x, 8 * k * k)) return;
             for (int d = 0; d < 4; ++d) {
                 reduce_into(x, d * k * k, k, k, sm->slot[SL_G0 + d]);
                 reduce_into(x, (4 + d) * k * k, k, k, sm->slot[SL_C0 + d]);
@@ -379,8 +475,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
             gram_acc(sm->acc, k * k, sm->tP, QM, P.q, sm->tA, KM, k, nr);
             __syncthreads();
         }
-        acc_publish(x, k * k + P.q * k);
-        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        if (!publish_sync(x, k * k + P.q * k)) return;
         // keep P = psi^T X (q x k) in slot P0+3 ; G0 of L into ja via range_finder
         reduce_into(x, k * k, P.q, k, sm->slot[SL_P0 + 3]);
         // range finder expects G0 of the W side at partial offset 0 when doX is false
@@ -403,8 +498,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
             store_rows(x.st.W, sm->tO, r0, nr, k);
             __syncthreads();
         }
-        acc_publish(x, k * k + P.q * k);
-        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        if (!publish_sync(x, k * k + P.q * k)) return;
         reduce_into(x, 0, k, k, Sm);
         reduce_into(x, k * k, P.q, k, sm->slot[SL_P0 + 2]);  // Bk (q x k)
         // ---------------- phase L: in-scattering K (X side) and L (W side)
@@ -449,8 +543,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
             gram_acc(sm->acc, k * k, sm->tO, KM, k, sm->tO, KM, k, nr);
             __syncthreads();
         }
-        acc_publish(x, 2 * k * k);
-        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        if (!publish_sync(x, 2 * k * k)) return;
         if (!range_finder(x, x.st.K, x.st.L, true, true, k)) return;
         // ---------------- phase O: new bases; MUp, X^T psi, NUp, MRed^T D W
         const int offM = 0, offXp = k * k, offN = k * k + k * P.q, offB = 2 * k * k + k * P.q;
@@ -484,8 +577,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
             store_rows(x.st.W, sm->tO, r0, nr, k);
             __syncthreads();
         }
-        acc_publish(x, 2 * k * k + 2 * k * P.q);
-        if (!team_sync(x.st.bar, x.st.status, G)) return;
+        if (!publish_sync(x, 2 * k * k + 2 * k * P.q)) return;
         reduce_into(x, offM, k, k, sm->slot[SL_M]);
         reduce_into(x, offXp, k, P.q, sm->slot[SL_P0 + 3]);   // XNew^T psi (k x q)
         reduce_into(x, offN, k, k, sm->slot[SL_N]);

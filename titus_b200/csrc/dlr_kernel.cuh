@@ -13,7 +13,7 @@
 // The range finder: Jacobi eig of A^T A -> V; Gram of A V -> Jacobi -> V2, nu;
 // C = A V V2_J / nu_J materialised; CholQR on C. Directions with
 // nu_j <= tol nu_0 are null; rank-deficient bases are completed with the
-// problem's candidate vectors (boundary cells for X, odd moments for W).
+// candidate canonical vectors in index order (boundary cells for X, moments for W).
 #pragma once
 #include "dlr_device.cuh"
 
@@ -55,7 +55,15 @@ struct Ctx {
     double* CX;          // n x KM scratch (materialised C of the X-side range finder)
     double* CW;          // N x KM scratch
     int rhoK, rhoL;
+    unsigned long long* prof;  // non-null only on the profiled CTA
+    int red_mode;              // 1: reductions read the team's two-stage buffer
+    unsigned gen;              // team barrier generation
+    int parity;                // partial buffer in use (double-buffered)
+    int cur_n;                 // energy index of the current step (diagnostics)
 };
+
+constexpr int kDirectReduceMax = 16;  // teams up to this size sum partials directly
+constexpr int kBigRows = 6 * TR;      // rows per chunk when tA..tO are used as one tile
 
 __device__ __forceinline__ bool is_bnd(const DevProblem& P, int c) {
     int i = c / P.ny, j = c - (c / P.ny) * P.ny;
@@ -67,16 +75,27 @@ __device__ __forceinline__ void acc_zero(Ctx& x, int count) {
     for (int e = threadIdx.x; e < count; e += NT) x.sm->acc[e] = 0.0;
     __syncthreads();
 }
+// Partials are double-buffered by parity: a CTA may publish the next
+// reduction while slower CTAs still read the previous one.
+__device__ __forceinline__ double* part_base(const Ctx& x, int g) {
+    return x.st.part + ((size_t)x.parity * x.G + g) * PMAX;
+}
 __device__ __forceinline__ void acc_publish(Ctx& x, int count) {
-    double* dst = x.st.part + (size_t)x.b * PMAX;
+    x.parity ^= 1;
+    double* dst = part_base(x, x.b);
     for (int e = threadIdx.x; e < count; e += NT) dst[e] = x.sm->acc[e];
 }
 // sum partial entries [off, off+m*n) over the team's CTAs into dst (KM stride)
 __device__ void reduce_into(Ctx& x, int off, int m, int n, double* dst, int ld = KM) {
-    for (int e = threadIdx.x; e < m * n; e += NT) {
-        double s = 0.0;
-        for (int g = 0; g < x.G; ++g) s += ldcg(x.st.part + (size_t)g * PMAX + off + e);
-        dst[(e / n) * ld + e % n] = s;
+    ProfScope ps(x.prof, PF_REDUCE);
+    if (x.red_mode) {
+        for (int e = threadIdx.x; e < m * n; e += NT) dst[(e / n) * ld + e % n] = ldcg(x.st.red + off + e);
+    } else {
+        for (int e = threadIdx.x; e < m * n; e += NT) {
+            double s = 0.0;
+            for (int g = 0; g < x.G; ++g) s += ldcg(part_base(x, g) + off + e);
+            dst[(e / n) * ld + e % n] = s;
+        }
     }
     __syncthreads();
 }
@@ -159,14 +178,20 @@ __device__ void spmm_tile(const Ctx& x, const double* B, int r0, int nr, int k, 
 // ----------------------------------------------------- range finder parts ---
 // After G0 (Gram of A) is reduced into sm->ja: Jacobi -> V slot.
 __device__ void rf_eig0(Ctx& x, double* V, double* lam, int k) {
-    jacobi_eig(x.sm->ja, x.sm->jv, lam, k, x.st.status);
+    {
+        ProfScope ps(x.prof, PF_JACOBI);
+        jacobi_eig(x.sm->ja, x.sm->jv, lam, k, x.st.status);
+    }
     sm_copy(V, x.sm->jv, k, k);
 }
 // After G1 (Gram of A V) in sm->ja: Jacobi -> V2 ; T1 = V V2_J diag(1/nu_J); returns rho.
 __device__ int rf_eig1(Ctx& x, const double* V, double* T1, int k, double tol) {
     __shared__ double s_nu[KM];
     __shared__ int s_rho;
-    jacobi_eig(x.sm->ja, x.sm->jv, s_nu, k, x.st.status);
+    {
+        ProfScope ps(x.prof, PF_JACOBI);
+        jacobi_eig(x.sm->ja, x.sm->jv, s_nu, k, x.st.status);
+    }
     if (threadIdx.x == 0) {
         double nu0 = sqrt(fmax(s_nu[0], 0.0));
         int rho = 0;
@@ -197,6 +222,7 @@ __device__ int rf_eig1(Ctx& x, const double* V, double* T1, int k, double tol) {
 // B = CW Ri. Stores per accepted vector its candidate, norm and coefficients
 // w_a = P_{a-1}[c_a, :] in slot SL_WC (row a).
 __device__ void w_complete(Ctx& x, int rho, int need) {
+    ProfScope ps(x.prof, PF_COMPLETE);
     SmemLayout* sm = x.sm;
     double* wc = sm->slot[SL_WC];
     double* Ri = sm->slot[SL_RIL];

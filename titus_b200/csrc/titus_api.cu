@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -56,6 +57,9 @@ struct titus_solver {
     int num_sms = 0;
     int r = 0;
     int last_method = -1;
+    int last_G = 0;
+    unsigned long long* prof = nullptr;
+    int clock_khz = 0;
 
     template <class T>
     int alloc(T** p, size_t count, const T* host = nullptr) {
@@ -75,7 +79,8 @@ static int validate(const titus_problem_t* pb) {
     if (pb->n_moments != (pb->npn + 1) * (pb->npn + 1))
         return fail(TITUS_ERR_ARG, "n_moments %d != (npn+1)^2", pb->n_moments);
     if (pb->n_ordinates < 1) return fail(TITUS_ERR_ARG, "n_ordinates < 1");
-    if (pb->n_ordinates > QM) return fail(TITUS_ERR_LIMIT, "n_ordinates %d > %d supported", pb->n_ordinates, QM);
+    if (pb->n_ordinates > std::min(QM, KM))
+        return fail(TITUS_ERR_LIMIT, "n_ordinates %d > %d supported", pb->n_ordinates, std::min(QM, KM));
     if (pb->n_energies < 2) return fail(TITUS_ERR_ARG, "n_energies < 2");
     if (pb->r < 1) return fail(TITUS_ERR_ARG, "r < 1");
     if (pb->r > KM) return fail(TITUS_ERR_LIMIT, "rank %d > %d supported by this build", pb->r, KM);
@@ -213,14 +218,18 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
     if ((rc = s->alloc(&st.X, nK)) || (rc = s->alloc(&st.K, nK)) || (rc = s->alloc(&st.W, NK)) ||
         (rc = s->alloc(&st.L, 2 * NK)) || (rc = s->alloc(&st.psi0, (size_t)n * QM)) ||
         (rc = s->alloc(&st.psi1, (size_t)n * QM)) || (rc = s->alloc(&st.dose, n)) ||
-        (rc = s->alloc(&st.S, KK)) || (rc = s->alloc(&st.part, (size_t)s->num_sms * PMAX)) ||
-        (rc = s->alloc(&bar, 2)) || (rc = s->alloc(&st.status, 1)) || (rc = s->alloc(&info, 4)) ||
-        (rc = s->alloc(&st.rank_hist, nE)))
+        (rc = s->alloc(&st.S, KK)) || (rc = s->alloc(&st.part, (size_t)2 * s->num_sms * PMAX)) ||
+        (rc = s->alloc(&st.red, PMAX)) ||
+        (rc = s->alloc(&bar, s->num_sms + 1)) || (rc = s->alloc(&st.status, 1)) || (rc = s->alloc(&info, 4)) ||
+        (rc = s->alloc(&st.rank_hist, nE)) || (rc = s->alloc(&st.diag, 16)))
         return cleanup(rc);
     st.bar = bar;
     st.info = info;
     st.eta_hist = st.bound_hist = st.time_hist = nullptr;
     if ((rc = s->alloc(&s->d_st, 1))) return cleanup(rc);
+    if ((rc = s->alloc(&s->prof, 16))) return cleanup(rc);
+    CK(cudaMemset(s->prof, 0, 16 * sizeof(unsigned long long)));
+    CK(cudaDeviceGetAttribute(&s->clock_khz, cudaDevAttrClockRate, s->device));
     CK(cudaMemcpy(s->d_st, &st, sizeof(TeamState), cudaMemcpyHostToDevice));
     CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sizeof(SmemLayout)));
@@ -229,28 +238,38 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
 }
 
 // Initial factors of SolverCSD.jl:931-955: X = first r identity columns with
-// boundary rows zeroed, W = first r identity columns, S = 0; psi = 0, dose = 0.
+// boundary rows zeroed, W = first r identity columns, S = 0.
+__global__ void init_factors_kernel(TeamState* states, int n, int N, int nx, int ny, int r, int nE) {
+    TeamState st = states[blockIdx.y];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < r; j += gridDim.x * blockDim.x) {
+        if (j < n) {
+            int i = j / ny, jj = j % ny;
+            bool bnd = (i == 0 || jj == 0 || i == nx - 1 || jj == ny - 1);
+            st.X[(size_t)j * KM + j] = bnd ? 0.0 : 1.0;
+        }
+        if (j < N) st.W[(size_t)j * KM + j] = 1.0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st.info[0] = r;
+        st.info[1] = 0;
+        st.info[2] = 0;
+        st.info[3] = 2;
+    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nE; e += gridDim.x * blockDim.x) st.rank_hist[e] = -1;
+}
+
+// Device-side reset of one team's state (no host copies): factors, psi, dose.
 static int init_state(titus_solver* s, int r, cudaStream_t stream) {
     const int n = s->n, N = s->N;
     TeamState& st = s->st;
-    std::vector<double> X((size_t)n * KM, 0.0), W((size_t)N * KM, 0.0);
-    const int nx = s->P.nx, ny = s->P.ny;
-    for (int j = 0; j < r && j < n; ++j) {
-        int i = j / ny, jj = j % ny;
-        bool bnd = (i == 0 || jj == 0 || i == nx - 1 || jj == ny - 1);
-        X[(size_t)j * KM + j] = bnd ? 0.0 : 1.0;
-    }
-    for (int j = 0; j < r && j < N; ++j) W[(size_t)j * KM + j] = 1.0;
-    CK(cudaMemcpyAsync(st.X, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(st.W, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(st.X, 0, (size_t)n * KM * sizeof(double), stream));
+    CK(cudaMemsetAsync(st.W, 0, (size_t)N * KM * sizeof(double), stream));
     CK(cudaMemsetAsync(st.S, 0, KK * sizeof(double), stream));
     CK(cudaMemsetAsync(st.psi0, 0, (size_t)n * QM * sizeof(double), stream));
     CK(cudaMemsetAsync(st.psi1, 0, (size_t)n * QM * sizeof(double), stream));
     CK(cudaMemsetAsync(st.dose, 0, (size_t)n * sizeof(double), stream));
-    int info[4] = {r, 0, 0, 2};
-    CK(cudaMemcpyAsync(st.info, info, sizeof(info), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemsetAsync(st.rank_hist, 0xff, s->nE * sizeof(int), stream));
-    CK(cudaStreamSynchronize(stream));
+    init_factors_kernel<<<dim3(1, 1), 256, 0, stream>>>(s->d_st, n, N, s->P.nx, s->P.ny, r, s->nE);
+    CK(cudaGetLastError());
     return TITUS_OK;
 }
 
@@ -267,18 +286,26 @@ static int launch(titus_solver* s, int method, const titus_options_t* opt, int n
     if (G > per_sm * s->num_sms) G = per_sm * s->num_sms;
     DevProblem P = s->P;
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
-    CK(cudaMemsetAsync(s->st.bar, 0, 2 * sizeof(unsigned), stream));
+    P.prof = nullptr;
+    P.zero_smem = getenv("TITUS_ZERO_SMEM") ? 1 : 0;
+    if (opt && opt->profile) {
+        CK(cudaMemsetAsync(s->prof, 0, 16 * sizeof(unsigned long long), stream));
+        P.prof = s->prof;
+    }
+    CK(cudaMemsetAsync(s->st.bar, 0, (s->num_sms + 1) * sizeof(unsigned), stream));
     CK(cudaMemsetAsync(s->st.status, 0, sizeof(int), stream));
+    CK(cudaMemsetAsync(s->st.diag, 0, 16 * sizeof(double), stream));
     TeamState* dst = s->d_st;
     void* args[] = {&P, &dst, &G, &n_begin, &n_end, &dose2_pending};
     CK(cudaLaunchCooperativeKernel((void*)dlr_kernel<TITUS_DLR_FIXED>, dim3(G), dim3(NT), args, sizeof(SmemLayout),
                                    stream));
     s->last_method = method;
+    s->last_G = G;
     return TITUS_OK;
 }
 
-static int check_status(titus_solver* s, cudaStream_t stream) {
-    CK(cudaStreamSynchronize(stream));
+static int check_status(titus_solver* s) {
+    CK(cudaDeviceSynchronize());
     int status = 0;
     CK(cudaMemcpy(&status, s->st.status, sizeof(int), cudaMemcpyDeviceToHost));
     if (status != 0) {
@@ -286,6 +313,21 @@ static int check_status(titus_solver* s, cudaStream_t stream) {
                            : status == ST_CHOL_BREAKDOWN ? "Cholesky breakdown in the range finder"
                            : status == ST_COMPLETION      ? "basis completion ran out of candidates"
                                                           : "device error";
+        double d[16];
+        CK(cudaMemcpy(d, s->st.diag, sizeof(d), cudaMemcpyDeviceToHost));
+        if (status == ST_BARRIER_TIMEOUT) {
+            std::vector<unsigned> fl(s->num_sms + 1);
+            CK(cudaMemcpy(fl.data(), s->st.bar, fl.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+            std::string arr;
+            for (int i = 0; i < s->last_G; ++i) arr += std::to_string(fl[i]) + " ";
+            return fail(TITUS_ERR_DEVICE, "device status %d: %s (waiter %g saw %g wanted %g; release %u; arrivals %s)",
+                        status, what, d[8], d[9], d[10], fl[s->last_G], arr.c_str());
+        }
+        if (status == ST_CHOL_BREAKDOWN)
+            return fail(TITUS_ERR_DEVICE,
+                        "device status %d: %s (stage %g side %g k %g pivot %g value %.3e G00 %.3e min diag %.3e step %g;"
+                        " last range finder flags %g rhoK %g rhoL %g)",
+                        status, what, d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[11], d[12], d[13]);
         return fail(TITUS_ERR_DEVICE, "device status %d: %s", status, what);
     }
     return TITUS_OK;
@@ -307,7 +349,7 @@ extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus
 
 extern "C" int titus_fetch(titus_solver_t* s, titus_result_t* res) {
     if (!s || !res) return fail(TITUS_ERR_ARG, "NULL argument");
-    int rc = check_status(s, 0);
+    int rc = check_status(s);
     if (rc) return rc;
     int info[4];
     CK(cudaMemcpy(info, s->st.info, sizeof(info), cudaMemcpyDeviceToHost));
@@ -402,6 +444,15 @@ extern "C" int titus_last_error(char* buf, size_t len) {
     return TITUS_OK;
 }
 
+extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
+    if (!s || !ns || n < 0) return fail(TITUS_ERR_ARG, "NULL argument");
+    unsigned long long cyc[16];
+    CK(cudaMemcpy(cyc, s->prof, sizeof(cyc), cudaMemcpyDeviceToHost));
+    const int m = std::min<int>(n, PF_COUNT);
+    for (int i = 0; i < m; ++i) ns[i] = (double)cyc[i] * 1e6 / (double)s->clock_khz;
+    return m;
+}
+
 extern "C" int titus_max_rank(void) { return KM; }
-extern "C" int titus_max_ordinates(void) { return QM; }
+extern "C" int titus_max_ordinates(void) { return QM < KM ? QM : KM; }
 extern "C" const char* titus_version(void) { return "titus-b200 0.1 (sm_100a, FP64)"; }

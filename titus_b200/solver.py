@@ -137,12 +137,20 @@ class SolverCSD:
         except Exception:
             pass
 
-    def options(self, max_steps=0, rank_tol=0.0):
+    def options(self, max_steps=0, rank_tol=0.0, profile=False):
         o = _lib.Options()
         o.team_ctas = self.team_ctas
         o.max_steps = max_steps
         o.rank_tol = rank_tol
+        o.profile = 1 if profile else 0
         return o
+
+    def profile(self):
+        """Per-phase device timers (ns) of the last solve run with profile=True."""
+        lib = _lib.load()
+        out = np.zeros(16)
+        m = lib.titus_profile(self.handle(), _lib.as_dp(out), 16)
+        return {name: out[i] for i, name in enumerate(_lib.PROFILE_NAMES[:m]) if name != "-"}
 
     def _result(self, r_cap):
         res = _lib.Result()
@@ -160,13 +168,13 @@ class SolverCSD:
         res.r_cap = r_cap
         return res, bufs
 
-    def run(self, method: int, max_steps: int = 0, rank_tol: float = 0.0):
+    def run(self, method: int, max_steps: int = 0, rank_tol: float = 0.0, profile: bool = False):
         """Run one integrator on the device; returns raw factors and histories."""
         lib = _lib.load()
         h = self.handle()
         r_cap = max(self.settings.r, 1)
         res, bufs = self._result(r_cap)
-        opt = self.options(max_steps, rank_tol)
+        opt = self.options(max_steps, rank_tol, profile)
         _lib.check(lib.titus_solve(h, method, C.byref(opt), C.byref(res)), "titus_solve")
         k = res.rank
         return dict(X=bufs["X"][:, :k], S=bufs["S"][:k, :k], W=bufs["W"][:, :k], dose=bufs["dose"],
