@@ -110,7 +110,7 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
 // publishes the release generation in flags[G]; the others poll that. Every
 // spin is bounded (about a second); on expiry the status flag is set and all
 // CTAs leave. Returns false if the team's status flag is set.
-__device__ bool team_sync(unsigned* flags, int* status, int G, int b, unsigned& gen, double* diag = nullptr) {
+__device__ inline bool team_sync(unsigned* flags, int* status, int G, int b, unsigned& gen, double* diag = nullptr) {
     __shared__ int s_ok;
     constexpr long long kSpinLimit = 1ll << 21;
     __syncthreads();
@@ -172,7 +172,7 @@ __device__ __forceinline__ void set_status(int* status, int code) {
 // ---------------------------------------------------------------------------
 
 // C = A(mxk) * B(kxn); C must not alias A or B.
-__device__ void sm_mm(double* C, const double* A, const double* B, int m, int k, int n) {
+__device__ inline void sm_mm(double* C, const double* A, const double* B, int m, int k, int n) {
     for (int e = threadIdx.x; e < m * n; e += NT) {
         int i = e / n, j = e % n;
         double s = 0.0;
@@ -182,7 +182,7 @@ __device__ void sm_mm(double* C, const double* A, const double* B, int m, int k,
     __syncthreads();
 }
 // C = A(mxk) * B^T (B is n x k)
-__device__ void sm_mmt(double* C, const double* A, const double* B, int m, int k, int n) {
+__device__ inline void sm_mmt(double* C, const double* A, const double* B, int m, int k, int n) {
     for (int e = threadIdx.x; e < m * n; e += NT) {
         int i = e / n, j = e % n;
         double s = 0.0;
@@ -192,7 +192,7 @@ __device__ void sm_mmt(double* C, const double* A, const double* B, int m, int k
     __syncthreads();
 }
 // C = A^T(mxk, A is k x m) * B(kxn)
-__device__ void sm_tmm(double* C, const double* A, const double* B, int m, int k, int n) {
+__device__ inline void sm_tmm(double* C, const double* A, const double* B, int m, int k, int n) {
     for (int e = threadIdx.x; e < m * n; e += NT) {
         int i = e / n, j = e % n;
         double s = 0.0;
@@ -201,11 +201,11 @@ __device__ void sm_tmm(double* C, const double* A, const double* B, int m, int k
     }
     __syncthreads();
 }
-__device__ void sm_copy(double* D, const double* A, int m, int n) {
+__device__ inline void sm_copy(double* D, const double* A, int m, int n) {
     for (int e = threadIdx.x; e < m * n; e += NT) D[(e / n) * KM + e % n] = A[(e / n) * KM + e % n];
     __syncthreads();
 }
-__device__ void sm_zero(double* D, int m, int n) {
+__device__ inline void sm_zero(double* D, int m, int n) {
     for (int e = threadIdx.x; e < m * n; e += NT) D[(e / n) * KM + e % n] = 0.0;
     __syncthreads();
 }
@@ -227,7 +227,7 @@ __device__ __forceinline__ bool rr_pair(int m, int t, int s, int k, int& p, int&
 // Symmetric eigendecomposition by parallel cyclic Jacobi.
 // In: A (k x k symmetric, in smem work array Aw). Out: lam[k] descending,
 // V (k x k, columns eigenvectors, same order). Aw and V are smem arrays.
-__device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* status) {
+static __device__ __noinline__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* status) {
     __shared__ double rc[KM / 2 + 1], rs[KM / 2 + 1];
     __shared__ int rp[KM / 2 + 1], rq[KM / 2 + 1];
     __shared__ int s_rot[2];  // per-sweep-parity flag: a reset never races a late reader
@@ -332,7 +332,7 @@ __device__ void jacobi_eig(double* Aw, double* V, double* lam, int k, int* statu
 // lane c keeps column c of R and of R^{-1} in registers (fully unrolled loops,
 // so all register indices are static), row entries travel by shuffles.
 // Returns ||R||_F ||R^{-1}||_F, or +inf on breakdown (non-positive pivot).
-__device__ double warp_chol_inv(const double* G, double* R, double* Ri, int k, int* bad_j = nullptr,
+static __device__ __noinline__ double warp_chol_inv(const double* G, double* R, double* Ri, int k, int* bad_j = nullptr,
                                 double* bad_d = nullptr) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -413,7 +413,7 @@ __device__ double warp_chol_inv(const double* G, double* R, double* Ri, int k, i
 // On breakdown with `flag`, the first CTA to fail records in diag:
 // [0] stage tag, [1] side (0 = X, 1 = W), [2] k, [3] first bad pivot index,
 // [4] its value, [5] G[0][0], [6] min diagonal of G, [7] energy index.
-__device__ void record_breakdown(double* diag, int* status, int tag, int side, int k, int bj, double bd,
+__device__ inline void record_breakdown(double* diag, int* status, int tag, int side, int k, int bj, double bd,
                                  const double* G, int n) {
     if (atomicCAS(status, 0, ST_CHOL_BREAKDOWN) == 0 && diag) {
         double mn = INFINITY;
@@ -429,7 +429,7 @@ __device__ void record_breakdown(double* diag, int* status, int tag, int side, i
     }
 }
 
-__device__ void dual_chol(bool dx, const double* GX, double* RX, double* RiX, int kx, double* condX,
+__device__ inline void dual_chol(bool dx, const double* GX, double* RX, double* RiX, int kx, double* condX,
                           bool dw, const double* GW, double* RW, double* RiW, int kw, double* condW,
                           int* status, bool flag, double* diag = nullptr, int tag = 0, int n = 0) {
     __shared__ double s_c[2];

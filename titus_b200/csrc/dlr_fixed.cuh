@@ -14,7 +14,7 @@ __device__ __forceinline__ bool tsync(Ctx& x) {
 // team. Large teams add a second stage: CTA b sums slice b of the entries over
 // all partials into the team's reduced buffer, then a second barrier; small
 // teams let every CTA sum the partials directly (reduce_into).
-__device__ bool publish_sync(Ctx& x, int count) {
+__device__ inline bool publish_sync(Ctx& x, int count) {
     acc_publish(x, count);
     if (!tsync(x)) return false;
     if (x.G <= kDirectReduceMax) {
@@ -37,7 +37,7 @@ __device__ bool publish_sync(Ctx& x, int count) {
 
 // ---- phase A: (pending) second dose half-step, boundary inflow, first dose
 // half-step, X[bnd,:] = 0.  Own cells only; no reduction.
-__device__ void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc) {
+__device__ inline void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc) {
     const DevProblem& P = x.P;
     SmemLayout* sm = x.sm;
     const int k = x.k;
@@ -84,7 +84,7 @@ __device__ void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc) {
 }
 
 // ---- uncollided sweep for own cells (psi_in -> psi_out)
-__device__ void sweep_cells(Ctx& x, double sigma0) {
+__device__ inline void sweep_cells(Ctx& x, double sigma0) {
     const DevProblem& P = x.P;
     const double dE = P.dE;
     const double den = 1.0 + dE * sigma0;
@@ -111,7 +111,7 @@ __device__ void sweep_cells(Ctx& x, double sigma0) {
 
 // ---- streaming Grams X^T L_d X (own cells) and W^T A_d W (own moments):
 // partial layout [G_0..G_3 | C_0..C_3], each k x k.
-__device__ void stream_grams_partial(Ctx& x) {
+__device__ inline void stream_grams_partial(Ctx& x) {
     SmemLayout* sm = x.sm;
     const int k = x.k;
     for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
@@ -133,7 +133,7 @@ __device__ void stream_grams_partial(Ctx& x) {
 }
 
 // ---- range finder pass 1 (G1 = (A V)^T (A V)) on one side; A is n x k in global
-__device__ void rf_pass_b(Ctx& x, const double* A, int r0b, int r1b, const double* V, int k, int off) {
+__device__ inline void rf_pass_b(Ctx& x, const double* A, int r0b, int r1b, const double* V, int k, int off) {
     SmemLayout* sm = x.sm;
     for (int r0 = r0b; r0 < r1b; r0 += TR) {
         int nr = min(TR, r1b - r0);
@@ -146,7 +146,7 @@ __device__ void rf_pass_b(Ctx& x, const double* A, int r0b, int r1b, const doubl
     }
 }
 // ---- range finder pass 2: C = A T1 (written to Cbuf), G2 = C^T C
-__device__ void rf_pass_c(Ctx& x, const double* A, double* Cbuf, int r0b, int r1b, const double* T1, int k,
+__device__ inline void rf_pass_c(Ctx& x, const double* A, double* Cbuf, int r0b, int r1b, const double* T1, int k,
                           int rho, int off) {
     SmemLayout* sm = x.sm;
     for (int r0 = r0b; r0 < r1b; r0 += TR) {
@@ -165,7 +165,7 @@ __device__ void rf_pass_c(Ctx& x, const double* A, double* Cbuf, int r0b, int r1
 // solves (written to Cbuf), G = Y^T Y.
 // Rows are processed in chunks of kBigRows over the contiguous tile area
 // tA..tO (free during the range finder), one thread per row for the solve.
-__device__ void rf_pass_solve(Ctx& x, const double* A, double* Cbuf, int r0b, int r1b, const double* R, int k, int off) {
+__device__ inline void rf_pass_solve(Ctx& x, const double* A, double* Cbuf, int r0b, int r1b, const double* R, int k, int off) {
     SmemLayout* sm = x.sm;
     double* big = sm->tA;
     for (int r0 = r0b; r0 < r1b; r0 += kBigRows) {
@@ -190,7 +190,7 @@ __device__ void rf_pass_solve(Ctx& x, const double* A, double* Cbuf, int r0b, in
 //  rank-revealing path: Jacobi eig of G0 -> V; Gram of A V -> Jacobi -> V2,
 //    nu; C = A V V2_J / nu_J with nu_j > tol nu_0; CholQR of C.
 // Returns false if the team aborted.
-__device__ bool range_finder(Ctx& x, const double* AX, const double* AW, bool doX, bool doW, int k) {
+static __device__ __noinline__ bool range_finder(Ctx& x, const double* AX, const double* AW, bool doX, bool doW, int k) {
     SmemLayout* sm = x.sm;
     const double tol = x.P.rank_tol;
     const double kCert = 1e5;
@@ -269,7 +269,7 @@ __device__ bool range_finder(Ctx& x, const double* AX, const double* AW, bool do
 }
 
 // small: D = A S B^T (k x k) with scratch
-__device__ void sm_asbt(double* D, const double* A, const double* S, const double* B, double* tmp, int k) {
+__device__ inline void sm_asbt(double* D, const double* A, const double* S, const double* B, double* tmp, int k) {
     sm_mm(tmp, A, S, k, k, k);
     sm_mmt(D, tmp, B, k, k, k);
 }

@@ -86,7 +86,7 @@ __device__ __forceinline__ void acc_publish(Ctx& x, int count) {
     for (int e = threadIdx.x; e < count; e += NT) dst[e] = x.sm->acc[e];
 }
 // sum partial entries [off, off+m*n) over the team's CTAs into dst (KM stride)
-__device__ void reduce_into(Ctx& x, int off, int m, int n, double* dst, int ld = KM) {
+__device__ inline void reduce_into(Ctx& x, int off, int m, int n, double* dst, int ld = KM) {
     ProfScope ps(x.prof, PF_REDUCE);
     if (x.red_mode) {
         for (int e = threadIdx.x; e < m * n; e += NT) dst[(e / n) * ld + e % n] = ldcg(x.st.red + off + e);
@@ -136,7 +136,7 @@ __device__ __forceinline__ void tile_mm(double* tO, const double* tA, const doub
 
 // Matrix-free stencils (stencils.jl:26-128) applied to rows [r0, r0+nr) of A:
 // t[0] = L2x A, t[1] = L2y A, t[2] = L1x A, t[3] = L1y A; zero on boundary rows.
-__device__ void stencil_tile(const Ctx& x, const double* A, int r0, int nr, int k, double (*t)[TR * KM]) {
+__device__ inline void stencil_tile(const Ctx& x, const double* A, int r0, int nr, int k, double (*t)[TR * KM]) {
     const DevProblem& P = x.P;
     const double hx = 0.5 / P.dx, hy = 0.5 / P.dy;
     for (int e = threadIdx.x; e < nr * k; e += NT) {
@@ -162,7 +162,7 @@ __device__ void stencil_tile(const Ctx& x, const double* A, int r0, int nr, int 
 }
 
 // Sparse P_N operators applied to rows [r0, r0+nr) of B (N x KM): t[d] = A_d B.
-__device__ void spmm_tile(const Ctx& x, const double* B, int r0, int nr, int k, double (*t)[TR * KM]) {
+__device__ inline void spmm_tile(const Ctx& x, const double* B, int r0, int nr, int k, double (*t)[TR * KM]) {
     for (int e = threadIdx.x; e < NOPS * nr * k; e += NT) {
         int d = e / (nr * k);
         int rem = e - d * nr * k;
@@ -177,7 +177,7 @@ __device__ void spmm_tile(const Ctx& x, const double* B, int r0, int nr, int k, 
 
 // ----------------------------------------------------- range finder parts ---
 // After G0 (Gram of A) is reduced into sm->ja: Jacobi -> V slot.
-__device__ void rf_eig0(Ctx& x, double* V, double* lam, int k) {
+__device__ inline void rf_eig0(Ctx& x, double* V, double* lam, int k) {
     {
         ProfScope ps(x.prof, PF_JACOBI);
         jacobi_eig(x.sm->ja, x.sm->jv, lam, k, x.st.status);
@@ -185,7 +185,7 @@ __device__ void rf_eig0(Ctx& x, double* V, double* lam, int k) {
     sm_copy(V, x.sm->jv, k, k);
 }
 // After G1 (Gram of A V) in sm->ja: Jacobi -> V2 ; T1 = V V2_J diag(1/nu_J); returns rho.
-__device__ int rf_eig1(Ctx& x, const double* V, double* T1, int k, double tol) {
+__device__ inline int rf_eig1(Ctx& x, const double* V, double* T1, int k, double tol) {
     __shared__ double s_nu[KM];
     __shared__ int s_rho;
     {
@@ -221,7 +221,7 @@ __device__ int rf_eig1(Ctx& x, const double* V, double* T1, int k, double tol) {
 // candidate c is accepted when 1 - ||P[c,:]||^2 > 1/4, P = [B, v_1..v_a],
 // B = CW Ri. Stores per accepted vector its candidate, norm and coefficients
 // w_a = P_{a-1}[c_a, :] in slot SL_WC (row a).
-__device__ void w_complete(Ctx& x, int rho, int need) {
+static __device__ __noinline__ void w_complete(Ctx& x, int rho, int need) {
     ProfScope ps(x.prof, PF_COMPLETE);
     SmemLayout* sm = x.sm;
     double* wc = sm->slot[SL_WC];
@@ -271,7 +271,7 @@ __device__ void w_complete(Ctx& x, int rho, int need) {
 
 // Materialise rows [r0, r0+nr) of the new W-side basis into tile t:
 // columns :rho = C Ri, columns rho+a = completion vector a.
-__device__ void w_basis_tile(Ctx& x, int r0, int nr, int rho, int need, double* t) {
+__device__ inline void w_basis_tile(Ctx& x, int r0, int nr, int rho, int need, double* t) {
     SmemLayout* sm = x.sm;
     const double* Ri = sm->slot[SL_RIL];
     load_rows(sm->tA, x.CW, r0, nr, rho);
@@ -300,7 +300,7 @@ __device__ void w_basis_tile(Ctx& x, int r0, int nr, int rho, int need, double* 
 }
 
 // Materialise rows of the new X-side basis: C Ri, then completion cells.
-__device__ void x_basis_tile(Ctx& x, int r0, int nr, int rho, int k, double* t) {
+__device__ inline void x_basis_tile(Ctx& x, int r0, int nr, int rho, int k, double* t) {
     SmemLayout* sm = x.sm;
     const double* Ri = sm->slot[SL_RIK];
     load_rows(sm->tA, x.CX, r0, nr, rho);
