@@ -139,6 +139,25 @@ int titus_last_error(char* buf, size_t len);
  * [8] (unused), [9] kernel total. Returns the number of entries written. */
 int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
 
+/* Fixed-rank solve (method TITUS_DLR_FIXED) that allocates nothing. No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc, because a host framework's allocator or memory pool owns their
+ * device memory or their policy forbids device allocation after start-up.
+ * `problem` holds DEVICE pointers in the same layout titus_create reads from
+ * host memory; dose (n), X (n x r), S (r x r), W (N x r) and psi (n x q) are
+ * device output buffers owned by the caller (row-major). All intermediates live
+ * in one static device array of 16 MiB that every GPU loading the library keeps
+ * until the process exits; problems that need more are rejected with
+ * TITUS_ERR_LIMIT (rank <= 24, q <= 24, at most 32 CTAs per solve). All calls
+ * on a device share that array, so calls that overlap on the GPU race: issue
+ * them one at a time per device. Each call clears what must start at zero. The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture. The call returns after the solve has finished on `stream`.
+ * Error text (if any) is written to err[0..err_len). */
+int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* options, double* dose,
+                        double* X, double* S, double* W, double* psi, int32_t* rank_out, void* stream,
+                        char* err, size_t err_len);
+
 /* Build / capability queries. */
 int titus_max_rank(void);        /* largest basis width (columns) supported */
 int titus_max_ordinates(void);   /* largest q supported */

@@ -63,6 +63,8 @@ SIGNATURES = [
     ("titus_destroy", None, [C.c_void_p]),
     ("titus_last_error", C.c_int, [C.c_char_p, C.c_size_t]),
     ("titus_profile", C.c_int, [C.c_void_p, _dp, C.c_int32]),
+    ("titus_solve_noalloc", C.c_int, [C.POINTER(Problem), C.POINTER(Options), _dp, _dp, _dp, _dp, _dp, _ip,
+                                      C.c_void_p, C.c_char_p, C.c_size_t]),
     ("titus_max_rank", C.c_int, []),
     ("titus_max_ordinates", C.c_int, []),
     ("titus_version", C.c_char_p, []),
