@@ -31,6 +31,10 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(name="csd_water_beam_100x100_P21_r20_fixed", Nx=101, r=20, nPN=21, problem="csdWaterBeam",
                 method="fixed")
 ORACLE_SAMPLE_STEPS = 40
+# DRAM bytes (read + write) per energy step of dlr_kernel on this workload, from
+# one ncu capture of energy steps 2..21 (5.01 MB read + 0.22 MB written); the
+# per-launch figure scales it to the launch's energy steps.
+DRAM_BYTES_PER_STEP_NCU = (5.010176e6 + 0.218112e6) / 20
 
 
 def algorithmic_bytes_per_step(n, r, q, w=8):
@@ -235,7 +239,9 @@ def run_gpu(args, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_STEP_NCU * steps_per_solve,
+                         "traffic_note": "ncu 20-step capture scaled to the launch's energy steps",
+                         "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
