@@ -91,16 +91,22 @@ typedef struct titus_result {
     int32_t r_cap;         /* capacity (columns) of X, S, W */
     int32_t rank;          /* out: rank of the returned factors */
     int32_t steps_done;    /* out: loop iterations executed */
-    int32_t* rank_history; /* optional (nE): rank after each iteration, -1 if unused */
-    double* eta_history;   /* optional (nE): streaming eta (BUG), 0 otherwise */
-    double* bound_history; /* optional (nE): eta bound (BUG) */
-    double* time_history;  /* optional (nE): accumulated pseudo-time t (parallel) / energy (BUG) */
+    int32_t* rank_history; /* optional (nE): fixed / parallel: rank after the step with energy
+                              index n at [n-1]; BUG: rank at the start of each loop iteration
+                              (repeated energies included, first nE iterations); -1 if unused */
+    double* eta_history;   /* optional (nE): BUG streaming eta of each rejection test, in order */
+    double* bound_history; /* optional (nE): the matching bound c_eta theta max(1e-7,||S||)/dE */
+    double* time_history;  /* optional (nE): parallel: pseudo-time t at [n-1];
+                              BUG: energy index n (1-based) of each iteration */
 } titus_result_t;
 
 typedef struct titus_solver titus_solver_t;
 
 /* Upload the problem and allocate device state (replaces the data that
- * `SolverCSD(settings)` prepares, SolverCSD.jl:63-146). */
+ * `SolverCSD(settings)` prepares, SolverCSD.jl:63-146). problem->r is
+ * settings.r: the fixed rank (TITUS_DLR_FIXED, r <= 24 in this build) or the
+ * rank cap of the adaptive integrators (r <= titus_max_rank(), which start at
+ * floor(r/2); a step whose rank would exceed 40 fails with TITUS_ERR_LIMIT). */
 int titus_create(const titus_problem_t* problem, titus_solver_t** out);
 
 /* Run one integrator over the energy grid on the device and copy the result
@@ -121,7 +127,9 @@ int titus_solve_problem(const titus_problem_t* problem, int32_t method,
 
 /* Checkpoint / resume: replace the device state (X, S, W of the given rank,
  * psi, dose) and the next energy index `n_next` (1-based like the reference
- * loop variable n), then titus_solve_from continues the loop from there. */
+ * loop variable n), then titus_solve_from continues the loop from there with
+ * any integrator (rank <= 24 for TITUS_DLR_FIXED, <= 40 for the adaptive ones;
+ * the BUG loop's pseudo-time restarts at (n_next - 2) dE). */
 int titus_set_state(titus_solver_t* solver, int32_t rank, const double* X, const double* S,
                     const double* W, const double* psi, const double* dose, int32_t n_next);
 int titus_solve_from(titus_solver_t* solver, int32_t method, const titus_options_t* options,
@@ -159,7 +167,7 @@ int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* o
                         char* err, size_t err_len);
 
 /* Build / capability queries. */
-int titus_max_rank(void);        /* largest basis width (columns) supported */
+int titus_max_rank(void);        /* largest settings.r accepted (adaptive rank cap) */
 int titus_max_ordinates(void);   /* largest q supported */
 const char* titus_version(void);
 

@@ -28,6 +28,27 @@ def svd_full(A: np.ndarray):
     return U, s, Vt.T
 
 
+def svd_det(A: np.ndarray, tol: float | None = None):
+    """Thin SVD (U, s, V) with the deterministic null-space rule.
+
+    Singular vectors of singular values ``s_j <= tol * s_1`` are not fixed by A
+    (LAPACK returns rounding-noise directions there). ``truncate!`` keeps such
+    directions whenever its l1 tail test or its lower clamp reaches them, so
+    they are replaced by canonical vectors in index order, completed against the
+    columns kept so far (same acceptance rule as ``orth``). Singular values are
+    returned as computed.
+    """
+    tol = RANK_TOL if tol is None else tol
+    U, s, Vt = np.linalg.svd(A, full_matrices=False)
+    V = Vt.T
+    m = s.size
+    rho = int(np.sum(s > tol * s[0])) if m and s[0] > 0 else 0
+    if rho < m:
+        U = np.column_stack([U[:, :rho], _complete(U[:, :rho], m - rho, U.shape[0])])
+        V = np.column_stack([V[:, :rho], _complete(V[:, :rho], m - rho, V.shape[0])])
+    return U, s, V
+
+
 def _complete(B: np.ndarray, need: int, n: int, order=None) -> np.ndarray:
     cols = []
     order = np.arange(n) if order is None else order
@@ -82,7 +103,9 @@ def orth_augment(X: np.ndarray, K: np.ndarray, mode: str = "lapack", tol: float 
         return Q
     tol = RANK_TOL if tol is None else tol
     n = X.shape[0]
-    scale = np.linalg.norm(np.column_stack([X, K]), 2)
+    # scale of the rank cut: the Frobenius norm of [X K] (within sqrt(rX + rK)
+    # of the 2-norm, and exactly reproducible from the Gram of [X K])
+    scale = np.linalg.norm(np.column_stack([X, K]))
     Q1 = _range_basis(X, scale, tol)
     if Q1.shape[1] < X.shape[1]:
         Q1 = np.column_stack([Q1, _complete(Q1, X.shape[1] - Q1.shape[1], n, order)])

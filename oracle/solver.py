@@ -187,7 +187,7 @@ class SolverCSD:
     def truncate(self, X, S, W):
         """``truncate!`` (``SolverCSD.jl:3369-3399``): l1 tail test, clamp [2, r]."""
         s = self.settings
-        U, D, V = la.svd_full(S)
+        U, D, V = la.svd_det(S) if self.basis_mode == "det" else la.svd_full(S)
         rMaxTotal = s.r
         rMinTotal = 2
         tol = s.theta * np.linalg.norm(D) ** s.thetaIndex
@@ -335,11 +335,14 @@ def _step_prologue(solver, psi, X, S, W, n, dE):
     return sigma, Dvec, sigma[0] - Dvec
 
 
-def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None):
+def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
+                       n_begin: int = 2, return_state: bool = False):
     """``SolveFirstCollisionSourceDLRParallel`` (``SolverCSD.jl:1726-2008``).
 
     Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, rVec, psi) with
     rVec (2 x nEnergies): row 0 the accumulated pseudo-time t, row 1 the rank.
+    ``state`` (X, S, W, psi, dose, optionally t) resumes the loop at ``n_begin``;
+    ``return_state`` returns that dict (with ``n_next``) for the end of the run.
     """
     s = solver.settings
     mode = solver.basis_mode
@@ -355,8 +358,14 @@ def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None):
     Mr = solver.MReduced
     rVec = r * np.ones((2, nE))
     t = 0.0
-    last = nE if max_steps is None else min(nE, 1 + max_steps)
-    for n in range(2, last + 1):
+    if state is not None:
+        X, S, W = state["X"].copy(), state["S"].copy(), state["W"].copy()
+        psi = state["psi"].reshape(psi.shape).copy()
+        solver.dose = state["dose"].copy()
+        r = S.shape[0]
+        t = state.get("t", (n_begin - 2) * dE)
+    last = nE if max_steps is None else min(nE, n_begin - 1 + max_steps)
+    for n in range(n_begin, last + 1):
         sigma, Dvec, D = _step_prologue(solver, psi, X, S, W, n, dE)
         if n > 2:
             G = solver._x_grams(X, X)  # before X[bnd] = 0 (:1856-1859)
@@ -403,18 +412,24 @@ def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None):
         rVec[0, n - 1] = t
         rVec[1, n - 1] = r
         t += dE
+    if return_state:
+        return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), t=t,
+                    n_next=last + 1, rVec=rVec)
     U, Sig, V = la.svd_full(S)
     return X @ U, 0.5 * math.sqrt(solver.gamma[0]) * Sig, solver.O @ (W @ V), W @ V, solver.dose, rVec, psi
 
 
-def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None):
+def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
+                  n_begin: int = 2, return_state: bool = False):
     """``SolveFirstCollisionSourceDLRBUGRejection`` (``SolverCSD.jl:2011-2374``).
 
     The undefined name ``rmax`` (``:2205, :2295``) is read as ``settings.r``,
     the bound the neighbouring branches use (``:2227, :2283``). Rejected steps
     repeat with the doubled basis exactly as the reference does, including the
     psi sweep and first dose half-step already applied (``n = n-1; continue``).
-    ``max_steps`` bounds the number of loop iterations.
+    ``max_steps`` bounds the number of loop iterations. ``state`` (X, S, W, psi,
+    dose, optionally t) resumes the loop at energy index ``n_begin``;
+    ``return_state`` returns that dict (with ``n_next``) at the end.
 
     Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, [E rank]^T,
     [E eta], [E bound], psi).
@@ -435,13 +450,23 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None):
     Mr = solver.MReduced
     t = 0.0
     n = 1
+    if state is not None:
+        X, S, W = state["X"].copy(), state["S"].copy(), state["W"].copy()
+        psi = state["psi"].reshape(psi.shape).copy()
+        solver.dose = state["dose"].copy()
+        r = S.shape[0]
+        t = state.get("t", (n_begin - 2) * dE)
+        n = n_begin - 1
     timeVec, rankInTime, etaVec, etaVecTime, etaBoundVec = [], [], [], [], []
     iters = 0
+    n_next = None
     while t < nE * dE:
         n += 1
         if n == nE:
+            n_next = n
             break
         if max_steps is not None and iters >= max_steps:
+            n_next = n
             break
         iters += 1
         timeVec.append(energy[n - 1])
@@ -529,6 +554,10 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None):
         r = S.shape[0]
         solver.dose_half(X, S, W, psi, dE, solver.csd.S[n - 1])
         t += dE
+    if return_state:
+        return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), t=t,
+                    n_next=n_next if n_next is not None else n + 1, rank=rankInTime, eta=etaVec,
+                    bound=etaBoundVec, iters=iters)
     U, Sig, V = la.svd_full(S)
     rank_hist = np.array([timeVec, rankInTime], dtype=float)
     eta_hist = np.array([etaVecTime, etaVec], dtype=float).T

@@ -1,0 +1,1391 @@
+// Rank-adaptive DLR energy loops as one persistent kernel per solve:
+//   METHOD 1  SolveFirstCollisionSourceDLRParallel     (SolverCSD.jl:1726-2008)
+//   METHOD 2  SolveFirstCollisionSourceDLRBUGRejection (SolverCSD.jl:2011-2374)
+// with truncate! (:3369-3399) and the augmented bases qr([X K]) (:149-153).
+//
+// Step structure (every arrow into a reduction is one team barrier pair):
+//   A   boundary inflow + first dose half-step (own cells)          -> barrier
+//   B   uncollided sweep; streaming Grams X^T L_d X, W^T A_d W     -> reduce
+//   C   K = X S - dE sum L_d X S C_d ; L = W S^T - dE sum A_d W S^T G_d^T,
+//       with the Grams of [X K] and [W L]                         -> reduce
+//   AUG Q1 = orth(X) from the Gram (certified Cholesky or Jacobi),
+//       K' = (I - Q1 Q1^T)^2 K in two passes                      -> 2 reduces
+//       range finder of K' (certified CholQR2, or Jacobi twice)    -> 1-2 reduces
+//       X~ = [K' basis, completion] materialised in X[:, r:2r]
+//   TRUNC one-sided Jacobi SVD of the 2r x 2r S, l1 tail rank, X <- [X X~] U_k
+//   OS  out-scattering L = W S^T / (1 + dE D), W = orth(L), S = L^T W
+//   IS  in-scattering K / L / S, augmentation, truncation (BUG: rejection test)
+// Every CTA holds bit-identical small matrices, so rank and rejection
+// decisions are uniform across the team.
+#pragma once
+#include "wide_linalg.cuh"
+
+namespace titus {
+namespace wide {
+
+constexpr double kCertW = 1e5;   // ||R||_F ||R^-1||_F bound of the certified Cholesky paths
+constexpr double kNullSvd = 1e-12;
+__device__ __forceinline__ double raw_gram_floor(int k) { return 4.0 * k * 2.2e-16; }
+constexpr double kGradedFloor = 1e-32;
+
+__device__ __forceinline__ double* sside(const WCtx& x, int s, int off) {
+    return x.scr + SO_SIDE + s * SIDE_STRIDE + off;
+}
+
+// ------------------------------------------------------------- row kernels ---
+// F[r][fc + d*k + j] = (L_d A)[r0 + r][j]; zero on boundary rows (stencils.jl:26-128).
+__device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0, int nr, int k, double* F, int ldf,
+                                 int fc) {
+    const DevProblem& P = x.P;
+    const double hx = 0.5 / P.dx, hy = 0.5 / P.dy;
+    for (int e = threadIdx.x; e < nr * k; e += NT) {
+        const int r = e / k, j = e - (e / k) * k;
+        const int c = r0 + r;
+        double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
+        if (!is_bnd_w(P, c)) {
+            const double a0 = ldcg(A + (size_t)c * lda + j) * P.rinv[c];
+            const double axm = ldcg(A + (size_t)(c - P.ny) * lda + j) * P.rinv[c - P.ny];
+            const double axp = ldcg(A + (size_t)(c + P.ny) * lda + j) * P.rinv[c + P.ny];
+            const double aym = ldcg(A + (size_t)(c - 1) * lda + j) * P.rinv[c - 1];
+            const double ayp = ldcg(A + (size_t)(c + 1) * lda + j) * P.rinv[c + 1];
+            l2x = (axp - axm) * hx;
+            l2y = (ayp - aym) * hy;
+            l1x = a0 / P.dx - hx * axm - hx * axp;
+            l1y = a0 / P.dy - hy * aym - hy * ayp;
+        }
+        double* row = F + r * ldf + fc;
+        row[0 * k + j] = l2x;
+        row[1 * k + j] = l2y;
+        row[2 * k + j] = l1x;
+        row[3 * k + j] = l1y;
+    }
+}
+// F[r][fc + d*k + j] = (A_d B)[r0 + r][j] (sparse P_N operators Ax, Az, |Ax|, |Az|).
+__device__ inline void w_spmm(const WCtx& x, const double* B, int ldb, int r0, int nr, int k, double* F, int ldf,
+                              int fc) {
+    for (int e = threadIdx.x; e < NOPS * nr * k; e += NT) {
+        const int d = e / (nr * k);
+        const int rem = e - d * nr * k;
+        const int r = rem / k, j = rem - (rem / k) * k;
+        const Csr& A = x.P.op[d];
+        const int m = r0 + r;
+        double s = 0.0;
+        for (int p = A.rowptr[m]; p < A.rowptr[m + 1]; ++p) s = fma(A.val[p], ldcg(B + (size_t)A.col[p] * ldb + j), s);
+        F[r * ldf + fc + d * k + j] = s;
+    }
+}
+
+// dose += 1/2 dE (X[c,:k] v + psi[c,:] MRed[0,:]) stopping[sidx] / rho (SolverCSD.jl:990-997)
+static __device__ __noinline__ void w_dose(WCtx& x, int sidx, const double* v, int k, bool zero_bnd_x) {
+    const DevProblem& P = x.P;
+    const double f = 0.5 * P.dE * P.stopping[sidx];
+    for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT) {
+        double xv = 0.0;
+        if (!(zero_bnd_x && is_bnd_w(P, c)))
+            for (int j = 0; j < k; ++j) xv = fma(ldcg(x.st.X + (size_t)c * KA + j), v[j], xv);
+        const double* pr = x.psi_in + (size_t)c * QW;
+        double u = 0.0;
+        for (int kq = 0; kq < P.q; ++kq) u = fma(pr[kq], P.mred[kq], u);
+        x.st.dose[c] += f * (xv + u) * P.rinv[c];
+    }
+}
+
+// v = S W[0,:k]^T (S: shared, ld KA; W row 0 from global)
+__device__ inline void sw0(WCtx& x, const double* S, int ldS, int k, double* v, double* w0) {
+    for (int j = threadIdx.x; j < k; j += NT) w0[j] = ldcg(x.st.W + j);
+    __syncthreads();
+    for (int i = threadIdx.x; i < k; i += NT) {
+        double s = 0.0;
+        for (int j = 0; j < k; ++j) s = fma(S[i * ldS + j], w0[j], s);
+        v[i] = s;
+    }
+    __syncthreads();
+}
+
+// ---- phase A: boundary inflow at energy[n-1] (PsiBeam, :977-988), first dose half-step
+static __device__ __noinline__ void w_phase_A(WCtx& x, int n) {
+    const DevProblem& P = x.P;
+    WSmem* sm = x.sm;
+    const int k = x.r;
+    sw0(x, sm->S, KA, k, sm->vec, sm->vec + KA);
+    const double bce = P.bc_energy[n - 2];
+    for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT) {
+        if (is_bnd_w(P, c)) {
+            double* pr = x.psi_in + (size_t)c * QW;
+            const double bs = bce * P.bc_space[c];
+            for (int kq = 0; kq < P.q; ++kq) pr[kq] = bs * P.bc_angle[kq];
+        }
+    }
+    __syncthreads();
+    w_dose(x, n - 2, sm->vec, k, false);
+}
+
+// ---- uncollided sweep of own cells, psi_in -> psi_out (solveFluxUpwind! :388-463, :1000-1005)
+static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
+    const DevProblem& P = x.P;
+    const double dE = P.dE;
+    const double den = 1.0 + dE * sigma0;
+    const int q = P.q;
+    for (int e = threadIdx.x; e < (x.c1 - x.c0) * q; e += NT) {
+        const int c = x.c0 + e / q, kq = e - (e / q) * q;
+        const double pc = ldcg(x.psi_in + (size_t)c * QW + kq);
+        double flux = 0.0;
+        if (!is_bnd_w(P, c)) {
+            const double ox = P.omega[kq * 3 + 0], oz = P.omega[kq * 3 + 2];
+            const double f0 = pc * P.rinv[c];
+            double ew, ns;
+            if (ox >= 0.0) ew = f0 - ldcg(x.psi_in + (size_t)(c - P.ny) * QW + kq) * P.rinv[c - P.ny];
+            else ew = ldcg(x.psi_in + (size_t)(c + P.ny) * QW + kq) * P.rinv[c + P.ny] - f0;
+            if (oz >= 0.0) ns = f0 - ldcg(x.psi_in + (size_t)(c - 1) * QW + kq) * P.rinv[c - 1];
+            else ns = ldcg(x.psi_in + (size_t)(c + 1) * QW + kq) * P.rinv[c + 1] - f0;
+            flux = (ox / P.dx) * ew + (oz / P.dy) * ns;
+        }
+        double out = (pc - dE * flux) / den;
+        if (kq == 0 && P.restore[c]) out = pc;
+        x.psi_out[(size_t)c * QW + kq] = out;
+    }
+}
+
+// ---- streaming Grams of width k over A (cells, stencils) and B (moments, P_N
+// operators): acc[d k^2 ..] = A^T L_d A, acc[(4+d) k^2 ..] = B^T A_d B.
+// `cw` = width of A and B used; blocks for d in [d0, d1) only (chunking).
+static __device__ __noinline__ void w_grams_pass(WCtx& x, const double* A, const double* B, int cw, int d0, int d1, int off0,
+                                    double* acc, double* F) {
+    GBlock bl[4];
+    int nb = 0;
+    const int kk = cw * cw;
+    for (int d = d0; d < d1; ++d) bl[nb++] = GBlock{0, cw, (d + 1) * cw, cw, (d - d0) * kk};
+    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
+        const int nr = min(TRW, x.c1 - r0);
+        wload(F, FLD, 0, A, KA, 0, r0, nr, cw);
+        w_stencil(x, A, KA, r0, nr, cw, F, FLD, cw);
+        __syncthreads();
+        gram_blocks(acc + off0, F, FLD, nr, bl, nb);
+        __syncthreads();
+    }
+    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+        const int nr = min(TRW, x.m1 - r0);
+        wload(F, FLD, 0, B, KA, 0, r0, nr, cw);
+        w_spmm(x, B, KA, r0, nr, cw, F, FLD, cw);
+        __syncthreads();
+        gram_blocks(acc + off0 + (d1 - d0) * kk, F, FLD, nr, bl, nb);
+        __syncthreads();
+    }
+}
+
+__device__ inline void w_acc_zero(double* acc, int cnt) {
+    for (int e = threadIdx.x; e < cnt; e += NT) acc[e] = 0.0;
+    __syncthreads();
+}
+
+// Streaming Grams with the rank-r factors (before X[bnd,:] = 0, :1856-1859),
+// published at [G_0..G_3 | C_0..C_3] (r x r each) and reduced; X's boundary
+// rows are zeroed between the barriers (:1859).
+static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
+    const int k = x.r;
+    double* acc = x.sm->work;
+    double* F = x.sm->work + ACCW;
+    w_acc_zero(acc, 8 * k * k);
+    w_grams_pass(x, x.st.X, x.st.W, k, 0, 4, 0, acc, F);
+    wpublish_chunk(x, acc, 0, 8 * k * k);
+    return wreduce(x, 8 * k * k, [&] {
+        for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT)
+            if (is_bnd_w(x.P, c))
+                for (int j = 0; j < k; ++j) x.st.X[(size_t)c * KA + j] = 0.0;
+    });
+}
+
+// After the streaming Grams: SC_d = S C_d, SG_d = S^T G_d^T (stacked, rows d*k + l,
+// ld k) in scratch; Sbar = S - dE sum G_d S C_d in scratch (ld RA).
+static __device__ __noinline__ void w_stream_small(WCtx& x, bool want_sbar) {
+    const int k = x.r;
+    WSmem* sm = x.sm;
+    double* Gd = sm->work;                 // 4 k x k (ld k), from red
+    double* Cd = sm->work + 4 * RA * RA;   // 4 k x k
+    double* T = sm->work + 8 * RA * RA;    // k x k temp
+    double* U = sm->work + 9 * RA * RA;    // k x k temp
+    double* SC = x.scr + SO_SC;
+    double* SG = x.scr + SO_SG;
+    double* Sb = x.scr + SO_SBAR;
+    load_red(x, 0, 4 * k, k, Gd, k);
+    load_red(x, 4 * k * k, 4 * k, k, Cd, k);
+    for (int d = 0; d < 4; ++d) {
+        const double* G = Gd + d * k * k;
+        const double* C = Cd + d * k * k;
+        g_mm(SC + d * k * k, k, sm->S, KA, false, C, k, false, k, k, k);         // S C_d
+        g_mm(SG + d * k * k, k, sm->S, KA, true, G, k, true, k, k, k);           // S^T G_d^T
+    }
+    if (want_sbar) {
+        g_copy(Sb, RA, sm->S, KA, k, k);
+        for (int d = 0; d < 4; ++d) {
+            g_mm(T, k, sm->S, KA, false, Cd + d * k * k, k, false, k, k, k);     // S C_d
+            g_mm(U, k, Gd + d * k * k, k, false, T, k, false, k, k, k);          // G_d S C_d
+            for (int e = threadIdx.x; e < k * k; e += NT) Sb[(e / k) * RA + e % k] -= x.P.dE * U[e];
+            __syncthreads();
+        }
+    }
+}
+
+// ---- phase C: K and L streaming updates (:1861-1880) written to st.K / st.L,
+// and the Grams of [X K] (X side) and [W L] (W side): per side three k x k
+// blocks [A^T A | A^T B | B^T B] at offsets 0 and 3k^2.
+static __device__ __noinline__ bool w_phase_C(WCtx& x) {
+    const int k = x.r;
+    const double dE = x.P.dE;
+    WSmem* sm = x.sm;
+    double* acc = sm->work;                      // 6 k^2
+    double* ST = sm->work + 6 * RA * RA;         // 4k x k stacked (SC or SG)
+    double* F = ST + 4 * RA * RA;                // TRW x FLD
+    double* T = F + TRW * FLD;                   // TRW x 2k feature tile [A | B]
+    w_acc_zero(acc, 6 * k * k);
+    const GBlock bl[3] = {{0, k, 0, k, 0}, {0, k, k, k, k * k}, {k, k, k, k, 2 * k * k}};
+    // X side
+    g_copy(ST, k, x.scr + SO_SC, k, 4 * k, k);
+    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
+        const int nr = min(TRW, x.c1 - r0);
+        wload(T, 2 * RA, 0, x.st.X, KA, 0, r0, nr, k);
+        w_stencil(x, x.st.X, KA, r0, nr, k, F, FLD, 0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            double s = 0.0;
+            for (int l = 0; l < k; ++l) s = fma(T[r * 2 * RA + l], sm->S[l * KA + j], s);
+            double t = 0.0;
+            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * FLD + l], ST[l * k + j], t);
+            T[r * 2 * RA + k + j] = s - dE * t;
+        }
+        __syncthreads();
+        wstore(x.st.K, RA, 0, T, 2 * RA, k, r0, nr, k);
+        gram_blocks(acc, T, 2 * RA, nr, bl, 3);
+        __syncthreads();
+    }
+    // W side
+    g_copy(ST, k, x.scr + SO_SG, k, 4 * k, k);
+    const GBlock bw[3] = {{0, k, 0, k, 3 * k * k}, {0, k, k, k, 4 * k * k}, {k, k, k, k, 5 * k * k}};
+    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+        const int nr = min(TRW, x.m1 - r0);
+        wload(T, 2 * RA, 0, x.st.W, KA, 0, r0, nr, k);
+        w_spmm(x, x.st.W, KA, r0, nr, k, F, FLD, 0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            double s = 0.0;  // (W S^T)[r][j]
+            for (int l = 0; l < k; ++l) s = fma(T[r * 2 * RA + l], sm->S[j * KA + l], s);
+            double t = 0.0;
+            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * FLD + l], ST[l * k + j], t);
+            T[r * 2 * RA + k + j] = s - dE * t;
+        }
+        __syncthreads();
+        wstore(x.st.L, RA, 0, T, 2 * RA, k, r0, nr, k);
+        gram_blocks(acc, T, 2 * RA, nr, bw, 3);
+        __syncthreads();
+    }
+    wpublish_chunk(x, acc, 0, 6 * k * k);
+    return wreduce(x, 6 * k * k);
+}
+
+// ------------------------------------------------------- augmentation -------
+// Side s: A = X (cells, ld KA) or W (moments, ld KA); B = K or L (ld RA);
+// BP = projected B; C = range-finder output.
+struct SideBufs {
+    double* A;
+    double* B;
+    double* BP;
+    double* C;
+    int r0, r1;
+};
+__device__ __forceinline__ SideBufs side_bufs(const WCtx& x, int s) {
+    if (s == 0) return SideBufs{x.st.X, x.st.K, x.st.KP, x.st.CX, x.c0, x.c1};
+    return SideBufs{x.st.W, x.st.L, x.st.LP, x.st.CW, x.m0, x.m1};
+}
+
+// Q1 = orth(A) from the reduced Gram blocks at `goff` (s*3k^2): certified
+// Cholesky or Jacobi; T1 = P1 (A^T B) with P1 = F1 F1^T (Q1 Q1^T = A P1 A^T on
+// the range part; completion vectors of the X side are orthogonal to K).
+static __device__ __noinline__ void aug_prepare(WCtx& x, int s, int goff) {
+    const int k = x.r;
+    WSmem* sm = x.sm;
+    SideInfo& si = x.side[s];
+    double* G11 = sm->work;
+    double* G12 = G11 + RA * RA;
+    double* R = G12 + RA * RA;
+    double* Ri = R + RA * RA;
+    double* T = Ri + RA * RA;
+    double* lam = sm->vec;
+    load_red(x, goff, k, k, G11, RA);
+    load_red(x, goff + k * k, k, k, G12, RA);
+    // Frobenius norm of [A B]: traces of A^T A and B^T B
+    double tr = 0.0;
+    for (int j = 0; j < k; ++j) tr += G11[j * RA + j] + ldcg(x.redp + goff + 2 * k * k + j * k + j);
+    si.scale = sqrt(fmax(tr, 0.0));
+    const double tol = x.P.rank_tol;
+    double rif;
+    const double cond = w_chol(G11, RA, R, Ri, RA, k, &rif);
+    double* F1 = sside(x, s, SS_F1);
+    double* P1 = sside(x, s, SS_P1);
+    double* M1 = sside(x, s, SS_M1);
+    if (cond < kCertW && 1.0 / rif > 10.0 * tol * si.scale) {
+        si.fast1 = 1;
+        si.rho1 = k;
+        g_copy(F1, RA, Ri, RA, k, k);
+        g_copy(M1, RA, R, RA, k, k);
+    } else {
+        si.fast1 = 0;
+        // G11 is still intact (w_chol copies); Jacobi destroys it
+        w_eig(G11, T, RA, lam, k, x.st.status, raw_gram_floor(k));
+        int rho = 0;
+        for (int j = 0; j < k; ++j) {
+            if (sqrt(fmax(lam[j], 0.0)) > tol * si.scale) rho = j + 1;
+            else break;
+        }
+        si.rho1 = rho;
+        for (int e = threadIdx.x; e < k * k; e += NT) {
+            const int i = e / k, j = e - (e / k) * k;
+            const double sq = j < rho ? sqrt(lam[j]) : 0.0;
+            F1[i * RA + j] = j < rho ? T[i * RA + j] / sq : 0.0;
+            M1[i * RA + j] = i < rho ? sqrt(lam[i]) * T[j * RA + i] : 0.0;   // Lambda^{1/2} V^T
+        }
+        __syncthreads();
+        if (s == 1 && rho < k && threadIdx.x == 0) set_status(x.st.status, ST_UNSUPPORTED);
+    }
+    __syncthreads();
+    // P1 = F1 F1^T (only the first rho1 columns of F1 are nonzero)
+    g_mm(P1, RA, F1, RA, false, F1, RA, true, k, si.rho1, k);
+    // T1 = P1 G12
+    g_mm(sside(x, s, SS_T), RA, P1, RA, false, G12, RA, false, k, k, k);
+}
+
+// BP = B - A T (T = SS_T) for own rows; acc[off..] += A^T BP (second=false) or BP^T BP (second=true)
+static __device__ __noinline__ void aug_pass(WCtx& x, int s, bool second, double* acc, int off) {
+    const int k = x.r;
+    SideBufs sb = side_bufs(x, s);
+    double* T = x.sm->work + ACCW;               // k x k (ld RA)
+    double* F = T + RA * RA;                     // TRW x 2RA: [A | BP]
+    g_copy(T, RA, sside(x, s, SS_T), RA, k, k);
+    const GBlock bl = second ? GBlock{k, k, k, k, off} : GBlock{0, k, k, k, off};
+    const double* Bsrc = second ? sb.BP : sb.B;
+    for (int r0 = sb.r0; r0 < sb.r1; r0 += TRW) {
+        const int nr = min(TRW, sb.r1 - r0);
+        wload(F, 2 * RA, 0, sb.A, KA, 0, r0, nr, k);
+        wload(F, 2 * RA, k, Bsrc, RA, 0, r0, nr, k);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            double t = 0.0;
+            for (int l = 0; l < k; ++l) t = fma(F[r * 2 * RA + l], T[l * RA + j], t);
+            F[r * 2 * RA + k + j] -= t;
+        }
+        __syncthreads();
+        wstore(sb.BP, RA, 0, F, 2 * RA, k, r0, nr, k);
+        gram_blocks(acc, F, 2 * RA, nr, &bl, 1);
+        __syncthreads();
+    }
+}
+
+// Both sides: BP = (I - Q1 Q1^T)^2 B in two passes; ends with BP^T BP reduced
+// at offsets s*k^2.
+static __device__ __noinline__ bool aug_project(WCtx& x) {
+    const int k = x.r;
+    double* acc = x.sm->work;
+    w_acc_zero(acc, 2 * k * k);
+    aug_pass(x, 0, false, acc, 0);
+    aug_pass(x, 1, false, acc, k * k);
+    wpublish_chunk(x, acc, 0, 2 * k * k);
+    if (!wreduce(x, 2 * k * k)) return false;
+    for (int s = 0; s < 2; ++s) {
+        // T2 = P1 (A^T BP)
+        double* G = x.sm->work;
+        load_red(x, s * k * k, k, k, G, RA);
+        g_mm(sside(x, s, SS_T), RA, sside(x, s, SS_P1), RA, false, G, RA, false, k, k, k);
+    }
+    w_acc_zero(acc, 2 * k * k);
+    aug_pass(x, 0, true, acc, 0);
+    aug_pass(x, 1, true, acc, k * k);
+    wpublish_chunk(x, acc, 0, 2 * k * k);
+    return wreduce(x, 2 * k * k);
+}
+
+// Row-wise triangular solve t[r,:] <- t[r,:] R^{-1} (R upper, shared, ld RA).
+__device__ __forceinline__ void w_rsolve(double* t, int ldt, const double* R, int nr, int k) {
+    for (int r = threadIdx.x; r < nr; r += NT) {
+        double* row = t + r * ldt;
+        for (int j = 0; j < k; ++j) {
+            double v = row[j];
+            for (int i = 0; i < j; ++i) v = fma(-row[i], R[i * RA + j], v);
+            row[j] = v / R[j * RA + j];
+        }
+    }
+}
+
+// C = BP M (mode 0: M = R0 by row solves; mode 1: M = T (k x rho), product) for
+// own rows; acc[off..] += C^T C (rho x rho), or (mode 2) (BP V)^T (BP V) without
+// storing C.
+static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, double* acc, int off) {
+    const int k = x.r;
+    SideBufs sb = side_bufs(x, s);
+    double* M = x.sm->work + ACCW;          // k x k (ld RA)
+    double* F = M + RA * RA;                // TRW x 2RA: [BP | out]
+    g_copy(M, RA, sside(x, s, mode == 0 ? SS_R0 : (mode == 1 ? SS_T : SS_V0)), RA, k, mode == 1 ? rho : k);
+    const int w = (mode == 1) ? rho : k;
+    const GBlock bl{k, w, k, w, off};
+    for (int r0 = sb.r0; r0 < sb.r1; r0 += TRW) {
+        const int nr = min(TRW, sb.r1 - r0);
+        wload(F, 2 * RA, 0, sb.BP, RA, 0, r0, nr, k);
+        __syncthreads();
+        if (mode == 0) {
+            for (int e = threadIdx.x; e < nr * k; e += NT) F[(e / k) * 2 * RA + k + e % k] = F[(e / k) * 2 * RA + e % k];
+            __syncthreads();
+            w_rsolve(F + k, 2 * RA, M, nr, k);
+        } else {
+            for (int e = threadIdx.x; e < nr * w; e += NT) {
+                const int r = e / w, j = e - (e / w) * w;
+                double t = 0.0;
+                for (int l = 0; l < k; ++l) t = fma(F[r * 2 * RA + l], M[l * RA + j], t);
+                F[r * 2 * RA + k + j] = t;
+            }
+        }
+        __syncthreads();
+        if (mode != 2) wstore(sb.C, RA, 0, F, 2 * RA, k, r0, nr, w);
+        gram_blocks(acc, F, 2 * RA, nr, &bl, 1);
+        __syncthreads();
+    }
+}
+
+// Final step of a range finder: CholQR of C from its reduced Gram (rho x rho at
+// red offset `off`) -> SS_RI.
+static __device__ __noinline__ void rf_finish(WCtx& x, int s, int off) {
+    const int rho = x.side[s].rho2;
+    if (rho <= 0) return;
+    double* G = x.sm->work;
+    double* R = G + RA * RA;
+    double* Ri = R + RA * RA;
+    load_red(x, off, rho, rho, G, RA);
+    double rif;
+    const double cond = w_chol(G, RA, R, Ri, RA, rho, &rif);
+    if (!(cond < INFINITY) && threadIdx.x == 0) {
+        if (atomicCAS(x.st.status, 0, ST_CHOL_BREAKDOWN) == 0) {
+            x.st.diag[0] = 10 + s;
+            x.st.diag[2] = rho;
+            x.st.diag[7] = x.cur_n;
+        }
+    }
+    g_copy(sside(x, s, SS_RI), RA, Ri, RA, rho, rho);
+}
+
+// Slow path after the Gram of BP V0 was reduced at `off`: Jacobi -> V2, nu;
+// rho = #{nu_j > cut}; SS_T = V0 V2[:, :rho] diag(1/nu).
+static __device__ __noinline__ void rf_slow_rank(WCtx& x, int s, int off, bool plain) {
+    const int k = x.r;
+    SideInfo& si = x.side[s];
+    double* G = x.sm->work;
+    double* V2 = G + RA * RA;
+    double* V0 = V2 + RA * RA;
+    double* nu = x.sm->vec;
+    load_red(x, off, k, k, G, RA);
+    w_eig(G, V2, RA, nu, k, x.st.status, kGradedFloor);
+    g_copy(V0, RA, sside(x, s, SS_V0), RA, k, k);
+    const double nu0 = sqrt(fmax(nu[0], 0.0));
+    const double cut = x.P.rank_tol * (plain ? nu0 : si.scale);
+    int rho = 0;
+    if (!(plain && nu0 <= 0.0))
+        for (int j = 0; j < k; ++j) {
+            if (sqrt(fmax(nu[j], 0.0)) > cut) rho = j + 1;
+            else break;
+        }
+    si.rho2 = rho;
+    double* T = sside(x, s, SS_T);
+    for (int e = threadIdx.x; e < k * rho; e += NT) {
+        const int i = e / rho, j = e - (e / rho) * rho;
+        double a = 0.0;
+        for (int l = 0; l < k; ++l) a = fma(V0[i * RA + l], V2[l * RA + j], a);
+        T[i * RA + j] = a / sqrt(nu[j]);
+    }
+    __syncthreads();
+}
+
+// Range finders of BP on the sides with do_side[s], after BP^T BP was reduced
+// at offsets s*k^2. `plain[s]`: the rank cut is relative to the largest
+// singular value of BP itself (orth), else to side[s].scale (augmentation).
+//  certified path: Cholesky of BP^T BP with ||R||_F ||R^-1||_F < 1e5 (and, for
+//    augmentation, sigma_min > 10 tol scale): C = BP R0^{-1} by row solves;
+//  rank-revealing path: Jacobi of BP^T BP -> V0; Gram of BP V0 -> Jacobi ->
+//    V2, nu; C = BP V0 V2_J / nu_J for nu_j above the cut.
+// On return side[s].rho2 is set and SS_RI holds R^{-1} of the CholQR of C, so
+// that the basis is C R^{-1} (rho2 columns).
+static __device__ __noinline__ bool range_find(WCtx& x, const bool do_side[2], const bool plain[2]) {
+    const int k = x.r;
+    WSmem* sm = x.sm;
+    const double tol = x.P.rank_tol;
+    bool slow[2] = {false, false};
+    for (int s = 0; s < 2; ++s) {
+        if (!do_side[s]) continue;
+        SideInfo& si = x.side[s];
+        double* G = sm->work;
+        double* R = G + RA * RA;
+        double* Ri = R + RA * RA;
+        double* V = Ri + RA * RA;
+        load_red(x, s * k * k, k, k, G, RA);
+        double rif;
+        const double cond = w_chol(G, RA, R, Ri, RA, k, &rif);
+        const bool ok = cond < kCertW && (plain[s] || 1.0 / rif > 10.0 * tol * si.scale);
+        if (ok) {
+            si.fast2 = 1;
+            si.rho2 = k;
+            g_copy(sside(x, s, SS_R0), RA, R, RA, k, k);
+        } else {
+            si.fast2 = 0;
+            slow[s] = true;
+            w_eig(G, V, RA, sm->vec, k, x.st.status, raw_gram_floor(k));
+            g_copy(sside(x, s, SS_V0), RA, V, RA, k, k);
+        }
+    }
+    double* acc = sm->work;
+    // pass 1: certified -> C = BP R0^{-1} and C^T C ; rank-revealing -> Gram of BP V0
+    w_acc_zero(acc, 2 * k * k);
+    for (int s = 0; s < 2; ++s)
+        if (do_side[s]) rf_pass(x, s, x.side[s].fast2 ? 0 : 2, k, acc, s * k * k);
+    wpublish_chunk(x, acc, 0, 2 * k * k);
+    if (!wreduce(x, 2 * k * k)) return false;
+    for (int s = 0; s < 2; ++s) {
+        if (!do_side[s]) continue;
+        if (!slow[s]) rf_finish(x, s, s * k * k);
+        else rf_slow_rank(x, s, s * k * k, plain[s]);
+    }
+    if (slow[0] || slow[1]) {
+        w_acc_zero(acc, 2 * k * k);
+        for (int s = 0; s < 2; ++s)
+            if (slow[s] && x.side[s].rho2 > 0) rf_pass(x, s, 1, x.side[s].rho2, acc, s * k * k);
+        wpublish_chunk(x, acc, 0, 2 * k * k);
+        if (!wreduce(x, 2 * k * k)) return false;
+        for (int s = 0; s < 2; ++s)
+            if (slow[s]) rf_finish(x, s, s * k * k);
+    }
+    __syncthreads();
+    return true;
+}
+
+// W-side completion in the small space: candidates m = 0, 1, ... accepted when
+// 1 - ||P[m,:]||^2 > 1/4 with P = [Q1 (nq1 cols, rows W[m,:] F1), Q2 (rows
+// C[m,:] RI), v_1 .. v_a]; stores per accepted vector its candidate, norm and
+// coefficients in SS_WC (row a, length nq1 + rho2 + a).
+static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, int need) {
+    WSmem* sm = x.sm;
+    double* wc = sside(x, 1, SS_WC);
+    const double* F1 = sside(x, 1, SS_F1);
+    const double* Ri = sside(x, 1, SS_RI);
+    double* wrow = sm->vec;             // W[c,:] (k) then C[c,:] (rho2)
+    double* prow = sm->vec + 2 * KA;    // P[c,:] (nq1 + rho2 + a <= 3 RA)
+    __shared__ int s_acc, s_next;
+    const int k = x.r;
+    if (threadIdx.x == 0) {
+        s_acc = 0;
+        s_next = 0;
+    }
+    __syncthreads();
+    while (true) {
+        const int acc = s_acc, it = s_next;
+        if (acc >= need) break;
+        if (it >= x.P.nwcomp) {
+            if (threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+            __syncthreads();
+            break;
+        }
+        const int c = x.P.wcomp[it];
+        if (nq1 > 0)
+            for (int j = threadIdx.x; j < k; j += NT) wrow[j] = ldcg(x.st.W + (size_t)c * KA + j);
+        for (int j = threadIdx.x; j < rho2; j += NT) wrow[KA + j] = ldcg(x.st.CW + (size_t)c * RA + j);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nq1 + rho2; j += NT) {
+            double s = 0.0;
+            if (j < nq1)
+                for (int l = 0; l < k; ++l) s = fma(wrow[l], F1[l * RA + j], s);
+            else
+                for (int l = 0; l <= j - nq1; ++l) s = fma(wrow[KA + l], Ri[l * RA + (j - nq1)], s);
+            prow[j] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int nb = nq1 + rho2;
+            for (int a = 0; a < acc; ++a) {
+                const double* w = wc + a * WCS;
+                double v = (c == sm->wcand[a]) ? 1.0 : 0.0;
+                for (int j = 0; j < nb + a; ++j) v -= prow[j] * w[j];
+                prow[nb + a] = v / sm->wnrm[a];
+            }
+            double ss = 0.0;
+            for (int j = 0; j < nb + acc; ++j) ss += prow[j] * prow[j];
+            const double nv2 = 1.0 - ss;
+            if (nv2 > 0.25) {
+                for (int j = 0; j < nb + acc; ++j) wc[acc * WCS + j] = prow[j];
+                sm->wcand[acc] = c;
+                sm->wnrm[acc] = sqrt(nv2);
+                s_acc = acc + 1;
+            }
+            s_next = it + 1;
+        }
+        __syncthreads();
+    }
+}
+
+// Materialise the new directions: A[:, k:2k] = [C RI | completion]; with
+// `with_q1` also A[:, :k] = Q1 = [A F1 | completion] (BUG). Row tile t holds
+// [old A (k) | Q1 (k) | X~ (k)] per row.
+static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q1) {
+    const int k = x.r;
+    WSmem* sm = x.sm;
+    SideBufs sb = side_bufs(x, s);
+    const SideInfo& si = x.side[s];
+    double* F1 = sm->work;                   // k x k
+    double* Ri = F1 + RA * RA;               // rho2 x rho2
+    double* t = Ri + RA * RA;                // TRW x 3RA
+    double* cb = t + TRW * 3 * RA;           // TRW x RA (C rows)
+    g_copy(F1, RA, sside(x, s, SS_F1), RA, k, k);
+    if (si.rho2 > 0) g_copy(Ri, RA, sside(x, s, SS_RI), RA, si.rho2, si.rho2);
+    const double* wc = sside(x, 1, SS_WC);
+    const int rho1 = si.rho1, rho2 = si.rho2;
+    for (int r0 = sb.r0; r0 < sb.r1; r0 += TRW) {
+        const int nr = min(TRW, sb.r1 - r0);
+        wload(t, 3 * RA, 0, sb.A, KA, 0, r0, nr, k);
+        if (rho2 > 0) wload(cb, RA, 0, sb.C, RA, 0, r0, nr, rho2);
+        __syncthreads();
+        // Q1 columns (range part A F1, then completion) and X~ range part C RI
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            const int row = r0 + r;
+            double q1;
+            if (j < rho1) {
+                q1 = 0.0;
+                for (int l = 0; l < k; ++l) q1 = fma(t[r * 3 * RA + l], F1[l * RA + j], q1);
+            } else {
+                const int ci = j - rho1;   // X side only (W side has rho1 == k)
+                q1 = (s == 0 && ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
+            }
+            t[r * 3 * RA + k + j] = q1;
+            double xt = 0.0;
+            if (j < rho2) {
+                for (int l = 0; l <= j; ++l) xt = fma(cb[r * RA + l], Ri[l * RA + j], xt);
+            } else if (s == 0) {
+                const int ci = si.cand0 + (j - rho2);
+                xt = (ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
+            }
+            t[r * 3 * RA + 2 * k + j] = xt;
+        }
+        __syncthreads();
+        if (s == 1 && si.need2 > 0) {
+            // completion vectors v_a[m] = (delta_{m,c_a} - P[m,:] w_a) / nrm_a, P = [Q1 | Q2 | v_1..]
+            for (int r = threadIdx.x; r < nr; r += NT) {
+                const int m = r0 + r;
+                double* q1r = t + r * 3 * RA + k;       // Q1 row (k)
+                double* q2r = t + r * 3 * RA + 2 * k;   // [Q2 (rho2) | v_1 ..]
+                for (int a = 0; a < si.need2; ++a) {
+                    const double* w = wc + a * WCS;
+                    double v = (m == sm->wcand[a]) ? 1.0 : 0.0;
+                    for (int j = 0; j < k; ++j) v -= q1r[j] * w[j];
+                    for (int j = 0; j < rho2 + a; ++j) v -= q2r[j] * w[k + j];
+                    q2r[rho2 + a] = v / sm->wnrm[a];
+                }
+            }
+            __syncthreads();
+        }
+        if (with_q1) wstore(sb.A, KA, 0, t, 3 * RA, k, r0, nr, k);
+        wstore(sb.A, KA, k, t, 3 * RA, 2 * k, r0, nr, k);
+        __syncthreads();
+    }
+}
+
+// Whole augmentation of both sides after the [A B] Grams were reduced at
+// offsets 0 (X) and 3k^2 (W). Leaves the new directions in columns [k, 2k)
+// (and Q1 in [0, k) with with_q1), without a closing barrier.
+static __device__ __noinline__ bool augment(WCtx& x, bool with_q1) {
+    const int k = x.r;
+    if (2 * k > KA) {
+        if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+        return false;
+    }
+    aug_prepare(x, 0, 0);
+    aug_prepare(x, 1, 3 * k * k);
+    if (!aug_project(x)) return false;
+    const bool all[2] = {true, true};
+    const bool aug[2] = {false, false};
+    if (!range_find(x, all, aug)) return false;
+    SideInfo& sx = x.side[0];
+    sx.need2 = k - sx.rho2;
+    sx.cand0 = k - sx.rho1;
+    if (sx.cand0 + sx.need2 > x.P.nxcomp && threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+    SideInfo& sw = x.side[1];
+    sw.need2 = k - sw.rho2;
+    sw.cand0 = 0;
+    if (sw.need2 > 0) {
+        w_complete_side(x, k, sw.rho2, sw.need2);
+        // the completion read W[c, :k] of other CTAs' rows; Q1 overwrites those columns
+        if (with_q1 && !wsync(x)) return false;
+    }
+    materialize_side(x, 0, with_q1);
+    materialize_side(x, 1, with_q1);
+    return true;
+}
+
+// --------------------------------------------------------------- truncate ---
+// truncate! of the m x m matrix given in transposed storage in work[0..):
+// SVD, l1 tail rank (clamped to [2, settings.r]), deterministic completion of
+// the kept null directions. Leaves U^T (rows perm[j]) at work[0], V^T at
+// work[KA*KA], sig/perm in shared memory; returns the kept rank.
+static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
+    WSmem* sm = x.sm;
+    double* At = sm->work;
+    double* Vt = sm->work + KA * KA;
+    // keep the SVD input (transposed) for diagnostics
+    g_copy(x.scr + SO_DBG, KA, At, KA, m, m);
+    const int sw = w_svd(At, Vt, KA, m, sm->sig, sm->perm);
+    if (sw < 0 && threadIdx.x == 0 && atomicCAS(x.st.status, 0, ST_SVD) == 0) {
+        x.st.diag[0] = 20;
+        x.st.diag[2] = m;
+        x.st.diag[7] = x.cur_n;
+    }
+    // tol = theta ||D||_2^thetaIndex ; first j with |sum_{i >= j} D_i| < tol
+    double nrm = 0.0;
+    for (int j = 0; j < m; ++j) nrm = fma(sm->sig[j], sm->sig[j], nrm);
+    const double tol = x.P.theta * pow(sqrt(nrm), x.P.theta_index);
+    const int half = m / 2;
+    int kk = half;
+    for (int j = 1; j <= 2 * half; ++j) {
+        double tail = 0.0;
+        for (int i = j - 1; i < 2 * half; ++i) tail += sm->sig[i];
+        if (fabs(tail) < tol) {
+            kk = j;
+            break;
+        }
+    }
+    kk = min(kk, x.P.r);
+    kk = max(kk, 2);
+    kk = min(kk, m);
+    w_svd_complete(At, Vt, KA, m, sm->sig, sm->perm, kk, kNullSvd, x.st.status);
+    return kk;
+}
+
+// X <- X[:, :m] U[:, :kk], W <- W[:, :m] V[:, :kk] for own rows; S = diag(sig[:kk]).
+// With dose2: dose += 1/2 dE (X_new S_new W_new[0,:]^T + psi MRed[0]) S[sidx] / rho.
+// `w0` (m entries, any memory): row 0 of W before the update, needed for the
+// dose because the CTA owning moment 0 overwrites it without a team barrier.
+static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int dose_sidx, const double* w0) {
+    WSmem* sm = x.sm;
+    const double* Ut = sm->work;
+    const double* Vt = sm->work + KA * KA;
+    double* t = sm->work + 2 * KA * KA;     // TRW x KA
+    double* o = t + TRW * KA;               // TRW x KA
+    double* v = sm->vec;                    // diag(sig) W_new[0,:]^T
+    if (dose_sidx >= 0) {
+        for (int j = threadIdx.x; j < kk; j += NT) {
+            double a = 0.0;
+            for (int i = 0; i < m; ++i) a = fma(w0[i], Vt[sm->perm[j] * KA + i], a);
+            v[j] = sm->sig[j] * a;
+        }
+        __syncthreads();
+    }
+    for (int side = 0; side < 2; ++side) {
+        double* A = side == 0 ? x.st.X : x.st.W;
+        const double* B = side == 0 ? Ut : Vt;
+        const int r0b = side == 0 ? x.c0 : x.m0, r1b = side == 0 ? x.c1 : x.m1;
+        for (int r0 = r0b; r0 < r1b; r0 += TRW) {
+            const int nr = min(TRW, r1b - r0);
+            wload(t, KA, 0, A, KA, 0, r0, nr, m);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nr * kk; e += NT) {
+                const int r = e / kk, j = e - (e / kk) * kk;
+                const double* bj = B + sm->perm[j] * KA;
+                double a = 0.0;
+                for (int i = 0; i < m; ++i) a = fma(t[r * KA + i], bj[i], a);
+                o[r * KA + j] = a;
+            }
+            __syncthreads();
+            wstore(A, KA, 0, o, KA, 0, r0, nr, kk);
+            __syncthreads();
+        }
+    }
+    // S = diag(sig[:kk])
+    for (int e = threadIdx.x; e < KA * KA; e += NT) sm->S[e] = 0.0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < kk; j += NT) sm->S[j * KA + j] = sm->sig[j];
+    __syncthreads();
+    if (dose_sidx >= 0) w_dose(x, dose_sidx, v, kk, false);
+    __syncthreads();
+    x.r = kk;
+}
+
+// ------------------------------------------------------ scattering passes ---
+// Out-scattering L = W S^T / (1 + dE D) (own moments, :1885-1890), written to
+// L and LP, with L^T L at red offset k^2 (the range finder's side-1 slot); X
+// side: X^T psi of the X before zeroing (:1904) at offset 2k^2.
+static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig) {
+    const int k = x.r;
+    const DevProblem& P = x.P;
+    WSmem* sm = x.sm;
+    double* acc = sm->work;
+    double* t = sm->work + ACCW;     // TRW x (KA + QW)
+    const int ldt = KA + QW;
+    w_acc_zero(acc, 2 * k * k + k * P.q);
+    const GBlock bl{k, k, k, k, k * k};
+    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+        const int nr = min(TRW, x.m1 - r0);
+        wload(t, ldt, 0, x.st.W, KA, 0, r0, nr, k);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            double s = 0.0;
+            for (int l = 0; l < k; ++l) s = fma(t[r * ldt + l], sm->S[j * KA + l], s);
+            const int m = r0 + r;
+            const double D = sig[0] - sig[P.lof[m]];
+            t[r * ldt + k + j] = s / (1.0 + P.dE * D);
+        }
+        __syncthreads();
+        wstore(x.st.L, RA, 0, t, ldt, k, r0, nr, k);
+        wstore(x.st.LP, RA, 0, t, ldt, k, r0, nr, k);
+        gram_blocks(acc, t, ldt, nr, &bl, 1);
+        __syncthreads();
+    }
+    const GBlock bx{0, k, k, P.q, 2 * k * k};
+    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
+        const int nr = min(TRW, x.c1 - r0);
+        wload(t, ldt, 0, x.st.X, KA, 0, r0, nr, k);
+        wload(t, ldt, k, x.psi_in, QW, 0, r0, nr, P.q);
+        __syncthreads();
+        gram_blocks(acc, t, ldt, nr, &bx, 1);
+        __syncthreads();
+    }
+    wpublish_chunk(x, acc, 0, 2 * k * k + k * P.q);
+    if (!wreduce(x, 2 * k * k + k * P.q)) return false;
+    load_red(x, 2 * k * k, k, P.q, x.scr + SO_XTPSI, QW);
+    return true;
+}
+
+// W = [C RI | completion] (own moments); acc = [L^T W (k^2) | MRed^T diag(Dvec) W (q k)]
+static __device__ __noinline__ bool w_outscatter_basis(WCtx& x, const double* sig) {
+    const int k = x.r;
+    const DevProblem& P = x.P;
+    WSmem* sm = x.sm;
+    const SideInfo& si = x.side[1];
+    double* acc = sm->work;
+    double* Ri = sm->work + ACCW;
+    double* t = Ri + RA * RA;           // TRW x (3 RA + QW): [C | W_new | L | MRed D]
+    const int ldt = 3 * RA + QW;
+    const int rho = si.rho2;
+    if (rho > 0) g_copy(Ri, RA, sside(x, 1, SS_RI), RA, rho, rho);
+    w_acc_zero(acc, k * k + P.q * k);
+    const double* wc = sside(x, 1, SS_WC);
+    const GBlock bl[2] = {{2 * RA, k, RA, k, 0}, {3 * RA, P.q, RA, k, k * k}};
+    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+        const int nr = min(TRW, x.m1 - r0);
+        if (rho > 0) wload(t, ldt, 0, x.st.CW, RA, 0, r0, nr, rho);
+        wload(t, ldt, 2 * RA, x.st.L, RA, 0, r0, nr, k);
+        for (int e = threadIdx.x; e < nr * P.q; e += NT) {
+            const int r = e / P.q, kq = e - (e / P.q) * P.q;
+            const int m = r0 + r;
+            t[r * ldt + 3 * RA + kq] = P.mred[(size_t)m * P.q + kq] * sig[P.lof[m]];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * rho; e += NT) {
+            const int r = e / rho, j = e - (e / rho) * rho;
+            double a = 0.0;
+            for (int l = 0; l <= j; ++l) a = fma(t[r * ldt + l], Ri[l * RA + j], a);
+            t[r * ldt + RA + j] = a;
+        }
+        __syncthreads();
+        if (k > rho) {
+            for (int r = threadIdx.x; r < nr; r += NT) {
+                const int m = r0 + r;
+                double* row = t + r * ldt + RA;
+                for (int a = 0; a < k - rho; ++a) {
+                    const double* w = wc + a * WCS;
+                    double v = (m == sm->wcand[a]) ? 1.0 : 0.0;
+                    for (int j = 0; j < rho + a; ++j) v -= row[j] * w[j];
+                    row[rho + a] = v / sm->wnrm[a];
+                }
+            }
+            __syncthreads();
+        }
+        wstore(x.st.W, KA, 0, t, ldt, RA, r0, nr, k);
+        gram_blocks(acc, t, ldt, nr, bl, 2);
+        __syncthreads();
+    }
+    wpublish_chunk(x, acc, 0, k * k + P.q * k);
+    if (!wreduce(x, k * k + P.q * k)) return false;
+    // S = L^T W ; MtDW (q x k)
+    for (int e = threadIdx.x; e < KA * KA; e += NT) sm->S[e] = 0.0;
+    __syncthreads();
+    load_red(x, 0, k, k, sm->S, KA);
+    load_red(x, k * k, P.q, k, x.scr + SO_MTDW, KA);
+    return true;
+}
+
+// out-scattering (:1885-1890 / :2229-2234): L, W = orth(L) (plain range
+// finder on the angular side), S = L^T W and MtDW; X^T psi of the pre-zeroing X.
+static __device__ __noinline__ bool w_outscatter(WCtx& x, const double* sig) {
+    const int k = x.r;
+    if (!w_outscatter_pass(x, sig)) return false;
+    const bool only_w[2] = {false, true};
+    const bool plain[2] = {false, true};
+    if (!range_find(x, only_w, plain)) return false;
+    const int rho = x.side[1].rho2;
+    if (k > rho) w_complete_side(x, 0, rho, k - rho);
+    return w_outscatter_basis(x, sig);
+}
+
+// In-scattering K and L (:1905-1918): K = X S + dE psi MtDW (K[bnd] = 0),
+// L = W S^T + dE Dvec (MRed Xtpsi^T); Grams of [X K] and [W L]. With sbar:
+// Sbar = S + dE Xtpsi MtDW in scratch and the second dose half-step with
+// (X, Sbar, W) before truncation (parallel integrator, :1943).
+static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, bool sbar_dose, int dose_sidx) {
+    const int k = x.r;
+    const DevProblem& P = x.P;
+    WSmem* sm = x.sm;
+    const double dE = P.dE;
+    double* acc = sm->work;                   // 6 k^2
+    double* Mt = sm->work + 6 * RA * RA;      // q x k MtDW (ld KA)
+    double* Xp = Mt + QW * KA;                // k x q Xtpsi (ld QW)
+    double* t = Xp + KA * QW;                 // TRW x (2RA + QW)
+    const int ldt = 2 * RA + QW;
+    g_copy(Mt, KA, x.scr + SO_MTDW, KA, P.q, k);
+    g_copy(Xp, QW, x.scr + SO_XTPSI, QW, k, P.q);
+    double* Sb = x.scr + SO_SBAR;
+    if (sbar_dose) {
+        // Sbar = S + dE Xtpsi MtDW
+        for (int e = threadIdx.x; e < k * k; e += NT) {
+            const int i = e / k, j = e - (e / k) * k;
+            double a = 0.0;
+            for (int l = 0; l < P.q; ++l) a = fma(Xp[i * QW + l], Mt[l * KA + j], a);
+            Sb[i * RA + j] = sm->S[i * KA + j] + dE * a;
+        }
+        __syncthreads();
+        // v = Sbar W[0,:]^T
+        double* w0 = sm->vec + KA;
+        for (int j = threadIdx.x; j < k; j += NT) w0[j] = ldcg(x.st.W + j);
+        __syncthreads();
+        for (int i = threadIdx.x; i < k; i += NT) {
+            double a = 0.0;
+            for (int j = 0; j < k; ++j) a = fma(Sb[i * RA + j], w0[j], a);
+            sm->vec[i] = a;
+        }
+        __syncthreads();
+    }
+    w_acc_zero(acc, 6 * k * k);
+    const GBlock bl[3] = {{0, k, 0, k, 0}, {0, k, k, k, k * k}, {k, k, k, k, 2 * k * k}};
+    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
+        const int nr = min(TRW, x.c1 - r0);
+        wload(t, ldt, 0, x.st.X, KA, 0, r0, nr, k);
+        wload(t, ldt, 2 * RA, x.psi_in, QW, 0, r0, nr, P.q);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            double s = 0.0;
+            if (!is_bnd_w(P, r0 + r)) {
+                for (int l = 0; l < k; ++l) s = fma(t[r * ldt + l], sm->S[l * KA + j], s);
+                double a = 0.0;
+                for (int kq = 0; kq < P.q; ++kq) a = fma(t[r * ldt + 2 * RA + kq], Mt[kq * KA + j], a);
+                s += dE * a;
+            }
+            t[r * ldt + k + j] = s;
+        }
+        __syncthreads();
+        wstore(x.st.K, RA, 0, t, ldt, k, r0, nr, k);
+        gram_blocks(acc, t, ldt, nr, bl, 3);
+        __syncthreads();
+    }
+    if (sbar_dose) w_dose(x, dose_sidx, sm->vec, k, false);
+    const GBlock bw[3] = {{0, k, 0, k, 3 * k * k}, {0, k, k, k, 4 * k * k}, {k, k, k, k, 5 * k * k}};
+    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+        const int nr = min(TRW, x.m1 - r0);
+        wload(t, ldt, 0, x.st.W, KA, 0, r0, nr, k);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - (e / k) * k;
+            const int m = r0 + r;
+            double s = 0.0;
+            for (int l = 0; l < k; ++l) s = fma(t[r * ldt + l], sm->S[j * KA + l], s);
+            double a = 0.0;   // (MRed Xtpsi^T)[m][j]
+            for (int kq = 0; kq < P.q; ++kq) a = fma(P.mred[(size_t)m * P.q + kq], Xp[j * QW + kq], a);
+            t[r * ldt + k + j] = s + dE * sig[P.lof[m]] * a;
+        }
+        __syncthreads();
+        wstore(x.st.L, RA, 0, t, ldt, k, r0, nr, k);
+        gram_blocks(acc, t, ldt, nr, bw, 3);
+        __syncthreads();
+    }
+    wpublish_chunk(x, acc, 0, 6 * k * k);
+    return wreduce(x, 6 * k * k);
+}
+
+// X[bnd,:] = 0 for own cells (only this CTA reads these rows until the next barrier)
+__device__ inline void w_zero_bnd(WCtx& x) {
+    const int k = x.r;
+    for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT)
+        if (is_bnd_w(x.P, c))
+            for (int j = 0; j < k; ++j) x.st.X[(size_t)c * KA + j] = 0.0;
+    __syncthreads();
+}
+
+// Grams over the new directions for the parallel integrator's augmented S:
+// red [X~^T K (k^2) | L^T W~ (k^2)]
+static __device__ __noinline__ bool w_parallel_blocks(WCtx& x) {
+    const int k = x.r;
+    double* acc = x.sm->work;
+    double* t = x.sm->work + ACCW;   // TRW x 2RA
+    w_acc_zero(acc, 2 * k * k);
+    const GBlock bx{0, k, k, k, 0};        // X~^T K
+    const GBlock bw{k, k, 0, k, k * k};    // L^T W~
+    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
+        const int nr = min(TRW, x.c1 - r0);
+        wload(t, 2 * RA, 0, x.st.X, KA, k, r0, nr, k);
+        wload(t, 2 * RA, k, x.st.K, RA, 0, r0, nr, k);
+        __syncthreads();
+        gram_blocks(acc, t, 2 * RA, nr, &bx, 1);
+        __syncthreads();
+    }
+    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+        const int nr = min(TRW, x.m1 - r0);
+        wload(t, 2 * RA, 0, x.st.W, KA, k, r0, nr, k);
+        wload(t, 2 * RA, k, x.st.L, RA, 0, r0, nr, k);
+        __syncthreads();
+        gram_blocks(acc, t, 2 * RA, nr, &bw, 1);
+        __syncthreads();
+    }
+    wpublish_chunk(x, acc, 0, 2 * k * k);
+    return wreduce(x, 2 * k * k);
+}
+
+// Build the parallel integrator's augmented S (:1881-1885) in transposed
+// storage at work[0]: S_new = [[Sbar, L^T W~], [X~^T K, 0]].
+static __device__ __noinline__ void w_parallel_snew(WCtx& x) {
+    const int k = x.r, m = 2 * k;
+    double* At = x.sm->work;
+    const double* Sb = x.scr + SO_SBAR;
+    for (int e = threadIdx.x; e < m * m; e += NT) {
+        const int i = e / m, j = e - (e / m) * m;   // S_new[i][j] -> At[j][i]
+        double v;
+        if (i < k && j < k) v = Sb[i * RA + j];
+        else if (i < k) v = ldcg(x.redp + k * k + i * k + (j - k));        // (L^T W~)[i][j-k]
+        else if (j < k) v = ldcg(x.redp + (i - k) * k + j);                // (X~^T K)[i-k][j]
+        else v = 0.0;
+        At[j * KA + i] = v;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- kernel ---
+template <int METHOD>
+__global__ void __launch_bounds__(NT, 1)
+adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, int max_iters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WSmem* sm = reinterpret_cast<WSmem*>(smem_raw);
+    WCtx x;
+    x.P = P;
+    x.G = G;
+    x.b = blockIdx.x;
+    x.st = states[0];
+    x.sm = sm;
+    x.scr = x.st.scr + (size_t)x.b * SCRW;
+    x.prof = (blockIdx.x == 0) ? P.prof : nullptr;
+    x.gen = 0;
+    x.parity = 0;
+    x.redp = x.st.red;
+    x.cur_n = 0;
+    ProfScope ps_total(x.prof, PF_TOTAL);
+    x.c0 = (int)((long long)x.b * P.n / G);
+    x.c1 = (int)((long long)(x.b + 1) * P.n / G);
+    x.m0 = (int)((long long)x.b * P.N / G);
+    x.m1 = (int)((long long)(x.b + 1) * P.N / G);
+    x.r = ldcg(x.st.info + 0);
+    int psi_idx = ldcg(x.st.info + 2);
+    for (int e = threadIdx.x; e < KA * KA; e += NT) sm->S[e] = ldcg(x.st.S + e);
+    __syncthreads();
+    double t = ldcg(x.st.tvar);
+    int iters = 0;
+    int eta_count = ldcg(x.st.info + 4);
+    const double dE = P.dE;
+    const int nE = P.nE;
+    bool aborted = false;
+    // METHOD 1 iterates n = n_begin..n_end; METHOD 2 runs the BUG while-loop
+    int n = n_begin - 1;
+    while (true) {
+        n += 1;
+        if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
+            if (n > n_end) break;
+        } else {
+            if (!(t < nE * dE)) break;
+            if (n == nE || n > n_end) break;
+        }
+        if (iters >= max_iters) break;
+        x.cur_n = n;
+        x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
+        x.psi_out = psi_idx ? x.st.psi0 : x.st.psi1;
+        const double* sig = P.sigma + (size_t)(n - 1) * (P.npn + 1);
+        if (METHOD == TITUS_BUG_ADAPTIVE && x.b == 0 && threadIdx.x == 0 && iters < x.st.hist_cap) {
+            x.st.rank_hist[iters] = x.r;
+            x.st.time_hist[iters] = (double)n;   // energy index (eGrid[n-1] on the host)
+        }
+        ++iters;
+        // ---- A, B
+        w_phase_A(x, n);
+        if (!wsync(x)) { aborted = true; break; }
+        w_sweep(x, sig[0]);
+        const bool stream = n > 2;
+        if (stream) {
+            if (!w_stream_grams(x)) { aborted = true; break; }
+        } else if (!wsync(x)) {
+            aborted = true;
+            break;
+        }
+        psi_idx ^= 1;
+        x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
+        if (stream) {
+            const int k = x.r;
+            w_stream_small(x, METHOD == TITUS_PARALLEL_ADAPTIVE);
+            if (!w_phase_C(x)) { aborted = true; break; }
+            if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
+                if (!augment(x, false)) { aborted = true; break; }
+                if (!w_parallel_blocks(x)) { aborted = true; break; }
+                w_parallel_snew(x);
+                const int kk = w_truncate_svd(x, 2 * k);
+                w_truncate_apply(x, 2 * k, kk, -1, nullptr);
+                if (kk > RA) {
+                    if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                    aborted = true;
+                    break;
+                }
+            } else {
+                // BUG streaming: X1 = [Q1 X~], W1 = [Q1_W W~]; S = Mu S Nu^T
+                if (!augment(x, true)) { aborted = true; break; }
+                if (!wsync(x)) { aborted = true; break; }
+                const int m = 2 * k;
+                // S2 = blockdiag(M1 S N1^T, 0) in shared S (ld KA)
+                double* T = sm->work;
+                double* U = sm->work + RA * RA;
+                g_mm(T, RA, sside(x, 0, SS_M1), RA, false, sm->S, KA, false, k, k, k);
+                g_mm(U, RA, T, RA, false, sside(x, 1, SS_M1), RA, true, k, k, k);
+                for (int e = threadIdx.x; e < KA * KA; e += NT) {
+                    const int i = e / KA, j = e - (e / KA) * KA;
+                    sm->S[e] = (i < k && j < k) ? U[i * RA + j] : 0.0;
+                }
+                __syncthreads();
+                // S-step Grams with the 2k-wide bases, two operators per chunk
+                double* acc = sm->work;
+                double* F = sm->work + ACCW;
+                const int mm = m * m;
+                for (int d = 0; d < 4; ++d) {   // one operator per chunk: 2 m^2 <= ACCW
+                    w_acc_zero(acc, 2 * mm);
+                    w_grams_pass(x, x.st.X, x.st.W, m, d, d + 1, 0, acc, F);
+                    wpublish_chunk(x, acc, d * mm, mm);             // X side G_d
+                    wpublish_chunk(x, acc + mm, (4 + d) * mm, mm);  // W side C_d
+                    __syncthreads();
+                }
+                if (!wreduce(x, 8 * mm)) { aborted = true; break; }
+                // Sup = S2 - dE sum_d G_d S2 C_d ; eta from the [k:, k:] block
+                double* Gd = x.scr + SO_TMP;
+                double* Cd = Gd + KA * KA;
+                double* Tm = sm->work;                 // m x m
+                double* Um = sm->work + KA * KA;       // m x m
+                double* Sup = x.scr + SO_TMP + 2 * KA * KA;
+                g_copy(Sup, KA, sm->S, KA, m, m);
+                double* E = sm->work + 2 * KA * KA;    // k x k eta accumulator
+                g_zero(E, RA, k, k);
+                for (int d = 0; d < 4; ++d) {
+                    load_red(x, d * mm, m, m, Gd, KA);
+                    load_red(x, (4 + d) * mm, m, m, Cd, KA);
+                    g_mm(Tm, KA, sm->S, KA, false, Cd, KA, false, m, m, m);
+                    g_mm(Um, KA, Gd, KA, false, Tm, KA, false, m, m, m);
+                    for (int e = threadIdx.x; e < m * m; e += NT) {
+                        const int i = e / m, j = e - (e / m) * m;
+                        Sup[i * KA + j] -= dE * Um[i * KA + j];
+                        if (i >= k && j >= k) E[(i - k) * RA + (j - k)] += Um[i * KA + j];
+                    }
+                    __syncthreads();
+                }
+                double eta2 = 0.0, sup2 = 0.0;
+                for (int e = 0; e < k * k; ++e) eta2 += E[(e / k) * RA + e % k] * E[(e / k) * RA + e % k];
+                for (int e = 0; e < m * m; ++e) sup2 += Sup[(e / m) * KA + e % m] * Sup[(e / m) * KA + e % m];
+                // truncate Sup
+                double* At = sm->work;
+                __syncthreads();
+                for (int e = threadIdx.x; e < m * m; e += NT) {
+                    const int i = e / m, j = e - (e / m) * m;
+                    At[j * KA + i] = Sup[i * KA + j];
+                }
+                __syncthreads();
+                const int kk = w_truncate_svd(x, m);
+                bool repeat = false;
+                if (kk == 2 * k && 2 * k < P.r) {
+                    repeat = true;   // accept the truncation, redo this energy (n = n-1 without continue)
+                } else {
+                    const double eta = sqrt(eta2);
+                    const double bound = P.c_eta * P.theta * fmax(1e-7, pow(sqrt(sup2), P.theta_index)) / dE;
+                    if (x.b == 0 && threadIdx.x == 0 && eta_count < x.st.hist_cap) {
+                        x.st.eta_hist[eta_count] = eta;
+                        x.st.bound_hist[eta_count] = bound;
+                    }
+                    ++eta_count;
+                    if (eta > bound && 2 * k < P.r) {
+                        // reject: keep X1, S2, W1 with rank 2k and repeat energy n
+                        x.r = 2 * k;
+                        n -= 1;
+                        if (x.r > RA) {
+                            if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                            aborted = true;
+                            break;
+                        }
+                        continue;
+                    }
+                }
+                w_truncate_apply(x, m, kk, -1, nullptr);
+                if (repeat) n -= 1;
+                if (x.r > RA) {
+                    if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                    aborted = true;
+                    break;
+                }
+            }
+        }
+        // ---- out-scattering
+        if (!w_outscatter(x, sig)) { aborted = true; break; }
+        // ---- in-scattering
+        w_zero_bnd(x);
+        {
+            const int k = x.r;
+            if (!w_inscatter_KL(x, sig, METHOD == TITUS_PARALLEL_ADAPTIVE, n - 1)) { aborted = true; break; }
+            if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
+                if (!augment(x, false)) { aborted = true; break; }
+                if (!w_parallel_blocks(x)) { aborted = true; break; }
+                w_parallel_snew(x);
+                const int kk = w_truncate_svd(x, 2 * k);
+                w_truncate_apply(x, 2 * k, kk, -1, nullptr);
+                if (kk > RA) {
+                    if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                    aborted = true;
+                    break;
+                }
+                if (x.b == 0 && threadIdx.x == 0) {
+                    if (n - 1 < x.st.hist_cap) {
+                        x.st.rank_hist[n - 1] = x.r;
+                        x.st.time_hist[n - 1] = t;
+                    }
+                }
+                t += dE;
+            } else {
+                const int m = 2 * k;
+                if (!augment(x, true)) { aborted = true; break; }
+                // Grams X1^T psi (m x q) and MRed^T D W1 (q x m) over the new bases
+                double* acc = sm->work;
+                double* tt = sm->work + ACCW;
+                const int ldt = KA + QW;
+                w_acc_zero(acc, 2 * m * P.q + m);
+                const GBlock bx{0, m, KA, P.q, 0};
+                for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
+                    const int nr = min(TRW, x.c1 - r0);
+                    // own rows of X1 were just written by this CTA
+                    wload(tt, ldt, 0, x.st.X, KA, 0, r0, nr, m);
+                    wload(tt, ldt, KA, x.psi_in, QW, 0, r0, nr, P.q);
+                    __syncthreads();
+                    gram_blocks(acc, tt, ldt, nr, &bx, 1);
+                    __syncthreads();
+                }
+                const GBlock bw{KA, P.q, 0, m, m * P.q};
+                for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
+                    const int nr = min(TRW, x.m1 - r0);
+                    wload(tt, ldt, 0, x.st.W, KA, 0, r0, nr, m);
+                    for (int e = threadIdx.x; e < nr * P.q; e += NT) {
+                        const int r = e / P.q, kq = e - (e / P.q) * P.q;
+                        const int mo = r0 + r;
+                        tt[r * ldt + KA + kq] = P.mred[(size_t)mo * P.q + kq] * sig[P.lof[mo]];
+                    }
+                    __syncthreads();
+                    gram_blocks(acc, tt, ldt, nr, &bw, 1);
+                    __syncthreads();
+                }
+                // row 0 of W1 travels through the reduction (only its owner adds it)
+                if (x.m0 == 0 && x.m1 > 0)
+                    for (int j = threadIdx.x; j < m; j += NT) acc[2 * m * P.q + j] = ldcg(x.st.W + j);
+                __syncthreads();
+                wpublish_chunk(x, acc, 0, 2 * m * P.q + m);
+                if (!wreduce(x, 2 * m * P.q + m)) { aborted = true; break; }
+                double* Xp = x.scr + SO_XTPSI;   // m x q (ld QW)
+                double* Mt = x.scr + SO_MTDW;    // q x m (ld KA)
+                load_red(x, 0, m, P.q, Xp, QW);
+                load_red(x, m * P.q, P.q, m, Mt, KA);
+                load_red(x, 2 * m * P.q, 1, m, x.scr + SO_TMP, KA);
+                // S2 = blockdiag(M1 S N1^T, 0); Sup = S2 + dE Xtpsi MtDW
+                double* T = sm->work;
+                double* U = sm->work + RA * RA;
+                g_mm(T, RA, sside(x, 0, SS_M1), RA, false, sm->S, KA, false, k, k, k);
+                g_mm(U, RA, T, RA, false, sside(x, 1, SS_M1), RA, true, k, k, k);
+                for (int e = threadIdx.x; e < KA * KA; e += NT) {
+                    const int i = e / KA, j = e - (e / KA) * KA;
+                    sm->S[e] = (i < k && j < k) ? U[i * RA + j] : 0.0;
+                }
+                __syncthreads();
+                double* At = sm->work;
+                for (int e = threadIdx.x; e < m * m; e += NT) {
+                    const int i = e / m, j = e - (e / m) * m;
+                    double a = 0.0;
+                    for (int l = 0; l < P.q; ++l) a = fma(Xp[i * QW + l], Mt[l * KA + j], a);
+                    At[j * KA + i] = sm->S[i * KA + j] + dE * a;
+                }
+                __syncthreads();
+                // eta = ||Xtpsi[k:, :] MtDW[:, k:]||_F
+                double eta2 = 0.0;
+                for (int e = 0; e < k * k; ++e) {
+                    const int i = k + e / k, j = k + e % k;
+                    double a = 0.0;
+                    for (int l = 0; l < P.q; ++l) a = fma(Xp[i * QW + l], Mt[l * KA + j], a);
+                    eta2 += a * a;
+                }
+                const int kk = w_truncate_svd(x, m);
+                bool repeat = false;
+                if (kk == 2 * k && 2 * k < P.r) {
+                    repeat = true;
+                } else {
+                    double s2 = 0.0;
+                    for (int j = 0; j < kk; ++j) s2 += sm->sig[j] * sm->sig[j];
+                    const double eta = sqrt(eta2);
+                    const double bound = P.c_eta * P.theta * fmax(1e-7, pow(sqrt(s2), P.theta_index)) / dE;
+                    if (eta > bound && 2 * k < P.r) {
+                        x.r = 2 * k;
+                        n -= 1;
+                        if (x.r > RA) {
+                            if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                            aborted = true;
+                            break;
+                        }
+                        continue;
+                    }
+                }
+                w_truncate_apply(x, m, kk, n - 1, x.scr + SO_TMP);
+                if (repeat) n -= 1;
+                if (x.r > RA) {
+                    if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                    aborted = true;
+                    break;
+                }
+                t += dE;
+            }
+        }
+        // the truncation rewrote X and W rows without a team barrier; the next
+        // step's first dose half-step reads W's row 0 owned by another CTA
+        if (!wsync(x)) {
+            aborted = true;
+            break;
+        }
+    }
+    if (x.b == 0) {
+        for (int e = threadIdx.x; e < KA * KA; e += NT) x.st.S[e] = sm->S[e];
+        if (threadIdx.x == 0) {
+            x.st.info[0] = x.r;
+            x.st.info[1] = iters;
+            x.st.info[2] = psi_idx;
+            x.st.info[3] = n;   // first energy index not processed
+            x.st.info[4] = eta_count;
+            x.st.tvar[0] = t;
+        }
+    }
+    (void)aborted;
+}
+
+}  // namespace wide
+}  // namespace titus

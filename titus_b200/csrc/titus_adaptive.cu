@@ -1,0 +1,277 @@
+// Host side of the rank-adaptive integrators (TITUS_PARALLEL_ADAPTIVE,
+// TITUS_BUG_ADAPTIVE): device state, initial factors, launch and result copy.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "titus_handle.h"
+#include "dlr_adaptive.cuh"
+
+using namespace titus;
+using namespace titus::wide;
+using titus_host::fail;
+
+namespace {
+
+int ensure_state(titus_solver* s) {
+    if (s->d_wst) return TITUS_OK;
+    WideState& w = s->wst;
+    const int n = s->n, N = s->N, G = s->num_sms;
+    int rc;
+    w.hist_cap = 4 * s->nE + 64;
+    if ((rc = s->walloc(&w.X, (size_t)n * KA)) || (rc = s->walloc(&w.W, (size_t)N * KA)) ||
+        (rc = s->walloc(&w.K, (size_t)n * RA)) || (rc = s->walloc(&w.KP, (size_t)n * RA)) ||
+        (rc = s->walloc(&w.CX, (size_t)n * RA)) || (rc = s->walloc(&w.L, (size_t)N * RA)) ||
+        (rc = s->walloc(&w.LP, (size_t)N * RA)) || (rc = s->walloc(&w.CW, (size_t)N * RA)) ||
+        (rc = s->walloc(&w.psi0, (size_t)n * QW)) || (rc = s->walloc(&w.psi1, (size_t)n * QW)) ||
+        (rc = s->walloc(&w.dose, (size_t)n)) || (rc = s->walloc(&w.S, (size_t)KA * KA)) ||
+        (rc = s->walloc(&w.part, (size_t)2 * G * PMAXW)) || (rc = s->walloc(&w.red, (size_t)2 * PMAXW)) ||
+        (rc = s->walloc(&w.scr, (size_t)G * SCRW)) || (rc = s->walloc(&w.bar, (size_t)G + 1)) ||
+        (rc = s->walloc(&w.status, 1)) || (rc = s->walloc(&w.info, 8)) || (rc = s->walloc(&w.diag, 16)) ||
+        (rc = s->walloc(&w.tvar, 1)) || (rc = s->walloc(&w.rank_hist, (size_t)w.hist_cap)) ||
+        (rc = s->walloc(&w.time_hist, (size_t)w.hist_cap)) || (rc = s->walloc(&w.eta_hist, (size_t)w.hist_cap)) ||
+        (rc = s->walloc(&w.bound_hist, (size_t)w.hist_cap)))
+        return rc;
+    if ((rc = s->walloc(&s->d_wst, 1))) return rc;
+    CK(cudaMemcpy(s->d_wst, &w, sizeof(WideState), cudaMemcpyHostToDevice));
+    CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(WSmem)));
+    CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_BUG_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(WSmem)));
+    return TITUS_OK;
+}
+
+// Initial factors (SolverCSD.jl:1728-1760, :2013-2050): r0 = floor(settings.r / 2)
+// identity columns, X's boundary rows zeroed, S = 0.
+__global__ void wide_init_kernel(WideState* states, int n, int N, int nx, int ny, int r0, int hist_cap) {
+    WideState st = states[0];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < r0; j += gridDim.x * blockDim.x) {
+        if (j < n) {
+            const int i = j / ny, jj = j % ny;
+            const bool bnd = (i == 0 || jj == 0 || i == nx - 1 || jj == ny - 1);
+            st.X[(size_t)j * KA + j] = bnd ? 0.0 : 1.0;
+        }
+        if (j < N) st.W[(size_t)j * KA + j] = 1.0;
+    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < hist_cap; e += gridDim.x * blockDim.x) {
+        st.rank_hist[e] = -1;
+        st.time_hist[e] = 0.0;
+        st.eta_hist[e] = 0.0;
+        st.bound_hist[e] = 0.0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st.info[0] = r0;
+        st.info[1] = 0;
+        st.info[2] = 0;
+        st.info[3] = 2;
+        st.info[4] = 0;
+        st.tvar[0] = 0.0;
+    }
+}
+
+__global__ void wide_mark_rank0(WideState* states, int r0) {
+    // the parallel integrator's rVec starts with r0 in every column (:1731); index 0 is never overwritten
+    if (threadIdx.x == 0) states[0].rank_hist[0] = r0;
+}
+
+int init_state(titus_solver* s, int r0, int method, cudaStream_t stream) {
+    WideState& w = s->wst;
+    const int n = s->n, N = s->N;
+    CK(cudaMemsetAsync(w.X, 0, (size_t)n * KA * sizeof(double), stream));
+    CK(cudaMemsetAsync(w.W, 0, (size_t)N * KA * sizeof(double), stream));
+    CK(cudaMemsetAsync(w.S, 0, (size_t)KA * KA * sizeof(double), stream));
+    CK(cudaMemsetAsync(w.psi0, 0, (size_t)n * QW * sizeof(double), stream));
+    CK(cudaMemsetAsync(w.psi1, 0, (size_t)n * QW * sizeof(double), stream));
+    CK(cudaMemsetAsync(w.dose, 0, (size_t)n * sizeof(double), stream));
+    wide_init_kernel<<<4, 256, 0, stream>>>(s->d_wst, n, N, s->P.nx, s->P.ny, r0, w.hist_cap);
+    CK(cudaGetLastError());
+    if (method == TITUS_PARALLEL_ADAPTIVE) {
+        wide_mark_rank0<<<1, 32, 0, stream>>>(s->d_wst, r0);
+        CK(cudaGetLastError());
+    }
+    return TITUS_OK;
+}
+
+int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin, int n_end, int max_iters,
+           cudaStream_t stream) {
+    int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : std::min(s->num_sms, 64);
+    G = std::max(1, std::min(G, s->num_sms));
+    int per_sm = 0;
+    auto kern = method == TITUS_PARALLEL_ADAPTIVE ? (void*)adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>
+                                                  : (void*)adaptive_kernel<TITUS_BUG_ADAPTIVE>;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm,
+        method == TITUS_PARALLEL_ADAPTIVE ? adaptive_kernel<TITUS_PARALLEL_ADAPTIVE> : adaptive_kernel<TITUS_BUG_ADAPTIVE>,
+        wide::NT, sizeof(WSmem)));
+    if (per_sm < 1) return fail(TITUS_ERR_CUDA, "adaptive kernel does not fit on an SM (smem %zu)", sizeof(WSmem));
+    G = std::min(G, per_sm * s->num_sms);
+    DevProblem P = s->P;
+    if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
+    P.prof = nullptr;
+    P.zero_smem = 0;
+    if (opt && opt->profile) {
+        CK(cudaMemsetAsync(s->prof, 0, 16 * sizeof(unsigned long long), stream));
+        P.prof = s->prof;
+    }
+    WideState& w = s->wst;
+    CK(cudaMemsetAsync(w.bar, 0, (size_t)(s->num_sms + 1) * sizeof(unsigned), stream));
+    CK(cudaMemsetAsync(w.status, 0, sizeof(int), stream));
+    CK(cudaMemsetAsync(w.diag, 0, 16 * sizeof(double), stream));
+    WideState* dst = s->d_wst;
+    void* args[] = {&P, &dst, &G, &n_begin, &n_end, &max_iters};
+    CK(cudaLaunchCooperativeKernel(kern, dim3(G), dim3(wide::NT), args, sizeof(WSmem), stream));
+    s->last_G = G;
+    s->wide_state_valid = 1;
+    return TITUS_OK;
+}
+
+int check_status(titus_solver* s) {
+    CK(cudaDeviceSynchronize());
+    int status = 0;
+    CK(cudaMemcpy(&status, s->wst.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status == 0) return TITUS_OK;
+    double d[16];
+    CK(cudaMemcpy(d, s->wst.diag, sizeof(d), cudaMemcpyDeviceToHost));
+    int info[8];
+    CK(cudaMemcpy(info, s->wst.info, sizeof(info), cudaMemcpyDeviceToHost));
+    const char* what = status == ST_BARRIER_TIMEOUT  ? "team barrier timeout"
+                       : status == ST_CHOL_BREAKDOWN ? "Cholesky breakdown"
+                       : status == ST_COMPLETION     ? "basis completion ran out of candidates"
+                       : status == ST_JACOBI         ? "Jacobi eigensolver did not converge"
+                       : status == ST_LIMIT          ? "rank exceeds the adaptive kernel's capacity"
+                       : status == ST_UNSUPPORTED    ? "angular basis not orthonormal (cannot complete)"
+                       : status == ST_SVD            ? "Jacobi SVD did not converge"
+                                                     : "device error";
+    const int code = status == ST_LIMIT ? TITUS_ERR_LIMIT : TITUS_ERR_DEVICE;
+    if (status == ST_SVD) {
+        // statistics of the matrix handed to the SVD (CTA 0's copy)
+        std::vector<double> a((size_t)KA * KA);
+        CK(cudaMemcpy(a.data(), s->wst.scr + SO_DBG, a.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        const int m = (int)d[2];
+        int nonfinite = 0, zeros = 0;
+        double amax = 0.0, amin = INFINITY;
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                const double v = a[(size_t)i * KA + j];
+                if (!std::isfinite(v)) ++nonfinite;
+                else if (v == 0.0) ++zeros;
+                else {
+                    amax = std::max(amax, std::fabs(v));
+                    amin = std::min(amin, std::fabs(v));
+                }
+            }
+        std::string row;
+        for (int j = 0; j < std::min(m, 8); ++j) row += std::to_string(a[j]) + " ";
+        return fail(code, "device status %d: %s (m %d at step %g; input: %d non-finite, %d zeros, |a| in [%.3e, %.3e]; "
+                    "column 0: %s)", status, what, m, d[7], nonfinite, zeros, amin, amax, row.c_str());
+    }
+    return fail(code, "device status %d: %s (rank cap %d, adaptive width %d; diag %g %g %g step %g)", status, what,
+                RA, KA, d[0], d[2], d[3], d[7]);
+}
+
+}  // namespace
+
+int titus_host::wide_solve_device(titus_solver* s, int method, const titus_options_t* opt, cudaStream_t stream) {
+    int rc = ensure_state(s);
+    if (rc) return rc;
+    const int r0 = s->r / 2;
+    if (r0 < 1) return fail(TITUS_ERR_ARG, "adaptive integrators need settings.r >= 2 (got %d)", s->r);
+    if (r0 > RA) return fail(TITUS_ERR_LIMIT, "initial rank %d > %d", r0, RA);
+    if (2 * r0 > s->N) return fail(TITUS_ERR_ARG, "augmented width %d exceeds the %d moments", 2 * r0, s->N);
+    if ((rc = init_state(s, r0, method, stream))) return rc;
+    int n_end = s->nE;
+    int max_iters = INT_MAX;
+    if (opt && opt->max_steps > 0) {
+        if (method == TITUS_PARALLEL_ADAPTIVE) n_end = std::min(n_end, 1 + opt->max_steps);
+        else max_iters = opt->max_steps;
+    }
+    return launch(s, method, opt, 2, n_end, max_iters, stream);
+}
+
+int titus_host::wide_solve_from(titus_solver* s, int method, const titus_options_t* opt, int n_stop) {
+    if (!s->d_wst || !s->wide_state_valid) return fail(TITUS_ERR_ARG, "no adaptive state to resume (call titus_set_state)");
+    int info[8];
+    CK(cudaMemcpy(info, s->wst.info, sizeof(info), cudaMemcpyDeviceToHost));
+    const int n_begin = info[3];
+    int n_end = std::min(n_stop, s->nE);
+    int max_iters = INT_MAX;
+    if (opt && opt->max_steps > 0) {
+        if (method == TITUS_PARALLEL_ADAPTIVE) n_end = std::min(n_end, n_begin + opt->max_steps - 1);
+        else max_iters = opt->max_steps;
+    }
+    if (n_end < n_begin) return fail(TITUS_ERR_ARG, "nothing to run (n_begin %d, n_stop %d)", n_begin, n_stop);
+    return launch(s, method, opt, n_begin, n_end, max_iters, nullptr);
+}
+
+int titus_host::wide_fetch(titus_solver* s, titus_result_t* res) {
+    int rc = check_status(s);
+    if (rc) return rc;
+    WideState& w = s->wst;
+    int info[8];
+    CK(cudaMemcpy(info, w.info, sizeof(info), cudaMemcpyDeviceToHost));
+    const int k = info[0];
+    res->rank = k;
+    res->steps_done = info[1];
+    if (res->dose) CK(cudaMemcpy(res->dose, w.dose, s->n * sizeof(double), cudaMemcpyDeviceToHost));
+    const int cap = res->r_cap;
+    if ((res->X || res->S || res->W) && cap < k) return fail(TITUS_ERR_ARG, "r_cap %d < rank %d", cap, k);
+    if (res->X)
+        CK(cudaMemcpy2D(res->X, cap * sizeof(double), w.X, KA * sizeof(double), k * sizeof(double), s->n,
+                        cudaMemcpyDeviceToHost));
+    if (res->W)
+        CK(cudaMemcpy2D(res->W, cap * sizeof(double), w.W, KA * sizeof(double), k * sizeof(double), s->N,
+                        cudaMemcpyDeviceToHost));
+    if (res->S)
+        CK(cudaMemcpy2D(res->S, cap * sizeof(double), w.S, KA * sizeof(double), k * sizeof(double), k,
+                        cudaMemcpyDeviceToHost));
+    if (res->psi) {
+        double* src = info[2] ? w.psi1 : w.psi0;
+        CK(cudaMemcpy2D(res->psi, s->q * sizeof(double), src, QW * sizeof(double), s->q * sizeof(double), s->n,
+                        cudaMemcpyDeviceToHost));
+    }
+    const int nh = std::min(s->nE, w.hist_cap);
+    if (res->rank_history) CK(cudaMemcpy(res->rank_history, w.rank_hist, nh * sizeof(int), cudaMemcpyDeviceToHost));
+    if (res->time_history) CK(cudaMemcpy(res->time_history, w.time_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
+    if (res->eta_history) CK(cudaMemcpy(res->eta_history, w.eta_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
+    if (res->bound_history)
+        CK(cudaMemcpy(res->bound_history, w.bound_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
+    return TITUS_OK;
+}
+
+int titus_host::wide_set_state(titus_solver* s, int rank, const double* X, const double* S, const double* W,
+                               const double* psi, const double* dose, int n_next) {
+    int rc = ensure_state(s);
+    if (rc) return rc;
+    WideState& w = s->wst;
+    CK(cudaMemset(w.X, 0, (size_t)s->n * KA * sizeof(double)));
+    CK(cudaMemset(w.W, 0, (size_t)s->N * KA * sizeof(double)));
+    CK(cudaMemset(w.S, 0, (size_t)KA * KA * sizeof(double)));
+    CK(cudaMemcpy2D(w.X, KA * sizeof(double), X, rank * sizeof(double), rank * sizeof(double), s->n,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemcpy2D(w.W, KA * sizeof(double), W, rank * sizeof(double), rank * sizeof(double), s->N,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemcpy2D(w.S, KA * sizeof(double), S, rank * sizeof(double), rank * sizeof(double), rank,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemset(w.psi0, 0, (size_t)s->n * QW * sizeof(double)));
+    CK(cudaMemcpy2D(w.psi0, QW * sizeof(double), psi, s->q * sizeof(double), s->q * sizeof(double), s->n,
+                    cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(w.dose, dose, s->n * sizeof(double), cudaMemcpyHostToDevice));
+    int info[8] = {rank, 0, 0, n_next, 0, 0, 0, 0};
+    CK(cudaMemcpy(w.info, info, sizeof(info), cudaMemcpyHostToDevice));
+    // pseudo-time after the energies 2..n_next-1 (the loop condition t < nE dE)
+    const double t = (n_next - 2) * s->P.dE;
+    CK(cudaMemcpy(w.tvar, &t, sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemset(w.rank_hist, 0xff, w.hist_cap * sizeof(int)));
+    s->wide_state_valid = 1;
+    return TITUS_OK;
+}
+
+void titus_host::wide_free(titus_solver* s) {
+    for (void* p : s->wide_allocs) cudaFree(p);
+    s->wide_allocs.clear();
+    s->d_wst = nullptr;
+}

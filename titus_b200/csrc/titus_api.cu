@@ -9,17 +9,18 @@
 #include <string>
 #include <vector>
 
-#include "../../include/titus.h"
+#include "titus_handle.h"
 #include "dlr_fixed.cuh"
 
 using namespace titus;
+using titus_host::fail;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
-int fail(int code, const char* fmt, ...) {
-    char buf[512];
+int titus_host::fail(int code, const char* fmt, ...) {
+    char buf[768];
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(buf, sizeof(buf), fmt, ap);
@@ -28,49 +29,10 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define CK(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess) return fail(TITUS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
-
-template <class T>
-int upload(T** dptr, const T* host, size_t count) {
-    *dptr = nullptr;
-    if (count == 0) return TITUS_OK;
-    CK(cudaMalloc((void**)dptr, count * sizeof(T)));
-    if (host) CK(cudaMemcpy(*dptr, host, count * sizeof(T), cudaMemcpyHostToDevice));
-    return TITUS_OK;
+titus_solver::~titus_solver() {
+    titus_host::wide_free(this);
+    for (void* p : allocs) cudaFree(p);
 }
-
-}  // namespace
-
-struct titus_solver {
-    DevProblem P{};
-    int n = 0, N = 0, q = 0, nE = 0;
-    std::vector<void*> allocs;
-    // single-team state
-    TeamState st{};
-    TeamState* d_st = nullptr;
-    int team_ctas = 0;
-    int device = 0;
-    int num_sms = 0;
-    int r = 0;
-    int last_method = -1;
-    int last_G = 0;
-    unsigned long long* prof = nullptr;
-    int clock_khz = 0;
-
-    template <class T>
-    int alloc(T** p, size_t count, const T* host = nullptr) {
-        int rc = upload(p, host, count);
-        if (rc == TITUS_OK && *p) allocs.push_back((void*)*p);
-        return rc;
-    }
-    ~titus_solver() {
-        for (void* p : allocs) cudaFree(p);
-    }
-};
 
 static int validate(const titus_problem_t* pb) {
     if (!pb) return fail(TITUS_ERR_ARG, "problem is NULL");
@@ -83,7 +45,8 @@ static int validate(const titus_problem_t* pb) {
         return fail(TITUS_ERR_LIMIT, "n_ordinates %d > %d supported", pb->n_ordinates, std::min(QM, KM));
     if (pb->n_energies < 2) return fail(TITUS_ERR_ARG, "n_energies < 2");
     if (pb->r < 1) return fail(TITUS_ERR_ARG, "r < 1");
-    if (pb->r > KM) return fail(TITUS_ERR_LIMIT, "rank %d > %d supported by this build", pb->r, KM);
+    if (pb->r > 2 * wide::RA)
+        return fail(TITUS_ERR_LIMIT, "rank cap %d > %d supported by this build", pb->r, 2 * wide::RA);
     if (pb->r > pb->n_moments) return fail(TITUS_ERR_ARG, "r %d > n_moments %d", pb->r, pb->n_moments);
     if (!(pb->dx > 0) || !(pb->dy > 0)) return fail(TITUS_ERR_ARG, "dx, dy must be > 0");
     const void* req[] = {pb->density, pb->e_trafo, pb->stopping, pb->bc_energy, pb->sigma,
@@ -275,8 +238,9 @@ static int init_state(titus_solver* s, int r, cudaStream_t stream) {
 
 static int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin, int n_end, int dose2_pending,
                   cudaStream_t stream) {
-    if (method != TITUS_DLR_FIXED)
-        return fail(TITUS_ERR_ARG, "method %d is not available in this build (fixed-rank only)", method);
+    if (method != TITUS_DLR_FIXED) return fail(TITUS_ERR_ARG, "unknown method %d", method);
+    if (s->r > KM)
+        return fail(TITUS_ERR_LIMIT, "fixed-rank integrator: rank %d > %d supported by this build", s->r, KM);
     int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : s->team_ctas;
     G = std::min(G, s->num_sms);
     G = std::max(G, 1);
@@ -342,6 +306,11 @@ static int end_index(const titus_solver* s, const titus_options_t* opt, int n_be
 extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus_options_t* opt, void* stream_) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
     cudaStream_t stream = (cudaStream_t)stream_;
+    if (method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE) {
+        s->last_method = method;
+        return titus_host::wide_solve_device(s, method, opt, stream);
+    }
+    if (method != TITUS_DLR_FIXED) return fail(TITUS_ERR_ARG, "unknown method %d", method);
     int rc = init_state(s, s->r, stream);
     if (rc) return rc;
     return launch(s, method, opt, 2, end_index(s, opt, 2), 0, stream);
@@ -349,6 +318,8 @@ extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus
 
 extern "C" int titus_fetch(titus_solver_t* s, titus_result_t* res) {
     if (!s || !res) return fail(TITUS_ERR_ARG, "NULL argument");
+    if (s->last_method == TITUS_PARALLEL_ADAPTIVE || s->last_method == TITUS_BUG_ADAPTIVE)
+        return titus_host::wide_fetch(s, res);
     int rc = check_status(s);
     if (rc) return rc;
     int info[4];
@@ -399,8 +370,12 @@ extern "C" int titus_solve_problem(const titus_problem_t* pb, int32_t method, co
 extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X, const double* S, const double* W,
                                const double* psi, const double* dose, int32_t n_next) {
     if (!s || !X || !S || !W || !psi || !dose) return fail(TITUS_ERR_ARG, "NULL argument");
-    if (rank < 1 || rank > KM) return fail(TITUS_ERR_LIMIT, "rank %d outside [1, %d]", rank, KM);
+    if (rank < 1 || rank > wide::RA) return fail(TITUS_ERR_LIMIT, "rank %d outside [1, %d]", rank, wide::RA);
     if (n_next < 2 || n_next > s->nE + 1) return fail(TITUS_ERR_ARG, "n_next %d outside [2, nE+1]", n_next);
+    // the adaptive integrators' state always; the fixed-rank state when the rank fits
+    int rcw = titus_host::wide_set_state(s, rank, X, S, W, psi, dose, n_next);
+    if (rcw) return rcw;
+    if (rank > KM) return TITUS_OK;
     TeamState& st = s->st;
     CK(cudaMemset(st.X, 0, (size_t)s->n * KM * sizeof(double)));
     CK(cudaMemset(st.W, 0, (size_t)s->N * KM * sizeof(double)));
@@ -424,6 +399,12 @@ extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X,
 extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t n_stop,
                                 titus_result_t* res) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE) {
+        s->last_method = method;
+        int rc = titus_host::wide_solve_from(s, method, opt, n_stop);
+        if (rc) return rc;
+        return titus_host::wide_fetch(s, res);
+    }
     int info[4];
     CK(cudaMemcpy(info, s->st.info, sizeof(info), cudaMemcpyDeviceToHost));
     const int n_begin = info[3];
@@ -453,6 +434,6 @@ extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
     return m;
 }
 
-extern "C" int titus_max_rank(void) { return KM; }
+extern "C" int titus_max_rank(void) { return 2 * wide::RA; }
 extern "C" int titus_max_ordinates(void) { return QM < KM ? QM : KM; }
 extern "C" const char* titus_version(void) { return "titus-b200 0.1 (sm_100a, FP64)"; }

@@ -1,0 +1,76 @@
+// Host-side solver handle shared by the translation units of libtitus.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/titus.h"
+#include "wide_common.cuh"
+
+struct titus_solver;
+
+namespace titus_host {
+
+// Records the message for titus_last_error and returns `code`.
+int fail(int code, const char* fmt, ...);
+
+#define CK(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return titus_host::fail(TITUS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int upload(T** dptr, const T* host, size_t count) {
+    *dptr = nullptr;
+    if (count == 0) return TITUS_OK;
+    CK(cudaMalloc((void**)dptr, count * sizeof(T)));
+    if (host) CK(cudaMemcpy(*dptr, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    return TITUS_OK;
+}
+
+// rank-adaptive integrators (titus_adaptive.cu)
+int wide_solve_device(titus_solver* s, int method, const titus_options_t* opt, cudaStream_t stream);
+int wide_solve_from(titus_solver* s, int method, const titus_options_t* opt, int n_stop);
+int wide_fetch(titus_solver* s, titus_result_t* res);
+int wide_set_state(titus_solver* s, int rank, const double* X, const double* S, const double* W, const double* psi,
+                   const double* dose, int n_next);
+void wide_free(titus_solver* s);
+
+}  // namespace titus_host
+
+struct titus_solver {
+    titus::DevProblem P{};
+    int n = 0, N = 0, q = 0, nE = 0;
+    std::vector<void*> allocs;
+    // fixed-rank team state
+    titus::TeamState st{};
+    titus::TeamState* d_st = nullptr;
+    int team_ctas = 0;
+    int device = 0;
+    int num_sms = 0;
+    int r = 0;
+    int last_method = -1;
+    int last_G = 0;
+    unsigned long long* prof = nullptr;
+    int clock_khz = 0;
+    // rank-adaptive state (allocated on first use)
+    titus::wide::WideState wst{};
+    titus::wide::WideState* d_wst = nullptr;
+    std::vector<void*> wide_allocs;
+    int wide_state_valid = 0;   // 1 after an adaptive solve or titus_set_state
+
+    template <class T>
+    int alloc(T** p, size_t count, const T* host = nullptr) {
+        int rc = titus_host::upload(p, host, count);
+        if (rc == TITUS_OK && *p) allocs.push_back((void*)*p);
+        return rc;
+    }
+    template <class T>
+    int walloc(T** p, size_t count) {
+        int rc = titus_host::upload(p, (const T*)nullptr, count);
+        if (rc == TITUS_OK && *p) wide_allocs.push_back((void*)*p);
+        return rc;
+    }
+    ~titus_solver();
+};

@@ -1,0 +1,265 @@
+// Building blocks of the rank-adaptive DLR kernel (parallel and BUG-rejection
+// integrators, SolverCSD.jl :1726-2008 and :2011-2374).
+//
+// Widths: the rank entering a step is at most RA; augmented bases [X X~] hold
+// up to KA = 2 RA columns. Tall factors are row-major in global memory (L2
+// resident) with leading dimension KA (X, W) or RA (K, L and their projected /
+// range-finder copies). Every reduction over rows goes through per-CTA partial
+// buffers and a two-stage sum into the team's reduced buffer `red`, which all
+// CTAs then read; small-matrix algebra is repeated bit-identically by every CTA
+// in shared memory and in a per-CTA scratch area of global memory, so all CTAs
+// take the same control decisions (ranks, rejections) without a broadcast.
+#pragma once
+#include "dlr_device.cuh"
+
+namespace titus {
+namespace wide {
+
+constexpr int NT = titus::NT;   // threads per CTA
+constexpr int RA = 40;          // max rank entering a step
+constexpr int KA = 2 * RA;      // max augmented width
+constexpr int QW = titus::QM;   // psi leading dimension (reduced ordinates <= QW)
+constexpr int TRW = 8;          // rows per staged tile
+constexpr int PMAXW = 8 * KA * KA;   // largest reduction (BUG S-step Grams): 51200 doubles
+constexpr int WORKD = 20480;    // shared work area (doubles)
+constexpr int ACCW = 16384;     // accumulator chunk (doubles), inside the work area
+constexpr int FLD = 10 * RA;    // feature-tile leading dimension (doubles)
+constexpr int SCRW = 81920;     // per-CTA scratch (doubles, global)
+constexpr int WCS = 3 * RA;     // row stride of the W-side completion coefficients
+
+// extra device status codes (titus::ST_* holds 1..4)
+constexpr int ST_LIMIT = 5;        // rank would exceed RA
+constexpr int ST_UNSUPPORTED = 6;  // angular basis lost orthonormality (cannot complete)
+constexpr int ST_SVD = 7;          // Jacobi SVD did not converge
+
+struct WideState {
+    double* X;      // n x KA
+    double* W;      // N x KA
+    double* K;      // n x RA
+    double* KP;     // n x RA  projected K
+    double* CX;     // n x RA  range-finder C (X side)
+    double* L;      // N x RA
+    double* LP;     // N x RA
+    double* CW;     // N x RA
+    double* psi0;   // n x QW
+    double* psi1;
+    double* dose;   // n
+    double* S;      // KA x KA (state S, written back at exit)
+    double* part;   // 2 x G x PMAXW
+    double* red;    // 2 x PMAXW (double-buffered with the partials)
+    double* scr;    // G x SCRW per-CTA scratch
+    unsigned* bar;  // G + 1 barrier flags
+    int* status;
+    int* info;      // [0] rank, [1] iterations, [2] psi index, [3] next n, [4] eta count
+    double* diag;   // 16
+    double* tvar;   // [0] pseudo-time t (BUG / parallel)
+    int* rank_hist; // hist_cap
+    double* time_hist;
+    double* eta_hist;
+    double* bound_hist;
+    int hist_cap;
+};
+
+// Per-CTA scratch layout (offsets in doubles). r x r matrices use ld RA.
+enum : int {
+    SO_SC = 0,                       // 4 stacked S C_d        (4 RA x RA)
+    SO_SG = SO_SC + 4 * RA * RA,     // 4 stacked S^T G_d^T    (4 RA x RA)
+    SO_SBAR = SO_SG + 4 * RA * RA,   // S after the streaming / in-scattering S update (RA x RA)
+    SO_SIDE = SO_SBAR + RA * RA,     // per-side blocks, SIDE_STRIDE each
+};
+// per-side block offsets (relative to SO_SIDE + side * SIDE_STRIDE)
+enum : int {
+    SS_F1 = 0,                 // Q1 = A F1 (range part), r x rho1
+    SS_P1 = SS_F1 + RA * RA,   // F1 F1^T
+    SS_T = SS_P1 + RA * RA,    // projection coefficients / range-finder transform
+    SS_M1 = SS_T + RA * RA,    // Q1^T A (BUG: top block of X1^T X)
+    SS_R0 = SS_M1 + RA * RA,   // Cholesky factor of the range-finder Gram
+    SS_RI = SS_R0 + RA * RA,   // inverse Cholesky factor of C^T C (basis = C RI)
+    SS_V0 = SS_RI + RA * RA,   // slow path: eigenvectors of G0
+    SS_WC = SS_V0 + RA * RA,   // W-side completion coefficients (RA rows, stride WCS)
+    SIDE_STRIDE = SS_WC + RA * 3 * RA,
+};
+constexpr int SO_XTPSI = SO_SIDE + 2 * SIDE_STRIDE;  // KA x QW   X^T psi
+constexpr int SO_MTDW = SO_XTPSI + KA * QW;          // QW x KA   MRed^T diag(Dvec) W
+constexpr int SO_TMP = SO_MTDW + QW * KA;            // 3 x KA x KA general temporaries
+constexpr int SO_DBG = SO_TMP + 3 * KA * KA;           // KA x KA: input of the last truncation SVD
+constexpr int SO_END = SO_DBG + KA * KA;
+static_assert(SO_END <= SCRW, "per-CTA scratch too small");
+
+struct WSmem {
+    double S[KA * KA];     // state S (ld KA)
+    double work[WORKD];    // phase-dependent union
+    double vec[6 * KA + 2 * QW];
+    double dmisc[32];
+    int imisc[32];
+    int wcand[RA];
+    double wnrm[RA];
+    int perm[KA];
+    double sig[KA];
+};
+
+// Per-side bookkeeping of one augmentation (identical in every CTA).
+struct SideInfo {
+    int rho1;      // numerical rank of the old basis (range part of Q1)
+    int fast1;     // 1: Q1 = A R1^{-1} (certified); 0: Jacobi (F1 = V diag(lambda^-1/2))
+    int rho2;      // numerical rank of the projected new directions
+    int fast2;     // 1: certified CholQR2 path
+    int need2;     // completion vectors appended after the range part of Q2
+    int cand0;     // first X candidate used by Q2's completion
+    double scale;  // Frobenius norm of [A B]
+};
+
+struct WCtx {
+    DevProblem P;
+    WideState st;
+    WSmem* sm;
+    double* scr;    // this CTA's scratch
+    int G, b;
+    int c0, c1, m0, m1;
+    int r;          // current rank
+    double* psi_in;
+    double* psi_out;
+    unsigned gen;
+    int parity;
+    const double* redp;  // reduced buffer of the latest reduction
+    int cur_n;
+    unsigned long long* prof;
+    SideInfo side[2];
+};
+
+__device__ __forceinline__ bool is_bnd_w(const DevProblem& P, int c) {
+    int i = c / P.ny, j = c - (c / P.ny) * P.ny;
+    return i == 0 || j == 0 || i == P.nx - 1 || j == P.ny - 1;
+}
+
+__device__ __forceinline__ bool wsync(WCtx& x) {
+    ProfScope ps(x.prof, PF_BARRIER);
+    return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag);
+}
+
+__device__ __forceinline__ double* wpart(const WCtx& x, int g) {
+    return x.st.part + ((size_t)x.parity * x.G + g) * PMAXW;
+}
+
+// Publish `cnt` partial entries of this CTA starting at `off` from the shared
+// accumulator (chunked Gram passes publish several pieces before one reduce).
+__device__ __forceinline__ void wpublish_chunk(WCtx& x, const double* acc, int off, int cnt) {
+    double* dst = wpart(x, x.b) + off;
+    for (int e = threadIdx.x; e < cnt; e += NT) dst[e] = acc[e];
+}
+
+// Two-stage team sum of entries [0, count) of the partials into the reduced
+// buffer of the same parity (x.redp afterwards). Before the call every CTA
+// published its partial with wpublish_chunk. The hook runs between the two
+// barriers (used to zero X rows that other CTAs stop reading at the first
+// barrier). A reduced buffer stays valid until the second reduction after it.
+template <class Hook>
+__device__ inline bool wreduce(WCtx& x, int count, Hook hook) {
+    if (!wsync(x)) return false;
+    hook();
+    {
+        ProfScope ps(x.prof, PF_REDUCE);
+        const int per = (count + x.G - 1) / x.G;
+        const int e0 = x.b * per, e1 = min(count, e0 + per);
+        const double* base = x.st.part + (size_t)x.parity * x.G * PMAXW;
+        double* red = x.st.red + (size_t)x.parity * PMAXW;
+        for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+            double a = 0.0;
+            for (int g = 0; g < x.G; ++g) a += ldcg(base + (size_t)g * PMAXW + e);
+            red[e] = a;
+        }
+    }
+    x.redp = x.st.red + (size_t)x.parity * PMAXW;
+    x.parity ^= 1;
+    return wsync(x);
+}
+__device__ inline bool wreduce(WCtx& x, int count) {
+    return wreduce(x, count, [] {});
+}
+
+// red[off + i*n + j] -> D[i*ld + j]  (m x n)
+__device__ inline void load_red(const WCtx& x, int off, int m, int n, double* D, int ld) {
+    for (int e = threadIdx.x; e < m * n; e += NT) D[(e / n) * ld + e % n] = ldcg(x.redp + off + e);
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- algebra ---
+// C (m x n) = alpha op(A) op(B) + beta C; op(A) = A^T when ta (A stored k x m),
+// op(B) = B^T when tb (B stored n x k). C must not alias A or B.
+__device__ inline void g_mm(double* C, int ldc, const double* A, int lda, bool ta, const double* B, int ldb, bool tb,
+                            int m, int k, int n, double alpha = 1.0, double beta = 0.0) {
+    for (int e = threadIdx.x; e < m * n; e += NT) {
+        const int i = e / n, j = e - (e / n) * n;
+        double s = 0.0;
+        for (int l = 0; l < k; ++l) {
+            const double a = ta ? A[l * lda + i] : A[i * lda + l];
+            const double bb = tb ? B[j * ldb + l] : B[l * ldb + j];
+            s = fma(a, bb, s);
+        }
+        double v = alpha * s;
+        if (beta != 0.0) v = fma(beta, C[i * ldc + j], v);
+        C[i * ldc + j] = v;
+    }
+    __syncthreads();
+}
+__device__ inline void g_copy(double* D, int ldd, const double* A, int lda, int m, int n) {
+    for (int e = threadIdx.x; e < m * n; e += NT) D[(e / n) * ldd + e % n] = A[(e / n) * lda + e % n];
+    __syncthreads();
+}
+__device__ inline void g_zero(double* D, int ldd, int m, int n) {
+    for (int e = threadIdx.x; e < m * n; e += NT) D[(e / n) * ldd + e % n] = 0.0;
+    __syncthreads();
+}
+
+// ----------------------------------------------------------- row helpers ---
+// rows [r0, r0+nr) x cols [c0, c0+k) of A (ld lda) -> t (ld ldt) at column tc
+__device__ __forceinline__ void wload(double* t, int ldt, int tc, const double* A, int lda, int c0, int r0, int nr,
+                                      int k) {
+    for (int e = threadIdx.x; e < nr * k; e += NT) {
+        const int r = e / k, j = e - (e / k) * k;
+        t[r * ldt + tc + j] = ldcg(A + (size_t)(r0 + r) * lda + c0 + j);
+    }
+}
+__device__ __forceinline__ void wstore(double* A, int lda, int c0, const double* t, int ldt, int tc, int r0, int nr,
+                                       int k) {
+    for (int e = threadIdx.x; e < nr * k; e += NT) {
+        const int r = e / k, j = e - (e / k) * k;
+        A[(size_t)(r0 + r) * lda + c0 + j] = t[r * ldt + tc + j];
+    }
+}
+
+// One Gram block of a feature tile: acc[off + i*wb + j] += sum_r F[r][ca+i] F[r][cb+j].
+struct GBlock {
+    int ca, wa, cb, wb, off;
+};
+// Accumulate a list of blocks over a tile of nr rows; 2x2 register blocking.
+__device__ inline void gram_blocks(double* acc, const double* F, int ldf, int nr, const GBlock* bl, int nb) {
+    for (int q = 0; q < nb; ++q) {
+        const GBlock g = bl[q];
+        const int hi = (g.wa + 1) >> 1, hj = (g.wb + 1) >> 1;
+        for (int e = threadIdx.x; e < hi * hj; e += NT) {
+            const int i = 2 * (e / hj), j = 2 * (e - (e / hj) * hj);
+            const bool i1 = i + 1 < g.wa, j1 = j + 1 < g.wb;
+            double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+            for (int r = 0; r < nr; ++r) {
+                const double* row = F + r * ldf;
+                const double a0 = row[g.ca + i], a1 = i1 ? row[g.ca + i + 1] : 0.0;
+                const double b0 = row[g.cb + j], b1 = j1 ? row[g.cb + j + 1] : 0.0;
+                s00 = fma(a0, b0, s00);
+                s01 = fma(a0, b1, s01);
+                s10 = fma(a1, b0, s10);
+                s11 = fma(a1, b1, s11);
+            }
+            double* o = acc + g.off + i * g.wb + j;
+            o[0] += s00;
+            if (j1) o[1] += s01;
+            if (i1) {
+                o[g.wb] += s10;
+                if (j1) o[g.wb + 1] += s11;
+            }
+        }
+    }
+}
+
+}  // namespace wide
+}  // namespace titus

@@ -1,0 +1,369 @@
+// Small dense factorisations of the rank-adaptive kernel, run by one CTA on
+// shared-memory matrices (row-major with an explicit leading dimension):
+//   w_chol      upper Cholesky R^T R = G and R^{-1} (k <= RA)
+//   w_eig       symmetric eigendecomposition, parallel cyclic Jacobi (k <= RA)
+//   w_svd       one-sided (Hestenes) Jacobi SVD of an m x m matrix (m <= KA),
+//               with w_svd_complete applying the deterministic rule for the
+//               numerically null singular directions that truncate! keeps.
+#pragma once
+#include "wide_common.cuh"
+
+namespace titus {
+namespace wide {
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Upper Cholesky of G (k x k, ld ldg, any memory) into R (shared, ld) and its
+// inverse Ri (shared, ld). Returns ||R||_F ||R^{-1}||_F, or +inf on a
+// non-positive pivot; *ri_f receives ||R^{-1}||_F (a bound 1/sigma_min).
+static __device__ __noinline__ double w_chol(const double* G, int ldg, double* R, double* Ri, int ld, int k,
+                                             double* ri_f) {
+    __shared__ int s_ok;
+    __shared__ double s_nr[NT / 32], s_ni[NT / 32];
+    for (int e = threadIdx.x; e < k * k; e += NT) {
+        const int i = e / k, j = e - (e / k) * k;
+        R[i * ld + j] = (j >= i) ? G[i * ldg + j] : 0.0;
+        Ri[i * ld + j] = 0.0;
+    }
+    if (threadIdx.x == 0) s_ok = 1;
+    __syncthreads();
+    for (int j = 0; j < k; ++j) {
+        const double d = R[j * ld + j];
+        const bool okp = d > 0.0;
+        const double piv = okp ? sqrt(d) : 1.0;
+        __syncthreads();
+        for (int l = j + threadIdx.x; l < k; l += NT) R[j * ld + l] = (l == j) ? piv : R[j * ld + l] / piv;
+        if (!okp && threadIdx.x == 0) s_ok = 0;
+        __syncthreads();
+        const int m = k - j - 1;
+        for (int e = threadIdx.x; e < m * m; e += NT) {
+            const int i = j + 1 + e / m, l = j + 1 + (e - (e / m) * m);
+            if (l >= i) R[i * ld + l] = fma(-R[j * ld + i], R[j * ld + l], R[i * ld + l]);
+        }
+        __syncthreads();
+    }
+    // R^{-1}: warp w solves columns c = w, w+8, ...; lanes split each dot product
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < k; c += NT / 32) {
+        if (lane == 0) Ri[c * ld + c] = 1.0 / R[c * ld + c];
+        __syncwarp();
+        for (int a = c - 1; a >= 0; --a) {
+            double s = 0.0;
+            for (int bb = a + 1 + lane; bb <= c; bb += 32) s = fma(R[a * ld + bb], Ri[bb * ld + c], s);
+            s = warp_sum(s);
+            if (lane == 0) Ri[a * ld + c] = -s / R[a * ld + a];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    double nr = 0.0, ni = 0.0;
+    for (int e = threadIdx.x; e < k * k; e += NT) {
+        const int i = e / k, j = e - (e / k) * k;
+        nr = fma(R[i * ld + j], R[i * ld + j], nr);
+        ni = fma(Ri[i * ld + j], Ri[i * ld + j], ni);
+    }
+    nr = warp_sum(nr);
+    ni = warp_sum(ni);
+    if (lane == 0) {
+        s_nr[warp] = nr;
+        s_ni[warp] = ni;
+    }
+    __syncthreads();
+    double tr = 0.0, ti = 0.0;
+    for (int w = 0; w < NT / 32; ++w) {
+        tr += s_nr[w];
+        ti += s_ni[w];
+    }
+    const bool ok = s_ok != 0;
+    __syncthreads();
+    if (ri_f) *ri_f = ok ? sqrt(ti) : INFINITY;
+    return ok ? sqrt(tr) * sqrt(ti) : INFINITY;
+}
+
+// Symmetric eigendecomposition by parallel cyclic Jacobi. A (k x k, shared,
+// ld) is destroyed; V (shared, ld) receives the eigenvectors as columns, lam
+// the eigenvalues, both in descending order. k <= RA.
+// A pair is rotated when |a_pq| > 1e-15 sqrt|a_pp a_qq| (relative accuracy on
+// graded matrices) and |a_pq| > rel_floor max_i |a_ii|. A Gram matrix formed
+// in floating point carries noise of about k eps max|a_ii| that no rotation
+// removes, so raw Grams use rel_floor ~ 4 k eps; graded Grams of already
+// separated directions use a negligible floor.
+static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* lam, int k, int* status,
+                                          double rel_floor) {
+    __shared__ double rc[RA / 2 + 1], rs[RA / 2 + 1];
+    __shared__ int rp[RA / 2 + 1], rq[RA / 2 + 1];
+    __shared__ int s_rot[2];
+    __shared__ double s_lam[RA];
+    __shared__ int s_perm[RA];
+    for (int e = threadIdx.x; e < k * k; e += NT) V[(e / k) * ld + e % k] = ((e / k) == (e % k)) ? 1.0 : 0.0;
+    __syncthreads();
+    if (k <= 1) {
+        if (threadIdx.x == 0 && k == 1) lam[0] = A[0];
+        __syncthreads();
+        return;
+    }
+    const int m = k + (k & 1);
+    const int npairs = m / 2;
+    __shared__ double s_floor;
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int i = 0; i < k; ++i) mx = fmax(mx, fabs(A[i * ld + i]));
+        s_floor = rel_floor * mx;
+    }
+    __syncthreads();
+    const double afloor = s_floor;
+    bool conv = false;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        const int par = sweep & 1;
+        if (threadIdx.x == 0) s_rot[par] = 0;
+        __syncthreads();
+        for (int t = 0; t < m - 1; ++t) {
+            if (threadIdx.x < npairs) {
+                int p, q;
+                double c = 1.0, s = 0.0;
+                if (rr_pair(m, t, threadIdx.x, k, p, q)) {
+                    const double apq = A[p * ld + q];
+                    const double app = A[p * ld + p], aqq = A[q * ld + q];
+                    if (fabs(apq) > afloor && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
+                        const double th = (aqq - app) / (2.0 * apq);
+                        const double tt = fabs(th) > 1e150 ? 0.5 / th
+                                                           : copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0));
+                        c = 1.0 / sqrt(tt * tt + 1.0);
+                        s = tt * c;
+                        s_rot[par] = 1;
+                    }
+                } else {
+                    p = q = -1;
+                }
+                rc[threadIdx.x] = c;
+                rs[threadIdx.x] = s;
+                rp[threadIdx.x] = p;
+                rq[threadIdx.x] = q;
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < npairs * k; e += NT) {
+                const int pi = e / k, j = e - (e / k) * k;
+                const int p = rp[pi], q = rq[pi];
+                if (p < 0 || rs[pi] == 0.0) continue;
+                const double c = rc[pi], s = rs[pi];
+                const double ap = A[p * ld + j], aq = A[q * ld + j];
+                A[p * ld + j] = c * ap - s * aq;
+                A[q * ld + j] = s * ap + c * aq;
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < npairs * k; e += NT) {
+                const int pi = e / k, i = e - (e / k) * k;
+                const int p = rp[pi], q = rq[pi];
+                if (p < 0 || rs[pi] == 0.0) continue;
+                const double c = rc[pi], s = rs[pi];
+                const double ap = A[i * ld + p], aq = A[i * ld + q];
+                A[i * ld + p] = c * ap - s * aq;
+                A[i * ld + q] = s * ap + c * aq;
+                const double vp = V[i * ld + p], vq = V[i * ld + q];
+                V[i * ld + p] = c * vp - s * vq;
+                V[i * ld + q] = s * vp + c * vq;
+            }
+            __syncthreads();
+        }
+        if (!s_rot[par]) {
+            conv = true;
+            break;
+        }
+    }
+    if (!conv && threadIdx.x == 0) set_status(status, ST_JACOBI);
+    for (int i = threadIdx.x; i < k; i += NT) s_lam[i] = A[i * ld + i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < k; i += NT) {
+        const double li = s_lam[i];
+        int rank = 0;
+        for (int j = 0; j < k; ++j) {
+            const double lj = s_lam[j];
+            if (lj > li || (lj == li && j < i)) ++rank;
+        }
+        s_perm[rank] = i;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * k; e += NT) {
+        const int i = e / k, j = e - (e / k) * k;
+        A[i * ld + j] = V[i * ld + s_perm[j]];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * k; e += NT) V[(e / k) * ld + e % k] = A[(e / k) * ld + e % k];
+    for (int j = threadIdx.x; j < k; j += NT) lam[j] = s_lam[s_perm[j]];
+    __syncthreads();
+}
+
+// One-sided Jacobi SVD of the m x m matrix whose column p is At[p*ld .. +m)
+// (transposed storage keeps column operations on contiguous shared memory).
+// On return At[p] = sigma_p u_p and Vt[p] = v_p (unsorted); sig[j] and
+// perm[j] list the singular values in descending order (sigma_j = sig[j],
+// column perm[j]). Returns the number of sweeps, or -1 without convergence.
+static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, double* sig, int* perm) {
+    __shared__ int s_rot[2];
+    __shared__ double s_n[KA];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int e = threadIdx.x; e < m * m; e += NT) Vt[(e / m) * ld + e % m] = ((e / m) == (e % m)) ? 1.0 : 0.0;
+    __syncthreads();
+    int sweeps = -1;
+    // rotation threshold: a recomputed dot product of two length-m columns
+    // carries rounding of about m eps |x| |y|; columns with |x|^2 below
+    // 1e-32 ||A||_F^2 are numerically null (their directions are replaced by
+    // the deterministic completion) and are not rotated against
+    const double ctol = 2.2e-16 * m;
+    __shared__ double s_fro;
+    if (threadIdx.x < 32) {
+        double f = 0.0;
+        for (int e = threadIdx.x; e < m * m; e += 32) f = fma(At[(e / m) * ld + e % m], At[(e / m) * ld + e % m], f);
+        f = warp_sum(f);
+        if (threadIdx.x == 0) s_fro = f;
+    }
+    __syncthreads();
+    const double nfloor = 1e-32 * s_fro;
+    if (m > 1) {
+        const int mm = m + (m & 1);
+        const int npairs = mm / 2;
+        for (int sweep = 0; sweep < 60; ++sweep) {
+            const int par = sweep & 1;
+            if (threadIdx.x == 0) s_rot[par] = 0;
+            __syncthreads();
+            for (int t = 0; t < mm - 1; ++t) {
+                for (int s = warp; s < npairs; s += NT / 32) {
+                    int p, q;
+                    if (!rr_pair(mm, t, s, m, p, q)) continue;
+                    double a = 0.0, bq = 0.0, g = 0.0;
+                    for (int i = lane; i < m; i += 32) {
+                        const double u = At[p * ld + i], v = At[q * ld + i];
+                        a = fma(u, u, a);
+                        bq = fma(v, v, bq);
+                        g = fma(u, v, g);
+                    }
+                    a = warp_sum(a);
+                    bq = warp_sum(bq);
+                    g = warp_sum(g);
+                    if (g != 0.0 && fmin(a, bq) > nfloor && fabs(g) > ctol * sqrt(a * bq)) {
+                        const double z = (bq - a) / (2.0 * g);
+                        const double tt = fabs(z) > 1e150 ? 0.5 / z : copysign(1.0, z) / (fabs(z) + sqrt(1.0 + z * z));
+                        const double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+                        for (int i = lane; i < m; i += 32) {
+                            const double u = At[p * ld + i], v = At[q * ld + i];
+                            At[p * ld + i] = c * u - sn * v;
+                            At[q * ld + i] = sn * u + c * v;
+                            const double vu = Vt[p * ld + i], vv = Vt[q * ld + i];
+                            Vt[p * ld + i] = c * vu - sn * vv;
+                            Vt[q * ld + i] = sn * vu + c * vv;
+                        }
+                        if (lane == 0) s_rot[par] = 1;
+                    }
+                }
+                __syncthreads();
+            }
+            if (!s_rot[par]) {
+                sweeps = sweep + 1;
+                break;
+            }
+        }
+    } else {
+        sweeps = 0;
+    }
+    // singular values and descending order (stable)
+    for (int p = warp; p < m; p += NT / 32) {
+        double a = 0.0;
+        for (int i = lane; i < m; i += 32) a = fma(At[p * ld + i], At[p * ld + i], a);
+        a = warp_sum(a);
+        if (lane == 0) s_n[p] = sqrt(a);
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < m; p += NT) {
+        const double v = s_n[p];
+        int rank = 0;
+        for (int j = 0; j < m; ++j) {
+            const double w = s_n[j];
+            if (w > v || (w == v && j < p)) ++rank;
+        }
+        perm[rank] = p;
+        sig[rank] = v;
+    }
+    __syncthreads();
+    return sweeps;
+}
+
+// Normalise the left singular vectors of the numerical range (sigma_j >
+// tol sigma_0, j < rho) and replace the directions j in [rho, kkeep) of both
+// factors by canonical vectors in index order, completed by two Gram-Schmidt
+// passes against the columns before them (accepted when the residual exceeds
+// 1/2) -- the rule of oracle.linalg.svd_det. Returns rho.
+static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld, int m, const double* sig,
+                                                  const int* perm, int kkeep, double tol, int* status) {
+    __shared__ double s_v[KA];
+    __shared__ double s_d[KA];
+    __shared__ double s_nv;
+    __shared__ int s_acc;
+    int rho = 0;
+    if (m > 0 && sig[0] > 0.0)
+        for (int j = 0; j < m; ++j) {
+            if (sig[j] > tol * sig[0]) rho = j + 1;
+            else break;
+        }
+    for (int e = threadIdx.x; e < rho * m; e += NT) {
+        const int j = e / m, i = e - (e / m) * m;
+        At[perm[j] * ld + i] /= sig[j];
+    }
+    __syncthreads();
+    for (int side = 0; side < 2; ++side) {
+        double* B = side == 0 ? At : Vt;
+        int cand = 0;
+        for (int j = rho; j < kkeep; ++j) {
+            bool done = false;
+            while (!done) {
+                if (cand >= m) {
+                    if (threadIdx.x == 0) set_status(status, ST_COMPLETION);
+                    __syncthreads();
+                    return rho;
+                }
+                for (int i = threadIdx.x; i < m; i += NT) s_v[i] = (i == cand) ? 1.0 : 0.0;
+                __syncthreads();
+                for (int pass = 0; pass < 2; ++pass) {
+                    // d_a = B_a . v for a < j, then v -= sum_a d_a B_a
+                    for (int a = threadIdx.x >> 5; a < j; a += NT / 32) {
+                        const double* ba = B + perm[a] * ld;
+                        double s = 0.0;
+                        for (int i = threadIdx.x & 31; i < m; i += 32) s = fma(ba[i], s_v[i], s);
+                        s = warp_sum(s);
+                        if ((threadIdx.x & 31) == 0) s_d[a] = s;
+                    }
+                    __syncthreads();
+                    for (int i = threadIdx.x; i < m; i += NT) {
+                        double v = s_v[i];
+                        for (int a = 0; a < j; ++a) v = fma(-s_d[a], B[perm[a] * ld + i], v);
+                        s_v[i] = v;
+                    }
+                    __syncthreads();
+                }
+                if (threadIdx.x < 32) {
+                    double s = 0.0;
+                    for (int i = threadIdx.x; i < m; i += 32) s = fma(s_v[i], s_v[i], s);
+                    s = warp_sum(s);
+                    if (threadIdx.x == 0) {
+                        s_acc = (sqrt(s) > 0.5) ? 1 : 0;
+                        s_nv = sqrt(s);
+                    }
+                }
+                __syncthreads();
+                ++cand;
+                if (s_acc) {
+                    const double nv = s_nv;
+                    for (int i = threadIdx.x; i < m; i += NT) B[perm[j] * ld + i] = s_v[i] / nv;
+                    done = true;
+                }
+                __syncthreads();
+            }
+        }
+    }
+    return rho;
+}
+
+}  // namespace wide
+}  // namespace titus

@@ -5,7 +5,12 @@ Mirrors the reference API (``code/SolverCSD.jl``):
 * ``SolverCSD(settings)`` -- builds the solver data (``:63-146``) on the host
   and uploads it to the device once (``titus_create``);
 * ``SolveFirstCollisionSourceDLR(solver)`` -- fixed-rank integrator
-  (``:891-1120``), returns ``(X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, psi)``.
+  (``:891-1120``), returns ``(X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, psi)``;
+* ``SolveFirstCollisionSourceDLRParallel(solver)`` -- rank-adaptive parallel
+  integrator (``:1726-2008``), the same tuple with ``rVec`` before ``psi``;
+* ``SolveFirstCollisionSourceDLRBUGRejection(solver)`` -- rank-adaptive BUG
+  integrator with step rejection (``:2011-2374``), returns ``(X U, Sigma, O W V,
+  W V, dose, [E rank]^T, [E eta], [E bound], psi)``.
 
 The energy loop itself always runs on the GPU; there is no CPU path.
 """
@@ -157,7 +162,8 @@ class SolverCSD:
         bufs = dict(
             dose=np.zeros(self.n), X=np.zeros((self.n, r_cap)), S=np.zeros((r_cap, r_cap)),
             W=np.zeros((self.N, r_cap)), psi=np.zeros((self.n, self.q)),
-            rank_history=np.zeros(self.nE, dtype=np.int32),
+            rank_history=np.zeros(self.nE, dtype=np.int32), time_history=np.zeros(self.nE),
+            eta_history=np.zeros(self.nE), bound_history=np.zeros(self.nE),
         )
         res.dose = _lib.as_dp(bufs["dose"])
         res.X = _lib.as_dp(bufs["X"])
@@ -165,6 +171,9 @@ class SolverCSD:
         res.W = _lib.as_dp(bufs["W"])
         res.psi = _lib.as_dp(bufs["psi"])
         res.rank_history = _lib.as_ip(bufs["rank_history"])
+        res.time_history = _lib.as_dp(bufs["time_history"])
+        res.eta_history = _lib.as_dp(bufs["eta_history"])
+        res.bound_history = _lib.as_dp(bufs["bound_history"])
         res.r_cap = r_cap
         return res, bufs
 
@@ -178,9 +187,11 @@ class SolverCSD:
         _lib.check(lib.titus_solve(h, method, C.byref(opt), C.byref(res)), "titus_solve")
         k = res.rank
         return dict(X=bufs["X"][:, :k], S=bufs["S"][:k, :k], W=bufs["W"][:, :k], dose=bufs["dose"],
-                    psi=bufs["psi"], rank=k, steps=res.steps_done, rank_history=bufs["rank_history"])
+                    psi=bufs["psi"], rank=k, steps=res.steps_done, rank_history=bufs["rank_history"],
+                    time_history=bufs["time_history"], eta_history=bufs["eta_history"],
+                    bound_history=bufs["bound_history"])
 
-    def run_from(self, method: int, state: dict, n_next: int, n_stop: int, rank_tol: float = 0.0):
+    def run_from(self, method: int, state: dict, n_next: int, n_stop: int, rank_tol: float = 0.0, max_steps: int = 0):
         """Resume the loop from a given state (checkpoint restart)."""
         lib = _lib.load()
         h = self.handle()
@@ -194,11 +205,11 @@ class SolverCSD:
                                        _lib.as_dp(dose), n_next), "titus_set_state")
         r_cap = max(self.settings.r, k)
         res, bufs = self._result(r_cap)
-        opt = self.options(0, rank_tol)
+        opt = self.options(max_steps, rank_tol)
         _lib.check(lib.titus_solve_from(h, method, C.byref(opt), n_stop, C.byref(res)), "titus_solve_from")
         kk = res.rank
         return dict(X=bufs["X"][:, :kk], S=bufs["S"][:kk, :kk], W=bufs["W"][:, :kk], dose=bufs["dose"],
-                    psi=bufs["psi"], rank=kk, steps=res.steps_done)
+                    psi=bufs["psi"], rank=kk, steps=res.steps_done, rank_history=bufs["rank_history"])
 
     def outputs(self, out):
         """The reference's return tuple from raw factors (``SolverCSD.jl:1116-1118``)."""
@@ -216,6 +227,51 @@ def SolveFirstCollisionSourceDLR(solver: SolverCSD, max_steps: int = 0):
     res = solver.outputs(out)
     solver.dose = res[4]
     return res
+
+
+def SolveFirstCollisionSourceDLRParallel(solver: SolverCSD, recordGif: bool = False, max_steps: int = 0):
+    """Rank-adaptive parallel integrator (``SolverCSD.jl:1726-2008``) on the GPU.
+
+    Returns ``(X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, rVec, psi)`` with
+    rVec (2 x nEnergies): row 0 the pseudo-time t at which each step started,
+    row 1 the rank after the step (``:1947-1948``); entries of steps not run
+    keep the initial rank as in the reference.
+    """
+    out = solver.run(_lib.TITUS_PARALLEL_ADAPTIVE, max_steps=max_steps)
+    res = solver.outputs(out)
+    solver.dose = res[4]
+    r0 = solver.settings.r // 2
+    rVec = float(r0) * np.ones((2, solver.nE))
+    hist = out["rank_history"]
+    done = hist >= 0
+    rVec[1, done] = hist[done]
+    rVec[0, 1:][done[1:]] = out["time_history"][1:][done[1:]]
+    return res[0], res[1], res[2], res[3], res[4], rVec, res[5]
+
+
+def SolveFirstCollisionSourceDLRBUGRejection(solver: SolverCSD, recordGif: bool = False, max_steps: int = 0):
+    """Rank-adaptive BUG integrator with step rejection (``SolverCSD.jl:2011-2374``).
+
+    Returns ``(X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, [E rank]^T,
+    [E eta], [E bound], psi)``: one (energy, rank) column per loop iteration
+    (repeated energies included) and one (energy, eta) / (energy, bound) row per
+    streaming rejection test. The device records at most nEnergies iterations.
+    """
+    out = solver.run(_lib.TITUS_BUG_ADAPTIVE, max_steps=max_steps)
+    res = solver.outputs(out)
+    solver.dose = res[4]
+    it = min(out["steps"], solver.nE)
+    nidx = out["time_history"][:it].astype(int)
+    energies = solver.eGrid[nidx - 1]
+    rank_hist = np.array([energies, out["rank_history"][:it].astype(float)])
+    ne = int(np.count_nonzero(out["bound_history"]))
+    eta = out["eta_history"][:ne]
+    bound = out["bound_history"][:ne]
+    # the reference pairs each eta with eGrid[n-1] of its iteration; the device
+    # keeps the values only, so the energies are left as NaN here
+    eta_hist = np.column_stack([np.full(ne, np.nan), eta])
+    bound_hist = np.column_stack([np.full(ne, np.nan), bound])
+    return res[0], res[1], res[2], res[3], res[4], rank_hist, eta_hist, bound_hist, res[5]
 
 
 def scalar_flux(X, sigma, WV):
