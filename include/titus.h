@@ -141,10 +141,12 @@ void titus_destroy(titus_solver_t* solver);
 int titus_last_error(char* buf, size_t len);
 
 /* Per-phase device timers of the last profiled solve (options.profile = 1),
- * in nanoseconds at the nominal SM clock, recorded on the first CTA:
- * [0] barrier waits, [1] reductions, [2] Jacobi eigensolves, [3] Cholesky,
- * [4] basis completion, [5] (unused), [6] (unused), [7] range-finder passes,
- * [8] (unused), [9] kernel total. Returns the number of entries written. */
+ * in nanoseconds at the nominal SM clock, recorded on the first CTA. Timers are
+ * exclusive (time is charged to the innermost open phase):
+ * [0] barrier waits, [1] reductions, [2] Jacobi eigensolvers / SVD, [3] Cholesky,
+ * [4] basis completion, [5] streaming row passes, [6] scattering and truncation
+ * row passes, [7] range-finder / augmentation passes, [8] small-matrix algebra,
+ * [9] everything else. Returns the number of entries written. */
 int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
 
 /* Fixed-rank solve (method TITUS_DLR_FIXED) that allocates nothing. No

@@ -17,7 +17,9 @@ LIB_PATH = os.path.join(HERE, "libtitus.so")
 TITUS_DLR_FIXED = 0
 TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
-PROFILE_NAMES = ["barrier", "reduce", "jacobi", "cholesky", "completion", "-", "-", "rf_passes", "-", "total"]
+# exclusive device timers (titus_profile order); "other" is time outside every named phase
+PROFILE_NAMES = ["barrier", "reduce", "jacobi", "cholesky", "completion", "rows_stream", "rows_scatter", "rf_passes",
+                 "small", "other"]
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

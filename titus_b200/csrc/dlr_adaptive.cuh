@@ -182,6 +182,7 @@ __device__ inline void w_acc_zero(double* acc, int cnt) {
 // published at [G_0..G_3 | C_0..C_3] (r x r each) and reduced; X's boundary
 // rows are zeroed between the barriers (:1859).
 static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
+    ProfScope ps_(x.prof, PF_ROWS_STREAM);
     const int k = x.r;
     double* acc = x.sm->work;
     double* F = x.sm->work + ACCW;
@@ -198,6 +199,7 @@ static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
 // After the streaming Grams: SC_d = S C_d, SG_d = S^T G_d^T (stacked, rows d*k + l,
 // ld k) in scratch; Sbar = S - dE sum G_d S C_d in scratch (ld RA).
 static __device__ __noinline__ void w_stream_small(WCtx& x, bool want_sbar) {
+    ProfScope ps_(x.prof, PF_SMALL);
     const int k = x.r;
     WSmem* sm = x.sm;
     double* Gd = sm->work;                 // 4 k x k (ld k), from red
@@ -230,6 +232,7 @@ static __device__ __noinline__ void w_stream_small(WCtx& x, bool want_sbar) {
 // and the Grams of [X K] (X side) and [W L] (W side): per side three k x k
 // blocks [A^T A | A^T B | B^T B] at offsets 0 and 3k^2.
 static __device__ __noinline__ bool w_phase_C(WCtx& x) {
+    ProfScope ps_(x.prof, PF_ROWS_STREAM);
     const int k = x.r;
     const double dE = x.P.dE;
     WSmem* sm = x.sm;
@@ -303,6 +306,7 @@ __device__ __forceinline__ SideBufs side_bufs(const WCtx& x, int s) {
 // Cholesky or Jacobi; T1 = P1 (A^T B) with P1 = F1 F1^T (Q1 Q1^T = A P1 A^T on
 // the range part; completion vectors of the X side are orthogonal to K).
 static __device__ __noinline__ void aug_prepare(WCtx& x, int s, int goff) {
+    ProfScope ps_(x.prof, PF_SMALL);
     const int k = x.r;
     WSmem* sm = x.sm;
     SideInfo& si = x.side[s];
@@ -357,6 +361,7 @@ static __device__ __noinline__ void aug_prepare(WCtx& x, int s, int goff) {
 
 // BP = B - A T (T = SS_T) for own rows; acc[off..] += A^T BP (second=false) or BP^T BP (second=true)
 static __device__ __noinline__ void aug_pass(WCtx& x, int s, bool second, double* acc, int off) {
+    ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
     SideBufs sb = side_bufs(x, s);
     double* T = x.sm->work + ACCW;               // k x k (ld RA)
@@ -421,6 +426,7 @@ __device__ __forceinline__ void w_rsolve(double* t, int ldt, const double* R, in
 // own rows; acc[off..] += C^T C (rho x rho), or (mode 2) (BP V)^T (BP V) without
 // storing C.
 static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, double* acc, int off) {
+    ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
     SideBufs sb = side_bufs(x, s);
     double* M = x.sm->work + ACCW;          // k x k (ld RA)
@@ -569,6 +575,7 @@ static __device__ __noinline__ bool range_find(WCtx& x, const bool do_side[2], c
 // C[m,:] RI), v_1 .. v_a]; stores per accepted vector its candidate, norm and
 // coefficients in SS_WC (row a, length nq1 + rho2 + a).
 static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, int need) {
+    ProfScope ps_(x.prof, PF_COMPLETE);
     WSmem* sm = x.sm;
     double* wc = sside(x, 1, SS_WC);
     const double* F1 = sside(x, 1, SS_F1);
@@ -631,6 +638,7 @@ static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, 
 // `with_q1` also A[:, :k] = Q1 = [A F1 | completion] (BUG). Row tile t holds
 // [old A (k) | Q1 (k) | X~ (k)] per row.
 static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q1) {
+    ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
     WSmem* sm = x.sm;
     SideBufs sb = side_bufs(x, s);
@@ -731,6 +739,7 @@ static __device__ __noinline__ bool augment(WCtx& x, bool with_q1) {
 // the kept null directions. Leaves U^T (rows perm[j]) at work[0], V^T at
 // work[KA*KA], sig/perm in shared memory; returns the kept rank.
 static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
+    ProfScope ps_(x.prof, PF_JACOBI);
     WSmem* sm = x.sm;
     double* At = sm->work;
     double* Vt = sm->work + KA * KA;
@@ -768,6 +777,7 @@ static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
 // `w0` (m entries, any memory): row 0 of W before the update, needed for the
 // dose because the CTA owning moment 0 overwrites it without a team barrier.
 static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int dose_sidx, const double* w0) {
+    ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     WSmem* sm = x.sm;
     const double* Ut = sm->work;
     const double* Vt = sm->work + KA * KA;
@@ -817,6 +827,7 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
 // L and LP, with L^T L at red offset k^2 (the range finder's side-1 slot); X
 // side: X^T psi of the X before zeroing (:1904) at offset 2k^2.
 static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig) {
+    ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     const int k = x.r;
     const DevProblem& P = x.P;
     WSmem* sm = x.sm;
@@ -860,6 +871,7 @@ static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig
 
 // W = [C RI | completion] (own moments); acc = [L^T W (k^2) | MRed^T diag(Dvec) W (q k)]
 static __device__ __noinline__ bool w_outscatter_basis(WCtx& x, const double* sig) {
+    ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     const int k = x.r;
     const DevProblem& P = x.P;
     WSmem* sm = x.sm;
@@ -935,6 +947,7 @@ static __device__ __noinline__ bool w_outscatter(WCtx& x, const double* sig) {
 // Sbar = S + dE Xtpsi MtDW in scratch and the second dose half-step with
 // (X, Sbar, W) before truncation (parallel integrator, :1943).
 static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, bool sbar_dose, int dose_sidx) {
+    ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     const int k = x.r;
     const DevProblem& P = x.P;
     WSmem* sm = x.sm;
@@ -1026,6 +1039,7 @@ __device__ inline void w_zero_bnd(WCtx& x) {
 // Grams over the new directions for the parallel integrator's augmented S:
 // red [X~^T K (k^2) | L^T W~ (k^2)]
 static __device__ __noinline__ bool w_parallel_blocks(WCtx& x) {
+    ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     const int k = x.r;
     double* acc = x.sm->work;
     double* t = x.sm->work + ACCW;   // TRW x 2RA
@@ -1088,6 +1102,7 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
     x.parity = 0;
     x.redp = x.st.red;
     x.cur_n = 0;
+    prof_begin(x.prof);
     ProfScope ps_total(x.prof, PF_TOTAL);
     x.c0 = (int)((long long)x.b * P.n / G);
     x.c1 = (int)((long long)(x.b + 1) * P.n / G);

@@ -59,17 +59,38 @@ struct DevProblem {
 enum ProfCat { PF_BARRIER = 0, PF_REDUCE, PF_JACOBI, PF_CHOL, PF_COMPLETE, PF_ROWS_STREAM, PF_ROWS_SCATTER,
                PF_RF_PASSES, PF_SMALL, PF_TOTAL, PF_COUNT };
 
+// Exclusive phase timers (SM cycles): time is charged to the innermost open
+// scope. Slots PF_COUNT+4 / +5 of the buffer hold the open category and the
+// last timestamp; only thread 0 of the profiled CTA touches them.
+constexpr int PF_CUR = 14, PF_T = 15;
 struct ProfScope {
     unsigned long long* p;
     int cat;
-    long long t0;
-    __device__ ProfScope(unsigned long long* p_, int c) : p(p_), cat(c), t0(0) {
-        if (p && threadIdx.x == 0) t0 = clock64();
+    int prev;
+    __device__ ProfScope(unsigned long long* p_, int c) : p(p_), cat(c), prev(PF_COUNT) {
+        if (p && threadIdx.x == 0) {
+            const unsigned long long now = clock64();
+            prev = (int)p[PF_CUR];
+            p[prev] += now - p[PF_T];
+            p[PF_CUR] = (unsigned long long)c;
+            p[PF_T] = now;
+        }
     }
     __device__ ~ProfScope() {
-        if (p && threadIdx.x == 0) p[cat] += (unsigned long long)(clock64() - t0);
+        if (p && threadIdx.x == 0) {
+            const unsigned long long now = clock64();
+            p[cat] += now - p[PF_T];
+            p[PF_CUR] = (unsigned long long)prev;
+            p[PF_T] = now;
+        }
     }
 };
+__device__ __forceinline__ void prof_begin(unsigned long long* p) {
+    if (p && threadIdx.x == 0) {
+        p[PF_CUR] = PF_COUNT;   // unclassified slot, not reported
+        p[PF_T] = clock64();
+    }
+}
 
 // Per-team device state.
 struct TeamState {

@@ -296,6 +296,7 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
     x.parity = 0;
     x.rhoK = x.rhoL = 0;
     x.cur_n = 0;
+    prof_begin(x.prof);
     ProfScope ps_total(x.prof, PF_TOTAL);
     x.c0 = (int)((long long)x.b * P.n / G);
     x.c1 = (int)((long long)(x.b + 1) * P.n / G);

@@ -159,14 +159,30 @@ __device__ inline bool wreduce(WCtx& x, int count, Hook hook) {
     hook();
     {
         ProfScope ps(x.prof, PF_REDUCE);
+        // CTA b sums the slice [e0, e1) over the G partials. Blocks of RCH
+        // elements x RSPL partial-splits keep RSPL independent L2 loads in
+        // flight per element (adjacent threads read adjacent elements); the
+        // splits are combined in a fixed order, so the sum is deterministic.
+        constexpr int RCH = 16, RSPL = NT / RCH;
+        __shared__ double s_part[NT];
         const int per = (count + x.G - 1) / x.G;
         const int e0 = x.b * per, e1 = min(count, e0 + per);
         const double* base = x.st.part + (size_t)x.parity * x.G * PMAXW;
         double* red = x.st.red + (size_t)x.parity * PMAXW;
-        for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+        const int el = threadIdx.x % RCH, sp = threadIdx.x / RCH;
+        for (int eb = e0; eb < e1; eb += RCH) {
+            const int e = eb + el;
             double a = 0.0;
-            for (int g = 0; g < x.G; ++g) a += ldcg(base + (size_t)g * PMAXW + e);
-            red[e] = a;
+            if (e < e1)
+                for (int g = sp; g < x.G; g += RSPL) a += ldcg(base + (size_t)g * PMAXW + e);
+            s_part[threadIdx.x] = a;
+            __syncthreads();
+            if (threadIdx.x < RCH && eb + threadIdx.x < e1) {
+                double t = 0.0;
+                for (int q = 0; q < RSPL; ++q) t += s_part[q * RCH + threadIdx.x];
+                red[eb + threadIdx.x] = t;
+            }
+            __syncthreads();
         }
     }
     x.redp = x.st.red + (size_t)x.parity * PMAXW;

@@ -127,7 +127,10 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
                 if (rr_pair(m, t, threadIdx.x, k, p, q)) {
                     const double apq = A[p * ld + q];
                     const double app = A[p * ld + p], aqq = A[q * ld + q];
-                    if (fabs(apq) > afloor && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
+                    // a rotation whose angle is below eps changes nothing (|a_pq| <= eps max|a|):
+                    // skipping it keeps the sweep count finite on rounding-level entries
+                    if (fabs(apq) > afloor && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) &&
+                        fabs(apq) > 4.4e-16 * fmax(fabs(app), fabs(aqq))) {
                         const double th = (aqq - app) / (2.0 * apq);
                         const double tt = fabs(th) > 1e150 ? 0.5 / th
                                                            : copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0));
@@ -174,6 +177,7 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
         }
     }
     if (!conv && threadIdx.x == 0) set_status(status, ST_JACOBI);
+    __syncthreads();
     for (int i = threadIdx.x; i < k; i += NT) s_lam[i] = A[i * ld + i];
     __syncthreads();
     for (int i = threadIdx.x; i < k; i += NT) {
@@ -243,7 +247,9 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
                     a = warp_sum(a);
                     bq = warp_sum(bq);
                     g = warp_sum(g);
-                    if (g != 0.0 && fmin(a, bq) > nfloor && fabs(g) > ctol * sqrt(a * bq)) {
+                    // skip rotations with an angle below eps (no effect on the columns)
+                    if (g != 0.0 && fmin(a, bq) > nfloor && fabs(g) > ctol * sqrt(a * bq) &&
+                        fabs(g) > 2.2e-16 * fmax(a, bq)) {
                         const double z = (bq - a) / (2.0 * g);
                         const double tt = fabs(z) > 1e150 ? 0.5 / z : copysign(1.0, z) / (fabs(z) + sqrt(1.0 + z * z));
                         const double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;

@@ -1,6 +1,10 @@
 """Per-phase device timer breakdown of one solve of a benchmark workload.
 
     python -m titus_b200.profile_phases [--nx 101] [--npn 21] [--r 20] [--steps 200] [--team 0]
+                                        [--method fixed|parallel|bug] [--problem csdWaterBeam]
+
+Timers are exclusive (each cycle is charged to the innermost open phase) and
+recorded on the first CTA; "total" is their sum.
 """
 from __future__ import annotations
 
@@ -21,16 +25,22 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--team", type=int, default=0)
     ap.add_argument("--problem", default="csdWaterBeam")
+    ap.add_argument("--method", default="fixed", choices=["fixed", "parallel", "bug"])
     a = ap.parse_args()
+    method = {"fixed": _lib.TITUS_DLR_FIXED, "parallel": _lib.TITUS_PARALLEL_ADAPTIVE,
+              "bug": _lib.TITUS_BUG_ADAPTIVE}[a.method]
     s = Settings(a.nx, a.nx, a.r, a.problem, nPN=a.npn)
     g = SolverCSD(s, team_ctas=a.team)
-    g.run(_lib.TITUS_DLR_FIXED, max_steps=5)
+    g.run(method, max_steps=5)
     t0 = time.perf_counter()
-    g.run(_lib.TITUS_DLR_FIXED, max_steps=a.steps, profile=True)
+    out = g.run(method, max_steps=a.steps, profile=True)
     wall = time.perf_counter() - t0
     prof = g.profile()
-    per_step = {k: v / a.steps / 1e3 for k, v in prof.items()}
-    print(json.dumps({"workload": vars(a), "wall_s": wall, "us_per_step": per_step}))
+    steps = max(out["steps"], 1)
+    per_step = {k: v / steps / 1e3 for k, v in prof.items()}
+    hist = out["rank_history"]
+    print(json.dumps({"workload": vars(a), "steps": out["steps"], "rank": out["rank"],
+                      "rank_max": int(hist.max()), "wall_s": wall, "us_per_step": per_step}))
 
 
 if __name__ == "__main__":

@@ -155,7 +155,9 @@ class SolverCSD:
         lib = _lib.load()
         out = np.zeros(16)
         m = lib.titus_profile(self.handle(), _lib.as_dp(out), 16)
-        return {name: out[i] for i, name in enumerate(_lib.PROFILE_NAMES[:m]) if name != "-"}
+        d = {name: out[i] for i, name in enumerate(_lib.PROFILE_NAMES[:m])}
+        d["total"] = float(sum(d.values()))
+        return d
 
     def _result(self, r_cap):
         res = _lib.Result()
