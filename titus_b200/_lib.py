@@ -19,7 +19,7 @@ TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
 # exclusive device timers (titus_profile order); "other" is time outside every named phase
 PROFILE_NAMES = ["barrier", "reduce", "jacobi", "cholesky", "completion", "rows_stream", "rows_scatter", "rf_passes",
-                 "small", "other"]
+                 "small", "other", "prologue"]
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

@@ -104,6 +104,7 @@ __device__ inline void sw0(WCtx& x, const double* S, int ldS, int k, double* v, 
 
 // ---- phase A: boundary inflow at energy[n-1] (PsiBeam, :977-988), first dose half-step
 static __device__ __noinline__ void w_phase_A(WCtx& x, int n) {
+    ProfScope ps_(x.prof, PF_PROLOGUE);
     const DevProblem& P = x.P;
     WSmem* sm = x.sm;
     const int k = x.r;
@@ -122,6 +123,7 @@ static __device__ __noinline__ void w_phase_A(WCtx& x, int n) {
 
 // ---- uncollided sweep of own cells, psi_in -> psi_out (solveFluxUpwind! :388-463, :1000-1005)
 static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
+    ProfScope ps_(x.prof, PF_PROLOGUE);
     const DevProblem& P = x.P;
     const double dE = P.dE;
     const double den = 1.0 + dE * sigma0;
@@ -150,25 +152,26 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
 // operators): acc[d k^2 ..] = A^T L_d A, acc[(4+d) k^2 ..] = B^T A_d B.
 // `cw` = width of A and B used; blocks for d in [d0, d1) only (chunking).
 static __device__ __noinline__ void w_grams_pass(WCtx& x, const double* A, const double* B, int cw, int d0, int d1, int off0,
-                                    double* acc, double* F) {
+                                    double* acc, double* F, int ldf, int tr) {
+    ProfScope ps_(x.prof, PF_ROWS_STREAM);
     GBlock bl[4];
     int nb = 0;
     const int kk = cw * cw;
     for (int d = d0; d < d1; ++d) bl[nb++] = GBlock{0, cw, (d + 1) * cw, cw, (d - d0) * kk};
-    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
-        const int nr = min(TRW, x.c1 - r0);
-        wload(F, FLD, 0, A, KA, 0, r0, nr, cw);
-        w_stencil(x, A, KA, r0, nr, cw, F, FLD, cw);
+    for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+        const int nr = min(tr, x.c1 - r0);
+        wload(F, ldf, 0, A, KA, 0, r0, nr, cw);
+        w_stencil(x, A, KA, r0, nr, cw, F, ldf, cw);
         __syncthreads();
-        gram_blocks(acc + off0, F, FLD, nr, bl, nb);
+        gram_blocks(acc + off0, F, ldf, nr, bl, nb);
         __syncthreads();
     }
-    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-        const int nr = min(TRW, x.m1 - r0);
-        wload(F, FLD, 0, B, KA, 0, r0, nr, cw);
-        w_spmm(x, B, KA, r0, nr, cw, F, FLD, cw);
+    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+        const int nr = min(tr, x.m1 - r0);
+        wload(F, ldf, 0, B, KA, 0, r0, nr, cw);
+        w_spmm(x, B, KA, r0, nr, cw, F, ldf, cw);
         __syncthreads();
-        gram_blocks(acc + off0 + (d1 - d0) * kk, F, FLD, nr, bl, nb);
+        gram_blocks(acc + off0 + (d1 - d0) * kk, F, ldf, nr, bl, nb);
         __syncthreads();
     }
 }
@@ -185,9 +188,9 @@ static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
     ProfScope ps_(x.prof, PF_ROWS_STREAM);
     const int k = x.r;
     double* acc = x.sm->work;
-    double* F = x.sm->work + ACCW;
+    double* F = x.sm->work + 8 * k * k;
     w_acc_zero(acc, 8 * k * k);
-    w_grams_pass(x, x.st.X, x.st.W, k, 0, 4, 0, acc, F);
+    w_grams_pass(x, x.st.X, x.st.W, k, 0, 4, 0, acc, F, 5 * k, rows_fit(WORKD - 8 * k * k, 5 * k));
     wpublish_chunk(x, acc, 0, 8 * k * k);
     return wreduce(x, 8 * k * k, [&] {
         for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT)
@@ -237,50 +240,52 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
     const double dE = x.P.dE;
     WSmem* sm = x.sm;
     double* acc = sm->work;                      // 6 k^2
-    double* ST = sm->work + 6 * RA * RA;         // 4k x k stacked (SC or SG)
-    double* F = ST + 4 * RA * RA;                // TRW x FLD
-    double* T = F + TRW * FLD;                   // TRW x 2k feature tile [A | B]
+    double* ST = sm->work + 6 * k * k;           // 4k x k stacked (SC or SG)
+    double* F = ST + 4 * k * k;                  // tr x 4k stencil / operator outputs
+    const int ldF = 4 * k, ldT = 2 * k;
+    const int tr = rows_fit(WORKD - 10 * k * k, ldF + ldT);
+    double* T = F + tr * ldF;                    // tr x 2k feature tile [A | B]
     w_acc_zero(acc, 6 * k * k);
     const GBlock bl[3] = {{0, k, 0, k, 0}, {0, k, k, k, k * k}, {k, k, k, k, 2 * k * k}};
     // X side
     g_copy(ST, k, x.scr + SO_SC, k, 4 * k, k);
-    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
-        const int nr = min(TRW, x.c1 - r0);
-        wload(T, 2 * RA, 0, x.st.X, KA, 0, r0, nr, k);
-        w_stencil(x, x.st.X, KA, r0, nr, k, F, FLD, 0);
+    for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+        const int nr = min(tr, x.c1 - r0);
+        wload(T, ldT, 0, x.st.X, KA, 0, r0, nr, k);
+        w_stencil(x, x.st.X, KA, r0, nr, k, F, ldF, 0);
         __syncthreads();
         for (int e = threadIdx.x; e < nr * k; e += NT) {
             const int r = e / k, j = e - (e / k) * k;
             double s = 0.0;
-            for (int l = 0; l < k; ++l) s = fma(T[r * 2 * RA + l], sm->S[l * KA + j], s);
+            for (int l = 0; l < k; ++l) s = fma(T[r * ldT + l], sm->S[l * KA + j], s);
             double t = 0.0;
-            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * FLD + l], ST[l * k + j], t);
-            T[r * 2 * RA + k + j] = s - dE * t;
+            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * ldF + l], ST[l * k + j], t);
+            T[r * ldT + k + j] = s - dE * t;
         }
         __syncthreads();
-        wstore(x.st.K, RA, 0, T, 2 * RA, k, r0, nr, k);
-        gram_blocks(acc, T, 2 * RA, nr, bl, 3);
+        wstore(x.st.K, RA, 0, T, ldT, k, r0, nr, k);
+        gram_blocks(acc, T, ldT, nr, bl, 3);
         __syncthreads();
     }
     // W side
     g_copy(ST, k, x.scr + SO_SG, k, 4 * k, k);
     const GBlock bw[3] = {{0, k, 0, k, 3 * k * k}, {0, k, k, k, 4 * k * k}, {k, k, k, k, 5 * k * k}};
-    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-        const int nr = min(TRW, x.m1 - r0);
-        wload(T, 2 * RA, 0, x.st.W, KA, 0, r0, nr, k);
-        w_spmm(x, x.st.W, KA, r0, nr, k, F, FLD, 0);
+    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+        const int nr = min(tr, x.m1 - r0);
+        wload(T, ldT, 0, x.st.W, KA, 0, r0, nr, k);
+        w_spmm(x, x.st.W, KA, r0, nr, k, F, ldF, 0);
         __syncthreads();
         for (int e = threadIdx.x; e < nr * k; e += NT) {
             const int r = e / k, j = e - (e / k) * k;
             double s = 0.0;  // (W S^T)[r][j]
-            for (int l = 0; l < k; ++l) s = fma(T[r * 2 * RA + l], sm->S[j * KA + l], s);
+            for (int l = 0; l < k; ++l) s = fma(T[r * ldT + l], sm->S[j * KA + l], s);
             double t = 0.0;
-            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * FLD + l], ST[l * k + j], t);
-            T[r * 2 * RA + k + j] = s - dE * t;
+            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * ldF + l], ST[l * k + j], t);
+            T[r * ldT + k + j] = s - dE * t;
         }
         __syncthreads();
-        wstore(x.st.L, RA, 0, T, 2 * RA, k, r0, nr, k);
-        gram_blocks(acc, T, 2 * RA, nr, bw, 3);
+        wstore(x.st.L, RA, 0, T, ldT, k, r0, nr, k);
+        gram_blocks(acc, T, ldT, nr, bw, 3);
         __syncthreads();
     }
     wpublish_chunk(x, acc, 0, 6 * k * k);
@@ -364,13 +369,14 @@ static __device__ __noinline__ void aug_pass(WCtx& x, int s, bool second, double
     ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
     SideBufs sb = side_bufs(x, s);
-    double* T = x.sm->work + ACCW;               // k x k (ld RA)
-    double* F = T + RA * RA;                     // TRW x 2RA: [A | BP]
+    double* T = x.sm->work + 2 * RA * RA;        // k x k (ld RA), after the 2k^2 accumulator
+    double* F = T + RA * RA;                     // tr x 2RA: [A | BP]
+    const int tr = rows_fit(WORKD - 3 * RA * RA, 2 * RA);
     g_copy(T, RA, sside(x, s, SS_T), RA, k, k);
     const GBlock bl = second ? GBlock{k, k, k, k, off} : GBlock{0, k, k, k, off};
     const double* Bsrc = second ? sb.BP : sb.B;
-    for (int r0 = sb.r0; r0 < sb.r1; r0 += TRW) {
-        const int nr = min(TRW, sb.r1 - r0);
+    for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
+        const int nr = min(tr, sb.r1 - r0);
         wload(F, 2 * RA, 0, sb.A, KA, 0, r0, nr, k);
         wload(F, 2 * RA, k, Bsrc, RA, 0, r0, nr, k);
         __syncthreads();
@@ -429,13 +435,14 @@ static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, d
     ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
     SideBufs sb = side_bufs(x, s);
-    double* M = x.sm->work + ACCW;          // k x k (ld RA)
-    double* F = M + RA * RA;                // TRW x 2RA: [BP | out]
+    double* M = x.sm->work + 2 * RA * RA;   // k x k (ld RA), after the 2k^2 accumulator
+    double* F = M + RA * RA;                // tr x 2RA: [BP | out]
+    const int tr = rows_fit(WORKD - 3 * RA * RA, 2 * RA);
     g_copy(M, RA, sside(x, s, mode == 0 ? SS_R0 : (mode == 1 ? SS_T : SS_V0)), RA, k, mode == 1 ? rho : k);
     const int w = (mode == 1) ? rho : k;
     const GBlock bl{k, w, k, w, off};
-    for (int r0 = sb.r0; r0 < sb.r1; r0 += TRW) {
-        const int nr = min(TRW, sb.r1 - r0);
+    for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
+        const int nr = min(tr, sb.r1 - r0);
         wload(F, 2 * RA, 0, sb.BP, RA, 0, r0, nr, k);
         __syncthreads();
         if (mode == 0) {
@@ -519,6 +526,7 @@ static __device__ __noinline__ void rf_slow_rank(WCtx& x, int s, int off, bool p
 // On return side[s].rho2 is set and SS_RI holds R^{-1} of the CholQR of C, so
 // that the basis is C R^{-1} (rho2 columns).
 static __device__ __noinline__ bool range_find(WCtx& x, const bool do_side[2], const bool plain[2]) {
+    ProfScope ps_(x.prof, PF_CHOL);
     const int k = x.r;
     WSmem* sm = x.sm;
     const double tol = x.P.rank_tol;
@@ -645,14 +653,15 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
     const SideInfo& si = x.side[s];
     double* F1 = sm->work;                   // k x k
     double* Ri = F1 + RA * RA;               // rho2 x rho2
-    double* t = Ri + RA * RA;                // TRW x 3RA
-    double* cb = t + TRW * 3 * RA;           // TRW x RA (C rows)
+    const int tr = rows_fit(WORKD - 2 * RA * RA, 4 * RA);
+    double* t = Ri + RA * RA;                // tr x 3RA
+    double* cb = t + tr * 3 * RA;            // tr x RA (C rows)
     g_copy(F1, RA, sside(x, s, SS_F1), RA, k, k);
     if (si.rho2 > 0) g_copy(Ri, RA, sside(x, s, SS_RI), RA, si.rho2, si.rho2);
     const double* wc = sside(x, 1, SS_WC);
     const int rho1 = si.rho1, rho2 = si.rho2;
-    for (int r0 = sb.r0; r0 < sb.r1; r0 += TRW) {
-        const int nr = min(TRW, sb.r1 - r0);
+    for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
+        const int nr = min(tr, sb.r1 - r0);
         wload(t, 3 * RA, 0, sb.A, KA, 0, r0, nr, k);
         if (rho2 > 0) wload(cb, RA, 0, sb.C, RA, 0, r0, nr, rho2);
         __syncthreads();
@@ -746,6 +755,10 @@ static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
     // keep the SVD input (transposed) for diagnostics
     g_copy(x.scr + SO_DBG, KA, At, KA, m, m);
     const int sw = w_svd(At, Vt, KA, m, sm->sig, sm->perm);
+    if (x.prof && threadIdx.x == 0) {
+        x.prof[PF_SVD_SWEEPS] += (unsigned long long)(sw > 0 ? sw : 60);
+        x.prof[PF_SVD_CALLS] += 1ull;
+    }
     if (sw < 0 && threadIdx.x == 0 && atomicCAS(x.st.status, 0, ST_SVD) == 0) {
         x.st.diag[0] = 20;
         x.st.diag[2] = m;
@@ -781,8 +794,9 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
     WSmem* sm = x.sm;
     const double* Ut = sm->work;
     const double* Vt = sm->work + KA * KA;
-    double* t = sm->work + 2 * KA * KA;     // TRW x KA
-    double* o = t + TRW * KA;               // TRW x KA
+    const int tr = rows_fit(WORKD - 2 * KA * KA, 2 * KA);
+    double* t = sm->work + 2 * KA * KA;     // tr x KA
+    double* o = t + tr * KA;                // tr x KA
     double* v = sm->vec;                    // diag(sig) W_new[0,:]^T
     if (dose_sidx >= 0) {
         for (int j = threadIdx.x; j < kk; j += NT) {
@@ -796,8 +810,8 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
         double* A = side == 0 ? x.st.X : x.st.W;
         const double* B = side == 0 ? Ut : Vt;
         const int r0b = side == 0 ? x.c0 : x.m0, r1b = side == 0 ? x.c1 : x.m1;
-        for (int r0 = r0b; r0 < r1b; r0 += TRW) {
-            const int nr = min(TRW, r1b - r0);
+        for (int r0 = r0b; r0 < r1b; r0 += tr) {
+            const int nr = min(tr, r1b - r0);
             wload(t, KA, 0, A, KA, 0, r0, nr, m);
             __syncthreads();
             for (int e = threadIdx.x; e < nr * kk; e += NT) {
@@ -832,12 +846,14 @@ static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig
     const DevProblem& P = x.P;
     WSmem* sm = x.sm;
     double* acc = sm->work;
-    double* t = sm->work + ACCW;     // TRW x (KA + QW)
     const int ldt = KA + QW;
+    const int tstart = 2 * RA * RA + RA * QW;   // after the largest accumulator
+    const int tr = rows_fit(WORKD - tstart, ldt);
+    double* t = sm->work + tstart;   // tr x (KA + QW)
     w_acc_zero(acc, 2 * k * k + k * P.q);
     const GBlock bl{k, k, k, k, k * k};
-    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-        const int nr = min(TRW, x.m1 - r0);
+    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+        const int nr = min(tr, x.m1 - r0);
         wload(t, ldt, 0, x.st.W, KA, 0, r0, nr, k);
         __syncthreads();
         for (int e = threadIdx.x; e < nr * k; e += NT) {
@@ -855,8 +871,8 @@ static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig
         __syncthreads();
     }
     const GBlock bx{0, k, k, P.q, 2 * k * k};
-    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
-        const int nr = min(TRW, x.c1 - r0);
+    for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+        const int nr = min(tr, x.c1 - r0);
         wload(t, ldt, 0, x.st.X, KA, 0, r0, nr, k);
         wload(t, ldt, k, x.psi_in, QW, 0, r0, nr, P.q);
         __syncthreads();
@@ -877,16 +893,17 @@ static __device__ __noinline__ bool w_outscatter_basis(WCtx& x, const double* si
     WSmem* sm = x.sm;
     const SideInfo& si = x.side[1];
     double* acc = sm->work;
-    double* Ri = sm->work + ACCW;
-    double* t = Ri + RA * RA;           // TRW x (3 RA + QW): [C | W_new | L | MRed D]
+    double* Ri = sm->work + RA * RA + RA * QW;   // after the largest accumulator
+    double* t = Ri + RA * RA;           // tr x (3 RA + QW): [C | W_new | L | MRed D]
     const int ldt = 3 * RA + QW;
+    const int tr = rows_fit(WORKD - (2 * RA * RA + RA * QW), ldt);
     const int rho = si.rho2;
     if (rho > 0) g_copy(Ri, RA, sside(x, 1, SS_RI), RA, rho, rho);
     w_acc_zero(acc, k * k + P.q * k);
     const double* wc = sside(x, 1, SS_WC);
     const GBlock bl[2] = {{2 * RA, k, RA, k, 0}, {3 * RA, P.q, RA, k, k * k}};
-    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-        const int nr = min(TRW, x.m1 - r0);
+    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+        const int nr = min(tr, x.m1 - r0);
         if (rho > 0) wload(t, ldt, 0, x.st.CW, RA, 0, r0, nr, rho);
         wload(t, ldt, 2 * RA, x.st.L, RA, 0, r0, nr, k);
         for (int e = threadIdx.x; e < nr * P.q; e += NT) {
@@ -955,8 +972,9 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
     double* acc = sm->work;                   // 6 k^2
     double* Mt = sm->work + 6 * RA * RA;      // q x k MtDW (ld KA)
     double* Xp = Mt + QW * KA;                // k x q Xtpsi (ld QW)
-    double* t = Xp + KA * QW;                 // TRW x (2RA + QW)
+    double* t = Xp + KA * QW;                 // tr x (2RA + QW)
     const int ldt = 2 * RA + QW;
+    const int tr = rows_fit(WORKD - (6 * RA * RA + 2 * KA * QW), ldt);
     g_copy(Mt, KA, x.scr + SO_MTDW, KA, P.q, k);
     g_copy(Xp, QW, x.scr + SO_XTPSI, QW, k, P.q);
     double* Sb = x.scr + SO_SBAR;
@@ -982,8 +1000,8 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
     }
     w_acc_zero(acc, 6 * k * k);
     const GBlock bl[3] = {{0, k, 0, k, 0}, {0, k, k, k, k * k}, {k, k, k, k, 2 * k * k}};
-    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
-        const int nr = min(TRW, x.c1 - r0);
+    for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+        const int nr = min(tr, x.c1 - r0);
         wload(t, ldt, 0, x.st.X, KA, 0, r0, nr, k);
         wload(t, ldt, 2 * RA, x.psi_in, QW, 0, r0, nr, P.q);
         __syncthreads();
@@ -1005,8 +1023,8 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
     }
     if (sbar_dose) w_dose(x, dose_sidx, sm->vec, k, false);
     const GBlock bw[3] = {{0, k, 0, k, 3 * k * k}, {0, k, k, k, 4 * k * k}, {k, k, k, k, 5 * k * k}};
-    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-        const int nr = min(TRW, x.m1 - r0);
+    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+        const int nr = min(tr, x.m1 - r0);
         wload(t, ldt, 0, x.st.W, KA, 0, r0, nr, k);
         __syncthreads();
         for (int e = threadIdx.x; e < nr * k; e += NT) {
@@ -1042,20 +1060,21 @@ static __device__ __noinline__ bool w_parallel_blocks(WCtx& x) {
     ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     const int k = x.r;
     double* acc = x.sm->work;
-    double* t = x.sm->work + ACCW;   // TRW x 2RA
+    double* t = x.sm->work + 2 * RA * RA;   // tr x 2RA, after the 2k^2 accumulator
+    const int tr = rows_fit(WORKD - 2 * RA * RA, 2 * RA);
     w_acc_zero(acc, 2 * k * k);
     const GBlock bx{0, k, k, k, 0};        // X~^T K
     const GBlock bw{k, k, 0, k, k * k};    // L^T W~
-    for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
-        const int nr = min(TRW, x.c1 - r0);
+    for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+        const int nr = min(tr, x.c1 - r0);
         wload(t, 2 * RA, 0, x.st.X, KA, k, r0, nr, k);
         wload(t, 2 * RA, k, x.st.K, RA, 0, r0, nr, k);
         __syncthreads();
         gram_blocks(acc, t, 2 * RA, nr, &bx, 1);
         __syncthreads();
     }
-    for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-        const int nr = min(TRW, x.m1 - r0);
+    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+        const int nr = min(tr, x.m1 - r0);
         wload(t, 2 * RA, 0, x.st.W, KA, k, r0, nr, k);
         wload(t, 2 * RA, k, x.st.L, RA, 0, r0, nr, k);
         __syncthreads();
@@ -1183,17 +1202,18 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
                 __syncthreads();
                 // S-step Grams with the 2k-wide bases, two operators per chunk
                 double* acc = sm->work;
-                double* F = sm->work + ACCW;
                 const int mm = m * m;
+                double* F = sm->work + 2 * mm;
                 for (int d = 0; d < 4; ++d) {   // one operator per chunk: 2 m^2 <= ACCW
                     w_acc_zero(acc, 2 * mm);
-                    w_grams_pass(x, x.st.X, x.st.W, m, d, d + 1, 0, acc, F);
+                    w_grams_pass(x, x.st.X, x.st.W, m, d, d + 1, 0, acc, F, 5 * m, rows_fit(WORKD - 2 * mm, 5 * m));
                     wpublish_chunk(x, acc, d * mm, mm);             // X side G_d
                     wpublish_chunk(x, acc + mm, (4 + d) * mm, mm);  // W side C_d
                     __syncthreads();
                 }
                 if (!wreduce(x, 8 * mm)) { aborted = true; break; }
                 // Sup = S2 - dE sum_d G_d S2 C_d ; eta from the [k:, k:] block
+                ProfScope ps_sup(x.prof, PF_SMALL);
                 double* Gd = x.scr + SO_TMP;
                 double* Cd = Gd + KA * KA;
                 double* Tm = sm->work;                 // m x m
@@ -1288,12 +1308,14 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
                 if (!augment(x, true)) { aborted = true; break; }
                 // Grams X1^T psi (m x q) and MRed^T D W1 (q x m) over the new bases
                 double* acc = sm->work;
-                double* tt = sm->work + ACCW;
                 const int ldt = KA + QW;
+                const int tstart = 2 * KA * QW + KA;   // after the largest accumulator
+                const int tr = rows_fit(WORKD - tstart, ldt);
+                double* tt = sm->work + tstart;
                 w_acc_zero(acc, 2 * m * P.q + m);
                 const GBlock bx{0, m, KA, P.q, 0};
-                for (int r0 = x.c0; r0 < x.c1; r0 += TRW) {
-                    const int nr = min(TRW, x.c1 - r0);
+                for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+                    const int nr = min(tr, x.c1 - r0);
                     // own rows of X1 were just written by this CTA
                     wload(tt, ldt, 0, x.st.X, KA, 0, r0, nr, m);
                     wload(tt, ldt, KA, x.psi_in, QW, 0, r0, nr, P.q);
@@ -1302,8 +1324,8 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
                     __syncthreads();
                 }
                 const GBlock bw{KA, P.q, 0, m, m * P.q};
-                for (int r0 = x.m0; r0 < x.m1; r0 += TRW) {
-                    const int nr = min(TRW, x.m1 - r0);
+                for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+                    const int nr = min(tr, x.m1 - r0);
                     wload(tt, ldt, 0, x.st.W, KA, 0, r0, nr, m);
                     for (int e = threadIdx.x; e < nr * P.q; e += NT) {
                         const int r = e / P.q, kq = e - (e / P.q) * P.q;

@@ -57,11 +57,14 @@ struct DevProblem {
 
 // Phase-timer categories (titus_profile reports them in this order).
 enum ProfCat { PF_BARRIER = 0, PF_REDUCE, PF_JACOBI, PF_CHOL, PF_COMPLETE, PF_ROWS_STREAM, PF_ROWS_SCATTER,
-               PF_RF_PASSES, PF_SMALL, PF_TOTAL, PF_COUNT };
+               PF_RF_PASSES, PF_SMALL, PF_TOTAL, PF_PROLOGUE, PF_COUNT };
+// event counters in the timer buffer (profiled CTA only)
+constexpr int PF_SVD_SWEEPS = 12, PF_SVD_CALLS = 13;
 
 // Exclusive phase timers (SM cycles): time is charged to the innermost open
-// scope. Slots PF_COUNT+4 / +5 of the buffer hold the open category and the
-// last timestamp; only thread 0 of the profiled CTA touches them.
+// scope. Slot PF_COUNT collects unscoped time (not reported), slots PF_CUR /
+// PF_T hold the open category and the last timestamp; only thread 0 of the
+// profiled CTA touches them.
 constexpr int PF_CUR = 14, PF_T = 15;
 struct ProfScope {
     unsigned long long* p;

@@ -431,6 +431,12 @@ extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
     CK(cudaMemcpy(cyc, s->prof, sizeof(cyc), cudaMemcpyDeviceToHost));
     const int m = std::min<int>(n, PF_COUNT);
     for (int i = 0; i < m; ++i) ns[i] = (double)cyc[i] * 1e6 / (double)s->clock_khz;
+    // entries after the timers: SVD sweeps and SVD calls (counts, not times)
+    if (n >= PF_COUNT + 2) {
+        ns[PF_COUNT] = (double)cyc[PF_SVD_SWEEPS];
+        ns[PF_COUNT + 1] = (double)cyc[PF_SVD_CALLS];
+        return PF_COUNT + 2;
+    }
     return m;
 }
 

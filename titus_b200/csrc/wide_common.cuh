@@ -19,7 +19,8 @@ constexpr int NT = titus::NT;   // threads per CTA
 constexpr int RA = 40;          // max rank entering a step
 constexpr int KA = 2 * RA;      // max augmented width
 constexpr int QW = titus::QM;   // psi leading dimension (reduced ordinates <= QW)
-constexpr int TRW = 8;          // rows per staged tile
+constexpr int TRW = 8;          // rows per staged tile (minimum layout)
+constexpr int TRMAX = 32;       // rows per staged tile when the phase's free shared memory allows
 constexpr int PMAXW = 8 * KA * KA;   // largest reduction (BUG S-step Grams): 51200 doubles
 constexpr int WORKD = 20480;    // shared work area (doubles)
 constexpr int ACCW = 16384;     // accumulator chunk (doubles), inside the work area
@@ -126,6 +127,12 @@ struct WCtx {
     unsigned long long* prof;
     SideInfo side[2];
 };
+
+// Rows per tile that fit `avail` doubles of shared memory at `per_row` doubles a row.
+__device__ __forceinline__ int rows_fit(int avail, int per_row) {
+    const int r = avail / per_row;
+    return r < 1 ? 1 : (r > TRMAX ? TRMAX : r);
+}
 
 __device__ __forceinline__ bool is_bnd_w(const DevProblem& P, int c) {
     int i = c / P.ny, j = c - (c / P.ny) * P.ny;

@@ -213,9 +213,10 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
     __syncthreads();
     int sweeps = -1;
     // rotation threshold: a recomputed dot product of two length-m columns
-    // carries rounding of about m eps |x| |y|; columns with |x|^2 below
-    // 1e-32 ||A||_F^2 are numerically null (their directions are replaced by
-    // the deterministic completion) and are not rotated against
+    // carries rounding of about m eps |x| |y|. Columns with |x| below
+    // 1e-16 ||A||_F are numerically null and not rotated. (A floor as high as
+    // 1e-13 ||A||_F moves the dose by 2e-9: a column that starts tiny can
+    // still carry a small kept singular direction.)
     const double ctol = 2.2e-16 * m;
     __shared__ double s_fro;
     if (threadIdx.x < 32) {
@@ -229,31 +230,40 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
     if (m > 1) {
         const int mm = m + (m & 1);
         const int npairs = mm / 2;
+        // LP lanes per pair (8 / 16 / 32), PPW = 32 / LP pairs per warp
+        const int LP = m <= 24 ? 8 : (m <= 48 ? 16 : 32);
+        const int PPW = 32 / LP;
+        const int grp = lane / LP, gl = lane % LP;
         for (int sweep = 0; sweep < 60; ++sweep) {
             const int par = sweep & 1;
             if (threadIdx.x == 0) s_rot[par] = 0;
             __syncthreads();
             for (int t = 0; t < mm - 1; ++t) {
-                for (int s = warp; s < npairs; s += NT / 32) {
-                    int p, q;
-                    if (!rr_pair(mm, t, s, m, p, q)) continue;
+                // warp-uniform loop; every lane runs the shuffles
+                for (int sb = warp * PPW; sb < npairs; sb += (NT / 32) * PPW) {
+                    const int sidx = sb + grp;
+                    int p = 0, q = 0;
+                    const bool valid = sidx < npairs && rr_pair(mm, t, sidx, m, p, q);
                     double a = 0.0, bq = 0.0, g = 0.0;
-                    for (int i = lane; i < m; i += 32) {
-                        const double u = At[p * ld + i], v = At[q * ld + i];
-                        a = fma(u, u, a);
-                        bq = fma(v, v, bq);
-                        g = fma(u, v, g);
+                    if (valid)
+                        for (int i = gl; i < m; i += LP) {
+                            const double u = At[p * ld + i], v = At[q * ld + i];
+                            a = fma(u, u, a);
+                            bq = fma(v, v, bq);
+                            g = fma(u, v, g);
+                        }
+                    for (int o = LP / 2; o > 0; o >>= 1) {
+                        a += __shfl_xor_sync(0xffffffffu, a, o);
+                        bq += __shfl_xor_sync(0xffffffffu, bq, o);
+                        g += __shfl_xor_sync(0xffffffffu, g, o);
                     }
-                    a = warp_sum(a);
-                    bq = warp_sum(bq);
-                    g = warp_sum(g);
                     // skip rotations with an angle below eps (no effect on the columns)
-                    if (g != 0.0 && fmin(a, bq) > nfloor && fabs(g) > ctol * sqrt(a * bq) &&
+                    if (valid && g != 0.0 && fmin(a, bq) > nfloor && fabs(g) > ctol * sqrt(a * bq) &&
                         fabs(g) > 2.2e-16 * fmax(a, bq)) {
                         const double z = (bq - a) / (2.0 * g);
                         const double tt = fabs(z) > 1e150 ? 0.5 / z : copysign(1.0, z) / (fabs(z) + sqrt(1.0 + z * z));
                         const double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
-                        for (int i = lane; i < m; i += 32) {
+                        for (int i = gl; i < m; i += LP) {
                             const double u = At[p * ld + i], v = At[q * ld + i];
                             At[p * ld + i] = c * u - sn * v;
                             At[q * ld + i] = sn * u + c * v;
@@ -261,7 +271,7 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
                             Vt[p * ld + i] = c * vu - sn * vv;
                             Vt[q * ld + i] = sn * vu + c * vv;
                         }
-                        if (lane == 0) s_rot[par] = 1;
+                        if (gl == 0) s_rot[par] = 1;
                     }
                 }
                 __syncthreads();

@@ -37,7 +37,11 @@ def main():
     wall = time.perf_counter() - t0
     prof = g.profile()
     steps = max(out["steps"], 1)
+    counters = {k: prof.pop(k) for k in ("svd_sweeps", "svd_calls") if k in prof}
     per_step = {k: v / steps / 1e3 for k, v in prof.items()}
+    if counters.get("svd_calls"):
+        per_step["svd_calls_per_step"] = counters["svd_calls"] / steps
+        per_step["svd_sweeps_per_call"] = counters["svd_sweeps"] / counters["svd_calls"]
     hist = out["rank_history"]
     print(json.dumps({"workload": vars(a), "steps": out["steps"], "rank": out["rank"],
                       "rank_max": int(hist.max()), "wall_s": wall, "us_per_step": per_step}))

@@ -155,8 +155,11 @@ class SolverCSD:
         lib = _lib.load()
         out = np.zeros(16)
         m = lib.titus_profile(self.handle(), _lib.as_dp(out), 16)
-        d = {name: out[i] for i, name in enumerate(_lib.PROFILE_NAMES[:m])}
+        nt = len(_lib.PROFILE_NAMES)
+        d = {name: out[i] for i, name in enumerate(_lib.PROFILE_NAMES[:min(m, nt)])}
         d["total"] = float(sum(d.values()))
+        if m >= nt + 2:
+            d["svd_sweeps"], d["svd_calls"] = out[nt], out[nt + 1]
         return d
 
     def _result(self, r_cap):
