@@ -146,9 +146,10 @@ int titus_last_error(char* buf, size_t len);
  * [0] barrier waits, [1] reductions, [2] Jacobi eigensolvers / SVD, [3] Cholesky,
  * [4] basis completion, [5] streaming row passes, [6] scattering and truncation
  * row passes, [7] range-finder / augmentation passes, [8] small-matrix algebra,
- * [9] everything else, [10] boundary inflow, dose half-step and sweep; then, if
- * n >= 13, [11] Jacobi SVD sweeps and [12] SVD calls (counts). Returns the
- * number of entries written. */
+ * [9] everything else, [10] boundary inflow, dose half-step and sweep; then
+ * event counts: [11] Jacobi SVD sweeps, [12] SVD calls, [13] eigensolver calls,
+ * [14] eigensolver sweeps, [15] Cholesky calls, [16] rank-revealing and [17]
+ * certified range-finder sides. Returns the number of entries written (<= n). */
 int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
 
 /* Fixed-rank solve (method TITUS_DLR_FIXED) that allocates nothing. No

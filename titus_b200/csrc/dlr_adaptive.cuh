@@ -329,6 +329,7 @@ static __device__ __noinline__ void aug_prepare(WCtx& x, int s, int goff) {
     si.scale = sqrt(fmax(tr, 0.0));
     const double tol = x.P.rank_tol;
     double rif;
+    prof_count(x.prof, PF_CHOL_CALLS, 1ull);
     const double cond = w_chol(G11, RA, R, Ri, RA, k, &rif);
     double* F1 = sside(x, s, SS_F1);
     double* P1 = sside(x, s, SS_P1);
@@ -341,7 +342,8 @@ static __device__ __noinline__ void aug_prepare(WCtx& x, int s, int goff) {
     } else {
         si.fast1 = 0;
         // G11 is still intact (w_chol copies); Jacobi destroys it
-        w_eig(G11, T, RA, lam, k, x.st.status, raw_gram_floor(k));
+        prof_count(x.prof, PF_EIG_SWEEPS, (unsigned long long)w_eig(G11, T, RA, lam, k, x.st.status, raw_gram_floor(k)));
+        prof_count(x.prof, PF_EIG_CALLS, 1ull);
         int rho = 0;
         for (int j = 0; j < k; ++j) {
             if (sqrt(fmax(lam[j], 0.0)) > tol * si.scale) rho = j + 1;
@@ -474,6 +476,7 @@ static __device__ __noinline__ void rf_finish(WCtx& x, int s, int off) {
     double* Ri = R + RA * RA;
     load_red(x, off, rho, rho, G, RA);
     double rif;
+    prof_count(x.prof, PF_CHOL_CALLS, 1ull);
     const double cond = w_chol(G, RA, R, Ri, RA, rho, &rif);
     if (!(cond < INFINITY) && threadIdx.x == 0) {
         if (atomicCAS(x.st.status, 0, ST_CHOL_BREAKDOWN) == 0) {
@@ -495,7 +498,8 @@ static __device__ __noinline__ void rf_slow_rank(WCtx& x, int s, int off, bool p
     double* V0 = V2 + RA * RA;
     double* nu = x.sm->vec;
     load_red(x, off, k, k, G, RA);
-    w_eig(G, V2, RA, nu, k, x.st.status, kGradedFloor);
+    prof_count(x.prof, PF_EIG_SWEEPS, (unsigned long long)w_eig(G, V2, RA, nu, k, x.st.status, kGradedFloor));
+    prof_count(x.prof, PF_EIG_CALLS, 1ull);
     g_copy(V0, RA, sside(x, s, SS_V0), RA, k, k);
     const double nu0 = sqrt(fmax(nu[0], 0.0));
     const double cut = x.P.rank_tol * (plain ? nu0 : si.scale);
@@ -540,8 +544,10 @@ static __device__ __noinline__ bool range_find(WCtx& x, const bool do_side[2], c
         double* V = Ri + RA * RA;
         load_red(x, s * k * k, k, k, G, RA);
         double rif;
-        const double cond = w_chol(G, RA, R, Ri, RA, k, &rif);
+        prof_count(x.prof, PF_CHOL_CALLS, 1ull);
+    const double cond = w_chol(G, RA, R, Ri, RA, k, &rif);
         const bool ok = cond < kCertW && (plain[s] || 1.0 / rif > 10.0 * tol * si.scale);
+        prof_count(x.prof, ok ? PF_RF_FAST : PF_RF_SLOW, 1ull);
         if (ok) {
             si.fast2 = 1;
             si.rho2 = k;
@@ -549,7 +555,10 @@ static __device__ __noinline__ bool range_find(WCtx& x, const bool do_side[2], c
         } else {
             si.fast2 = 0;
             slow[s] = true;
-            w_eig(G, V, RA, sm->vec, k, x.st.status, raw_gram_floor(k));
+            // first Jacobi of the rank-revealing path: it only separates scales for
+            // the graded Gram of BP V0, whose Jacobi (tolerance 1e-15) fixes nu
+            prof_count(x.prof, PF_EIG_SWEEPS, (unsigned long long)w_eig(G, V, RA, sm->vec, k, x.st.status, raw_gram_floor(k), 1e-8));
+            prof_count(x.prof, PF_EIG_CALLS, 1ull);
             g_copy(sside(x, s, SS_V0), RA, V, RA, k, k);
         }
     }
@@ -1203,12 +1212,15 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
                 // S-step Grams with the 2k-wide bases, two operators per chunk
                 double* acc = sm->work;
                 const int mm = m * m;
-                double* F = sm->work + 2 * mm;
-                for (int d = 0; d < 4; ++d) {   // one operator per chunk: 2 m^2 <= ACCW
-                    w_acc_zero(acc, 2 * mm);
-                    w_grams_pass(x, x.st.X, x.st.W, m, d, d + 1, 0, acc, F, 5 * m, rows_fit(WORKD - 2 * mm, 5 * m));
-                    wpublish_chunk(x, acc, d * mm, mm);             // X side G_d
-                    wpublish_chunk(x, acc + mm, (4 + d) * mm, mm);  // W side C_d
+                // operators per chunk: as many as fit with at least 16 feature rows
+                const int opc = (8 * mm + 16 * 5 * m <= WORKD) ? 4 : ((4 * mm + 16 * 5 * m <= WORKD) ? 2 : 1);
+                double* F = sm->work + 2 * opc * mm;
+                for (int d = 0; d < 4; d += opc) {
+                    w_acc_zero(acc, 2 * opc * mm);
+                    w_grams_pass(x, x.st.X, x.st.W, m, d, d + opc, 0, acc, F, 5 * m,
+                                 rows_fit(WORKD - 2 * opc * mm, 5 * m));
+                    wpublish_chunk(x, acc, d * mm, opc * mm);                   // X side G_d
+                    wpublish_chunk(x, acc + opc * mm, (4 + d) * mm, opc * mm);  // W side C_d
                     __syncthreads();
                 }
                 if (!wreduce(x, 8 * mm)) { aborted = true; break; }

@@ -114,7 +114,7 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     P.prof = nullptr;
     P.zero_smem = 0;
     if (opt && opt->profile) {
-        CK(cudaMemsetAsync(s->prof, 0, 16 * sizeof(unsigned long long), stream));
+        CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));
         P.prof = s->prof;
     }
     WideState& w = s->wst;

@@ -190,8 +190,8 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
     st.info = info;
     st.eta_hist = st.bound_hist = st.time_hist = nullptr;
     if ((rc = s->alloc(&s->d_st, 1))) return cleanup(rc);
-    if ((rc = s->alloc(&s->prof, 16))) return cleanup(rc);
-    CK(cudaMemset(s->prof, 0, 16 * sizeof(unsigned long long)));
+    if ((rc = s->alloc(&s->prof, PF_SLOTS))) return cleanup(rc);
+    CK(cudaMemset(s->prof, 0, PF_SLOTS * sizeof(unsigned long long)));
     CK(cudaDeviceGetAttribute(&s->clock_khz, cudaDevAttrClockRate, s->device));
     CK(cudaMemcpy(s->d_st, &st, sizeof(TeamState), cudaMemcpyHostToDevice));
     CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -253,7 +253,7 @@ static int launch(titus_solver* s, int method, const titus_options_t* opt, int n
     P.prof = nullptr;
     P.zero_smem = getenv("TITUS_ZERO_SMEM") ? 1 : 0;
     if (opt && opt->profile) {
-        CK(cudaMemsetAsync(s->prof, 0, 16 * sizeof(unsigned long long), stream));
+        CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));
         P.prof = s->prof;
     }
     CK(cudaMemsetAsync(s->st.bar, 0, (s->num_sms + 1) * sizeof(unsigned), stream));
@@ -427,16 +427,17 @@ extern "C" int titus_last_error(char* buf, size_t len) {
 
 extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
     if (!s || !ns || n < 0) return fail(TITUS_ERR_ARG, "NULL argument");
-    unsigned long long cyc[16];
+    unsigned long long cyc[PF_SLOTS];
     CK(cudaMemcpy(cyc, s->prof, sizeof(cyc), cudaMemcpyDeviceToHost));
-    const int m = std::min<int>(n, PF_COUNT);
-    for (int i = 0; i < m; ++i) ns[i] = (double)cyc[i] * 1e6 / (double)s->clock_khz;
-    // entries after the timers: SVD sweeps and SVD calls (counts, not times)
-    if (n >= PF_COUNT + 2) {
-        ns[PF_COUNT] = (double)cyc[PF_SVD_SWEEPS];
-        ns[PF_COUNT + 1] = (double)cyc[PF_SVD_CALLS];
-        return PF_COUNT + 2;
-    }
+    // [0, PF_COUNT): phase times (ns); then event counts: SVD sweeps, SVD calls,
+    // eigensolver calls, eigensolver sweeps, Cholesky calls, rank-revealing and
+    // certified range-finder sides
+    const int counters[] = {PF_SVD_SWEEPS, PF_SVD_CALLS, PF_EIG_CALLS, PF_EIG_SWEEPS, PF_CHOL_CALLS, PF_RF_SLOW,
+                            PF_RF_FAST};
+    const int nc = (int)(sizeof(counters) / sizeof(counters[0]));
+    int m = 0;
+    for (int i = 0; i < PF_COUNT && m < n; ++i, ++m) ns[m] = (double)cyc[i] * 1e6 / (double)s->clock_khz;
+    for (int i = 0; i < nc && m < n; ++i, ++m) ns[m] = (double)cyc[counters[i]];
     return m;
 }
 

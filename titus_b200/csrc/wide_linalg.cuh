@@ -86,13 +86,13 @@ static __device__ __noinline__ double w_chol(const double* G, int ldg, double* R
 // Symmetric eigendecomposition by parallel cyclic Jacobi. A (k x k, shared,
 // ld) is destroyed; V (shared, ld) receives the eigenvectors as columns, lam
 // the eigenvalues, both in descending order. k <= RA.
-// A pair is rotated when |a_pq| > 1e-15 sqrt|a_pp a_qq| (relative accuracy on
-// graded matrices) and |a_pq| > rel_floor max_i |a_ii|. A Gram matrix formed
+// A pair is rotated when |a_pq| > rel_tol sqrt|a_pp a_qq| (1e-15: relative
+// accuracy on graded matrices) and |a_pq| > rel_floor max_i |a_ii|. A Gram matrix formed
 // in floating point carries noise of about k eps max|a_ii| that no rotation
 // removes, so raw Grams use rel_floor ~ 4 k eps; graded Grams of already
 // separated directions use a negligible floor.
-static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* lam, int k, int* status,
-                                          double rel_floor) {
+static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* lam, int k, int* status,
+                                         double rel_floor, double rel_tol = 1e-15) {
     __shared__ double rc[RA / 2 + 1], rs[RA / 2 + 1];
     __shared__ int rp[RA / 2 + 1], rq[RA / 2 + 1];
     __shared__ int s_rot[2];
@@ -103,7 +103,7 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
     if (k <= 1) {
         if (threadIdx.x == 0 && k == 1) lam[0] = A[0];
         __syncthreads();
-        return;
+        return 0;
     }
     const int m = k + (k & 1);
     const int npairs = m / 2;
@@ -116,6 +116,7 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
     __syncthreads();
     const double afloor = s_floor;
     bool conv = false;
+    int nsw = 60;
     for (int sweep = 0; sweep < 60; ++sweep) {
         const int par = sweep & 1;
         if (threadIdx.x == 0) s_rot[par] = 0;
@@ -129,12 +130,12 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
                     const double app = A[p * ld + p], aqq = A[q * ld + q];
                     // a rotation whose angle is below eps changes nothing (|a_pq| <= eps max|a|):
                     // skipping it keeps the sweep count finite on rounding-level entries
-                    if (fabs(apq) > afloor && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) &&
+                    if (fabs(apq) > afloor && fabs(apq) > rel_tol * sqrt(fabs(app * aqq)) &&
                         fabs(apq) > 4.4e-16 * fmax(fabs(app), fabs(aqq))) {
                         const double th = (aqq - app) / (2.0 * apq);
                         const double tt = fabs(th) > 1e150 ? 0.5 / th
                                                            : copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0));
-                        c = 1.0 / sqrt(tt * tt + 1.0);
+                        c = rsqrt(tt * tt + 1.0);
                         s = tt * c;
                         s_rot[par] = 1;
                     }
@@ -173,6 +174,7 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
         }
         if (!s_rot[par]) {
             conv = true;
+            nsw = sweep + 1;
             break;
         }
     }
@@ -198,6 +200,7 @@ static __device__ __noinline__ void w_eig(double* A, double* V, int ld, double* 
     for (int e = threadIdx.x; e < k * k; e += NT) V[(e / k) * ld + e % k] = A[(e / k) * ld + e % k];
     for (int j = threadIdx.x; j < k; j += NT) lam[j] = s_lam[s_perm[j]];
     __syncthreads();
+    return nsw;
 }
 
 // One-sided Jacobi SVD of the m x m matrix whose column p is At[p*ld .. +m)
@@ -262,7 +265,7 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
                         fabs(g) > 2.2e-16 * fmax(a, bq)) {
                         const double z = (bq - a) / (2.0 * g);
                         const double tt = fabs(z) > 1e150 ? 0.5 / z : copysign(1.0, z) / (fabs(z) + sqrt(1.0 + z * z));
-                        const double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+                        const double c = rsqrt(1.0 + tt * tt), sn = c * tt;
                         for (int i = gl; i < m; i += LP) {
                             const double u = At[p * ld + i], v = At[q * ld + i];
                             At[p * ld + i] = c * u - sn * v;

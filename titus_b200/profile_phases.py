@@ -37,14 +37,17 @@ def main():
     wall = time.perf_counter() - t0
     prof = g.profile()
     steps = max(out["steps"], 1)
-    counters = {k: prof.pop(k) for k in ("svd_sweeps", "svd_calls") if k in prof}
+    counters = {k: prof.pop(k) for k in _lib.PROFILE_COUNTERS if k in prof}
     per_step = {k: v / steps / 1e3 for k, v in prof.items()}
+    events = {k: v / steps for k, v in counters.items()}
     if counters.get("svd_calls"):
-        per_step["svd_calls_per_step"] = counters["svd_calls"] / steps
-        per_step["svd_sweeps_per_call"] = counters["svd_sweeps"] / counters["svd_calls"]
+        events["svd_sweeps_per_call"] = counters["svd_sweeps"] / counters["svd_calls"]
+    if counters.get("eig_calls"):
+        events["eig_sweeps_per_call"] = counters["eig_sweeps"] / counters["eig_calls"]
     hist = out["rank_history"]
     print(json.dumps({"workload": vars(a), "steps": out["steps"], "rank": out["rank"],
-                      "rank_max": int(hist.max()), "wall_s": wall, "us_per_step": per_step}))
+                      "rank_max": int(hist.max()), "wall_s": wall, "us_per_step": per_step,
+                      "events_per_step": events}))
 
 
 if __name__ == "__main__":

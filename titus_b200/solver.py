@@ -153,13 +153,14 @@ class SolverCSD:
     def profile(self):
         """Per-phase device timers (ns) of the last solve run with profile=True."""
         lib = _lib.load()
-        out = np.zeros(16)
-        m = lib.titus_profile(self.handle(), _lib.as_dp(out), 16)
+        out = np.zeros(32)
+        m = lib.titus_profile(self.handle(), _lib.as_dp(out), 32)
         nt = len(_lib.PROFILE_NAMES)
         d = {name: out[i] for i, name in enumerate(_lib.PROFILE_NAMES[:min(m, nt)])}
         d["total"] = float(sum(d.values()))
-        if m >= nt + 2:
-            d["svd_sweeps"], d["svd_calls"] = out[nt], out[nt + 1]
+        for i, name in enumerate(_lib.PROFILE_COUNTERS):
+            if m > nt + i:
+                d[name] = out[nt + i]
         return d
 
     def _result(self, r_cap):
