@@ -47,7 +47,8 @@ ORACLE_SAMPLE_STEPS = 40
 # DRAM bytes (read + write) per energy step of each kernel on its workload, from
 # one ncu capture of the first energy steps (see profiles/); the per-launch
 # figure scales it to the launch's energy steps.
-DRAM_BYTES_PER_STEP_NCU = {"fixed": (5.010176e6 + 0.218112e6) / 20, "bug": None, "parallel": None}
+DRAM_BYTES_PER_STEP_NCU = {"fixed": (5.010176e6 + 0.218112e6) / 20,
+                           "bug": (70.252288e6 + 149.431552e6) / 20, "parallel": None}
 
 
 def algorithmic_bytes_per_step(n, r, q, w=8):

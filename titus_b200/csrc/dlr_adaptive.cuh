@@ -760,10 +760,10 @@ static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
     ProfScope ps_(x.prof, PF_JACOBI);
     WSmem* sm = x.sm;
     double* At = sm->work;
-    double* Vt = sm->work + KA * KA;
+    double* Vt = sm->work + KA * LDS;
     // keep the SVD input (transposed) for diagnostics
-    g_copy(x.scr + SO_DBG, KA, At, KA, m, m);
-    const int sw = w_svd(At, Vt, KA, m, sm->sig, sm->perm);
+    g_copy(x.scr + SO_DBG, KA, At, LDS, m, m);
+    const int sw = w_svd(At, Vt, LDS, m, sm->sig, sm->perm);
     if (x.prof && threadIdx.x == 0) {
         x.prof[PF_SVD_SWEEPS] += (unsigned long long)(sw > 0 ? sw : 60);
         x.prof[PF_SVD_CALLS] += 1ull;
@@ -790,7 +790,7 @@ static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
     kk = min(kk, x.P.r);
     kk = max(kk, 2);
     kk = min(kk, m);
-    w_svd_complete(At, Vt, KA, m, sm->sig, sm->perm, kk, kNullSvd, x.st.status);
+    w_svd_complete(At, Vt, LDS, m, sm->sig, sm->perm, kk, kNullSvd, x.st.status);
     return kk;
 }
 
@@ -802,15 +802,15 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
     ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     WSmem* sm = x.sm;
     const double* Ut = sm->work;
-    const double* Vt = sm->work + KA * KA;
-    const int tr = rows_fit(WORKD - 2 * KA * KA, 2 * KA);
-    double* t = sm->work + 2 * KA * KA;     // tr x KA
+    const double* Vt = sm->work + KA * LDS;
+    const int tr = rows_fit(WORKD - 2 * KA * LDS, 2 * KA);
+    double* t = sm->work + 2 * KA * LDS;    // tr x KA
     double* o = t + tr * KA;                // tr x KA
     double* v = sm->vec;                    // diag(sig) W_new[0,:]^T
     if (dose_sidx >= 0) {
         for (int j = threadIdx.x; j < kk; j += NT) {
             double a = 0.0;
-            for (int i = 0; i < m; ++i) a = fma(w0[i], Vt[sm->perm[j] * KA + i], a);
+            for (int i = 0; i < m; ++i) a = fma(w0[i], Vt[sm->perm[j] * LDS + i], a);
             v[j] = sm->sig[j] * a;
         }
         __syncthreads();
@@ -825,7 +825,7 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
             __syncthreads();
             for (int e = threadIdx.x; e < nr * kk; e += NT) {
                 const int r = e / kk, j = e - (e / kk) * kk;
-                const double* bj = B + sm->perm[j] * KA;
+                const double* bj = B + sm->perm[j] * LDS;
                 double a = 0.0;
                 for (int i = 0; i < m; ++i) a = fma(t[r * KA + i], bj[i], a);
                 o[r * KA + j] = a;
@@ -1107,7 +1107,7 @@ static __device__ __noinline__ void w_parallel_snew(WCtx& x) {
         else if (i < k) v = ldcg(x.redp + k * k + i * k + (j - k));        // (L^T W~)[i][j-k]
         else if (j < k) v = ldcg(x.redp + (i - k) * k + j);                // (X~^T K)[i-k][j]
         else v = 0.0;
-        At[j * KA + i] = v;
+        At[j * LDS + i] = v;
     }
     __syncthreads();
 }
@@ -1254,7 +1254,7 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
                 __syncthreads();
                 for (int e = threadIdx.x; e < m * m; e += NT) {
                     const int i = e / m, j = e - (e / m) * m;
-                    At[j * KA + i] = Sup[i * KA + j];
+                    At[j * LDS + i] = Sup[i * KA + j];
                 }
                 __syncthreads();
                 const int kk = w_truncate_svd(x, m);
@@ -1374,7 +1374,7 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
                     const int i = e / m, j = e - (e / m) * m;
                     double a = 0.0;
                     for (int l = 0; l < P.q; ++l) a = fma(Xp[i * QW + l], Mt[l * KA + j], a);
-                    At[j * KA + i] = sm->S[i * KA + j] + dE * a;
+                    At[j * LDS + i] = sm->S[i * KA + j] + dE * a;
                 }
                 __syncthreads();
                 // eta = ||Xtpsi[k:, :] MtDW[:, k:]||_F

@@ -242,10 +242,14 @@ __device__ inline void sm_zero(double* D, int m, int n) {
 // Round-robin (tournament) pairing for the parallel cyclic Jacobi method:
 // round t, slot s -> pair (p, q), p < q; returns false for the dummy slot.
 __device__ __forceinline__ bool rr_pair(int m, int t, int s, int k, int& p, int& q) {
-    // positions 0..m-1; position 0 fixed, others rotate by t
+    // positions 0..m-1; position 0 fixed, others rotate by t. For pos >= 1 and
+    // 0 <= t <= m-2 the rotated index lies in [1, 2m-3]: one conditional
+    // subtraction replaces the modulo.
     auto at = [&](int pos) -> int {
         if (pos == 0) return 0;
-        return 1 + ((pos - 1 + (m - 1) - t) % (m - 1));
+        int v = pos - 1 + (m - 1) - t;
+        if (v >= m - 1) v -= m - 1;
+        return 1 + v;
     };
     int a = at(s), b = at(m - 1 - s);
     p = min(a, b);

@@ -18,6 +18,7 @@ namespace wide {
 constexpr int NT = titus::NT;   // threads per CTA
 constexpr int RA = 40;          // max rank entering a step
 constexpr int KA = 2 * RA;      // max augmented width
+constexpr int LDS = KA + 1;     // row stride of the truncation SVD's column arrays (odd: no bank conflicts)
 constexpr int QW = titus::QM;   // psi leading dimension (reduced ordinates <= QW)
 constexpr int TRW = 8;          // rows per staged tile (minimum layout)
 constexpr int TRMAX = 32;       // rows per staged tile when the phase's free shared memory allows
