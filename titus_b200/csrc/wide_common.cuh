@@ -21,7 +21,7 @@ constexpr int KA = 2 * RA;      // max augmented width
 constexpr int LDS = KA + 1;     // row stride of the truncation SVD's column arrays (odd: no bank conflicts)
 constexpr int QW = titus::QM;   // psi leading dimension (reduced ordinates <= QW)
 constexpr int TRW = 8;          // rows per staged tile (minimum layout)
-constexpr int TRMAX = 32;       // rows per staged tile when the phase's free shared memory allows
+constexpr int TRMAX = 128;      // rows per staged tile when the phase's free shared memory allows
 constexpr int PMAXW = 8 * KA * KA;   // largest reduction (BUG S-step Grams): 51200 doubles
 constexpr int WORKD = 20480;    // shared work area (doubles)
 constexpr int ACCW = 16384;     // accumulator chunk (doubles), inside the work area
