@@ -165,6 +165,7 @@ def run_gpu(args, rank, world, local_rank):
 
     from titus_b200 import Settings, SolverCSD
     from titus_b200 import _lib
+    from titus_b200.replicas import replica_throughput
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -213,12 +214,7 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     _lib.check(lib.titus_fetch(h, C.byref(res)), "titus_fetch")
-    t_max = elapsed
-    if dist:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * args.steps / t_max
+    value, t_max = replica_throughput(args.steps, elapsed, world, device="cuda")
     ms_per_step = t_max / args.steps * 1e3
 
     # end-to-end: one-shot C-ABI call with host buffers (upload, solve, copy-out)
@@ -235,11 +231,7 @@ def run_gpu(args, rank, world, local_rank):
         _lib.check(lib.titus_solve_problem(C.byref(p), method, C.byref(opt), C.byref(res2)),
                    "titus_solve_problem")
     t_e2e = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e_value = world * e2e_steps / t_e2e
+    e2e_value, t_e2e = replica_throughput(e2e_steps, t_e2e, world, device="cuda")
 
     n, q = solver.n, solver.q
     steps_per_solve = int(res.steps_done)
