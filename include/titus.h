@@ -135,6 +135,29 @@ int titus_set_state(titus_solver_t* solver, int32_t rank, const double* X, const
 int titus_solve_from(titus_solver_t* solver, int32_t method, const titus_options_t* options,
                      int32_t n_stop, titus_result_t* result);
 
+/* One pencil beam of a batched solve: its own energy grid (5 MeV -> cutoff
+ * grid of the base problem replaced by this spot's) and entry profile. All
+ * spots share the base problem's phantom, P_N operators, quadrature and
+ * reduced ordinates. Arrays are host memory, copied by the call. */
+typedef struct titus_spot {
+    int32_t n_energies;        /* nE of this spot's grid */
+    double d_e;                /* its tau step (e_trafo[1] - e_trafo[0]) */
+    const double* stopping;    /* nE */
+    const double* bc_energy;   /* nE: PsiBeam energy factor */
+    const double* sigma;       /* nE x (npn+1) */
+    const double* bc_space;    /* n: PsiBeam spatial factor (entry point of this spot) */
+} titus_spot_t;
+
+/* Batched pencil-beam solves (no counterpart in the reference, which solves
+ * one beam per Solve* call): all `nspots` spots advance in one persistent
+ * launch, options->team_ctas CTAs per spot (default 1) and as many spots at a
+ * time as the GPU holds teams. method: TITUS_PARALLEL_ADAPTIVE or
+ * TITUS_BUG_ADAPTIVE; options->max_steps bounds each spot's loop.
+ * dose_out: nspots x n (row s = dose of spot s); rank_out / iters_out
+ * (nspots, optional): final rank and loop iterations per spot. */
+int titus_solve_batched(titus_solver_t* solver, int32_t method, const titus_options_t* options, int32_t nspots,
+                        const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out);
+
 void titus_destroy(titus_solver_t* solver);
 
 /* Copy the last error message of this thread into buf (always terminated). */

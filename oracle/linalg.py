@@ -28,9 +28,29 @@ def svd_full(A: np.ndarray):
     return U, s, Vt.T
 
 
+def svd_jacobi(A: np.ndarray):
+    """SVD of a square matrix by LAPACK's preconditioned one-sided Jacobi
+    (dgejsv, JOBA='F': high relative accuracy). ``truncate!``'s l1 tail rule
+    keeps directions with sigma / sigma_1 down to ~1e-10; a Householder SVD
+    (gesdd) determines their vectors only to eps sigma_1 / sigma_j, a one-sided
+    Jacobi SVD to a few eps. Returns (U, s, V), s descending."""
+    import scipy.linalg.lapack as lapack
+
+    m = A.shape[0]
+    if m == 0 or not np.any(A):
+        return np.eye(m), np.zeros(m), np.eye(m)
+    sva, u, v, work, _, info = lapack.dgejsv(np.asarray(A, dtype=np.float64, order="F"), joba=2, jobu=0, jobv=0,
+                                              jobr=1, jobt=0, jobp=0)
+    if info != 0:
+        raise RuntimeError(f"dgejsv failed (info {info})")
+    scale = work[1] / work[0] if work[0] != 0 else 1.0
+    return u[:, :m], sva[:m] * scale, v[:, :m]
+
+
 def svd_det(A: np.ndarray, tol: float | None = None):
     """Thin SVD (U, s, V) with the deterministic null-space rule.
 
+    Computed by the one-sided Jacobi SVD (``svd_jacobi``) for relative accuracy.
     Singular vectors of singular values ``s_j <= tol * s_1`` are not fixed by A
     (LAPACK returns rounding-noise directions there). ``truncate!`` keeps such
     directions whenever its l1 tail test or its lower clamp reaches them, so
@@ -39,8 +59,7 @@ def svd_det(A: np.ndarray, tol: float | None = None):
     returned as computed.
     """
     tol = RANK_TOL if tol is None else tol
-    U, s, Vt = np.linalg.svd(A, full_matrices=False)
-    V = Vt.T
+    U, s, V = svd_jacobi(A)
     m = s.size
     rho = int(np.sum(s > tol * s[0])) if m and s[0] > 0 else 0
     if rho < m:

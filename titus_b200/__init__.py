@@ -1,4 +1,4 @@
 """titus_b200: B200-native (sm_100a) CSD energy step of TITUS behind its Settings/SolverCSD/Solve* API."""
 from .settings import Settings  # noqa: F401
-from .solver import (SolverCSD, SolveFirstCollisionSourceDLR, SolveFirstCollisionSourceDLRBUGRejection,  # noqa: F401
-                     SolveFirstCollisionSourceDLRParallel, scalar_flux)
+from .solver import (SolveBatchedPencilBeams, SolverCSD, SolveFirstCollisionSourceDLR,  # noqa: F401
+                     SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel, scalar_flux)

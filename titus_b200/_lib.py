@@ -55,6 +55,11 @@ class Result(C.Structure):
     ]
 
 
+class Spot(C.Structure):
+    _fields_ = [("n_energies", C.c_int32), ("d_e", C.c_double), ("stopping", _dp), ("bc_energy", _dp),
+                ("sigma", _dp), ("bc_space", _dp)]
+
+
 # (name, restype, argtypes) for every symbol include/titus.h declares
 SIGNATURES = [
     ("titus_create", C.c_int, [C.POINTER(Problem), C.POINTER(C.c_void_p)]),
@@ -64,6 +69,8 @@ SIGNATURES = [
     ("titus_solve_problem", C.c_int, [C.POINTER(Problem), C.c_int32, C.POINTER(Options), C.POINTER(Result)]),
     ("titus_set_state", C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _dp, _dp, _dp, C.c_int32]),
     ("titus_solve_from", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_int32, C.POINTER(Result)]),
+    ("titus_solve_batched", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_int32, C.POINTER(Spot), _dp,
+                                      _ip, _ip]),
     ("titus_destroy", None, [C.c_void_p]),
     ("titus_last_error", C.c_int, [C.c_char_p, C.c_size_t]),
     ("titus_profile", C.c_int, [C.c_void_p, _dp, C.c_int32]),

@@ -1113,36 +1113,26 @@ static __device__ __noinline__ void w_parallel_snew(WCtx& x) {
 }
 
 // ---------------------------------------------------------------- kernel ---
+// Loop state of one solve, carried into and out of energy_loop.
+struct LoopState {
+    int psi_idx;
+    double t;
+    int iters;
+    int eta_count;
+    int n;          // on return: first energy index not processed
+    bool aborted;
+};
+
+// The energy loop of one solve on this team (METHOD 1: n = n_begin..n_end;
+// METHOD 2: the BUG while-loop with rejections), from the state in x / ls.
 template <int METHOD>
-__global__ void __launch_bounds__(NT, 1)
-adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, int max_iters) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    WSmem* sm = reinterpret_cast<WSmem*>(smem_raw);
-    WCtx x;
-    x.P = P;
-    x.G = G;
-    x.b = blockIdx.x;
-    x.st = states[0];
-    x.sm = sm;
-    x.scr = x.st.scr + (size_t)x.b * SCRW;
-    x.prof = (blockIdx.x == 0) ? P.prof : nullptr;
-    x.gen = 0;
-    x.parity = 0;
-    x.redp = x.st.red;
-    x.cur_n = 0;
-    prof_begin(x.prof);
-    ProfScope ps_total(x.prof, PF_TOTAL);
-    x.c0 = (int)((long long)x.b * P.n / G);
-    x.c1 = (int)((long long)(x.b + 1) * P.n / G);
-    x.m0 = (int)((long long)x.b * P.N / G);
-    x.m1 = (int)((long long)(x.b + 1) * P.N / G);
-    x.r = ldcg(x.st.info + 0);
-    int psi_idx = ldcg(x.st.info + 2);
-    for (int e = threadIdx.x; e < KA * KA; e += NT) sm->S[e] = ldcg(x.st.S + e);
-    __syncthreads();
-    double t = ldcg(x.st.tvar);
-    int iters = 0;
-    int eta_count = ldcg(x.st.info + 4);
+static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end, int max_iters, LoopState& ls) {
+    WSmem* sm = x.sm;
+    const DevProblem& P = x.P;
+    int psi_idx = ls.psi_idx;
+    double t = ls.t;
+    int iters = ls.iters;
+    int eta_count = ls.eta_count;
     const double dE = P.dE;
     const int nE = P.nE;
     bool aborted = false;
@@ -1422,18 +1412,153 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
             break;
         }
     }
+    ls.psi_idx = psi_idx;
+    ls.t = t;
+    ls.iters = iters;
+    ls.eta_count = eta_count;
+    ls.n = n;
+    ls.aborted = aborted;
+}
+
+template <int METHOD>
+__global__ void __launch_bounds__(NT, 1)
+adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, int max_iters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WSmem* sm = reinterpret_cast<WSmem*>(smem_raw);
+    WCtx x;
+    x.P = P;
+    x.G = G;
+    x.b = blockIdx.x;
+    x.st = states[0];
+    x.sm = sm;
+    x.scr = x.st.scr + (size_t)x.b * SCRW;
+    x.prof = (blockIdx.x == 0) ? P.prof : nullptr;
+    x.gen = 0;
+    x.parity = 0;
+    x.redp = x.st.red;
+    x.cur_n = 0;
+    prof_begin(x.prof);
+    ProfScope ps_total(x.prof, PF_TOTAL);
+    x.c0 = (int)((long long)x.b * P.n / G);
+    x.c1 = (int)((long long)(x.b + 1) * P.n / G);
+    x.m0 = (int)((long long)x.b * P.N / G);
+    x.m1 = (int)((long long)(x.b + 1) * P.N / G);
+    x.r = ldcg(x.st.info + 0);
+    for (int e = threadIdx.x; e < KA * KA; e += NT) sm->S[e] = ldcg(x.st.S + e);
+    __syncthreads();
+    LoopState ls;
+    ls.psi_idx = ldcg(x.st.info + 2);
+    ls.t = ldcg(x.st.tvar);
+    ls.iters = 0;
+    ls.eta_count = ldcg(x.st.info + 4);
+    ls.n = n_begin;
+    ls.aborted = false;
+    energy_loop<METHOD>(x, n_begin, n_end, max_iters, ls);
     if (x.b == 0) {
         for (int e = threadIdx.x; e < KA * KA; e += NT) x.st.S[e] = sm->S[e];
         if (threadIdx.x == 0) {
             x.st.info[0] = x.r;
-            x.st.info[1] = iters;
-            x.st.info[2] = psi_idx;
-            x.st.info[3] = n;   // first energy index not processed
-            x.st.info[4] = eta_count;
-            x.st.tvar[0] = t;
+            x.st.info[1] = ls.iters;
+            x.st.info[2] = ls.psi_idx;
+            x.st.info[3] = ls.n;   // first energy index not processed
+            x.st.info[4] = ls.eta_count;
+            x.st.tvar[0] = ls.t;
         }
     }
-    (void)aborted;
+}
+
+
+// Per-spot tables of a batched launch (pencil beams with their own energy and
+// entry point): the energy grid and everything indexed by it, and the beam's
+// spatial profile. All spots share the phantom, the P_N operators and dE's rule.
+struct SpotData {
+    int nE;                    // energies of this spot's grid
+    int n_end;                 // last energy index to run (parallel integrator)
+    double dE;                 // its tau step
+    const double* stopping;    // nE
+    const double* bc_energy;   // nE
+    const double* sigma;       // nE x (npn+1)
+    const double* bc_space;    // n
+    double* dose;              // n (output)
+    int* result;               // [rank, iterations]
+};
+
+// Initial factors of one spot (SolverCSD.jl:1728-1760, :2013-2050) on this
+// CTA's own rows: X, W = first r0 identity columns (X's boundary rows zero),
+// S = 0, psi = 0, dose = 0.
+static __device__ __noinline__ void init_spot(WCtx& x, int r0) {
+    const DevProblem& P = x.P;
+    for (int e = threadIdx.x; e < (x.c1 - x.c0) * KA; e += NT) x.st.X[(size_t)x.c0 * KA + e] = 0.0;
+    for (int e = threadIdx.x; e < (x.m1 - x.m0) * KA; e += NT) x.st.W[(size_t)x.m0 * KA + e] = 0.0;
+    for (int e = threadIdx.x; e < (x.c1 - x.c0) * QW; e += NT) {
+        x.st.psi0[(size_t)x.c0 * QW + e] = 0.0;
+        x.st.psi1[(size_t)x.c0 * QW + e] = 0.0;
+    }
+    for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT) x.st.dose[c] = 0.0;
+    for (int e = threadIdx.x; e < KA * KA; e += NT) x.sm->S[e] = 0.0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < r0; j += NT) {
+        if (j >= x.c0 && j < x.c1) x.st.X[(size_t)j * KA + j] = is_bnd_w(P, j) ? 0.0 : 1.0;
+        if (j >= x.m0 && j < x.m1) x.st.W[(size_t)j * KA + j] = 1.0;
+    }
+    __syncthreads();
+}
+
+// Batched solves: T teams of G CTAs; team t solves spots t, t+T, ... one after
+// the other with the same integrator, re-initialising its factors on the
+// device between spots. Each spot's dose goes to its own output buffer.
+template <int METHOD>
+__global__ void __launch_bounds__(NT, 1)
+adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const SpotData* spots, int nspots, int r0,
+                        int max_iters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WSmem* sm = reinterpret_cast<WSmem*>(smem_raw);
+    const int team = blockIdx.x / G;
+    WCtx x;
+    x.P = P0;
+    x.G = G;
+    x.b = blockIdx.x - team * G;
+    x.st = states[team];
+    x.sm = sm;
+    x.scr = x.st.scr + (size_t)x.b * SCRW;
+    x.prof = (blockIdx.x == 0) ? P0.prof : nullptr;
+    x.gen = 0;
+    x.parity = 0;
+    x.redp = x.st.red;
+    x.cur_n = 0;
+    prof_begin(x.prof);
+    ProfScope ps_total(x.prof, PF_TOTAL);
+    x.c0 = (int)((long long)x.b * P0.n / G);
+    x.c1 = (int)((long long)(x.b + 1) * P0.n / G);
+    x.m0 = (int)((long long)x.b * P0.N / G);
+    x.m1 = (int)((long long)(x.b + 1) * P0.N / G);
+    for (int sidx = team; sidx < nspots; sidx += T) {
+        const SpotData sp = spots[sidx];
+        x.P = P0;
+        x.P.nE = sp.nE;
+        x.P.dE = sp.dE;
+        x.P.stopping = sp.stopping;
+        x.P.bc_energy = sp.bc_energy;
+        x.P.sigma = sp.sigma;
+        x.P.bc_space = sp.bc_space;
+        x.st.dose = sp.dose;
+        init_spot(x, r0);
+        x.r = r0;
+        if (!wsync(x)) return;
+        LoopState ls;
+        ls.psi_idx = 0;
+        ls.t = 0.0;
+        ls.iters = 0;
+        ls.eta_count = 0;
+        ls.n = 2;
+        ls.aborted = false;
+        energy_loop<METHOD>(x, 2, sp.n_end, max_iters, ls);
+        if (ls.aborted) return;
+        if (x.b == 0 && threadIdx.x == 0) {
+            sp.result[0] = x.r;
+            sp.result[1] = ls.iters;
+        }
+    }
 }
 
 }  // namespace wide

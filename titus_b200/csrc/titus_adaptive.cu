@@ -6,6 +6,7 @@
 #include <climits>
 #include <cmath>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "titus_handle.h"
@@ -270,8 +271,167 @@ int titus_host::wide_set_state(titus_solver* s, int rank, const double* X, const
     return TITUS_OK;
 }
 
+
+namespace {
+
+struct DevTemps {
+    std::vector<void*> ptrs;
+    ~DevTemps() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <class T>
+    int alloc(T** p, size_t count, const T* host = nullptr) {
+        int rc = titus_host::upload(p, host, count);
+        if (rc == TITUS_OK && *p) ptrs.push_back((void*)*p);
+        return rc;
+    }
+};
+
+int ensure_batch_states(titus_solver* s, int T, int G) {
+    if (s->d_bst && s->b_teams >= T && s->b_G == G) return TITUS_OK;
+    for (void* p : s->batch_allocs) cudaFree(p);
+    s->batch_allocs.clear();
+    s->d_bst = nullptr;
+    const int n = s->n, N = s->N;
+    auto al = [&](auto** p, size_t count) -> int {
+        using Elem = std::remove_pointer_t<std::remove_reference_t<decltype(*p)>>;
+        int rc = titus_host::upload(p, static_cast<const Elem*>(nullptr), count);
+        if (rc == TITUS_OK && *p) s->batch_allocs.push_back((void*)*p);
+        return rc;
+    };
+    int* status = nullptr;
+    double* diag = nullptr;
+    int rc;
+    if ((rc = al(&status, 1)) || (rc = al(&diag, 16))) return rc;
+    s->bst.assign(T, WideState{});
+    for (int t = 0; t < T; ++t) {
+        WideState& w = s->bst[t];
+        if ((rc = al(&w.X, (size_t)n * KA)) || (rc = al(&w.W, (size_t)N * KA)) || (rc = al(&w.K, (size_t)n * RA)) ||
+            (rc = al(&w.KP, (size_t)n * RA)) || (rc = al(&w.CX, (size_t)n * RA)) || (rc = al(&w.L, (size_t)N * RA)) ||
+            (rc = al(&w.LP, (size_t)N * RA)) || (rc = al(&w.CW, (size_t)N * RA)) ||
+            (rc = al(&w.psi0, (size_t)n * QW)) || (rc = al(&w.psi1, (size_t)n * QW)) ||
+            (rc = al(&w.S, (size_t)KA * KA)) || (rc = al(&w.part, (size_t)2 * G * PMAXW)) ||
+            (rc = al(&w.red, (size_t)2 * PMAXW)) || (rc = al(&w.scr, (size_t)G * SCRW)) ||
+            (rc = al(&w.bar, (size_t)G + 1)) || (rc = al(&w.info, 8)) || (rc = al(&w.tvar, 1)))
+            return rc;
+        w.dose = nullptr;          // per spot
+        w.status = status;         // shared: a failing team stops the batch
+        w.diag = diag;
+        w.rank_hist = nullptr;
+        w.time_hist = w.eta_hist = w.bound_hist = nullptr;
+        w.hist_cap = 0;
+    }
+    WideState* d = nullptr;
+    if ((rc = al(&d, (size_t)T))) return rc;
+    CK(cudaMemcpy(d, s->bst.data(), T * sizeof(WideState), cudaMemcpyHostToDevice));
+    s->d_bst = d;
+    s->b_teams = T;
+    s->b_G = G;
+    CK(cudaFuncSetAttribute(adaptive_batched_kernel<TITUS_PARALLEL_ADAPTIVE>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WSmem)));
+    CK(cudaFuncSetAttribute(adaptive_batched_kernel<TITUS_BUG_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(WSmem)));
+    return TITUS_OK;
+}
+
+}  // namespace
+
+int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots,
+                                   const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
+    const int n = s->n, npn1 = s->P.npn + 1;
+    for (int i = 0; i < nspots; ++i) {
+        const titus_spot_t& sp = spots[i];
+        if (sp.n_energies < 2) return fail(TITUS_ERR_ARG, "spot %d: n_energies < 2", i);
+        if (!(sp.d_e > 0)) return fail(TITUS_ERR_ARG, "spot %d: d_e must be > 0", i);
+        if (!sp.stopping || !sp.bc_energy || !sp.sigma || !sp.bc_space)
+            return fail(TITUS_ERR_ARG, "spot %d: a table is NULL", i);
+    }
+    const int r0 = s->r / 2;
+    if (r0 < 1) return fail(TITUS_ERR_ARG, "adaptive integrators need settings.r >= 2 (got %d)", s->r);
+    if (r0 > RA) return fail(TITUS_ERR_LIMIT, "initial rank %d > %d", r0, RA);
+    if (2 * r0 > s->N) return fail(TITUS_ERR_ARG, "augmented width %d exceeds the %d moments", 2 * r0, s->N);
+    int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : 1;
+    G = std::max(1, std::min(G, s->num_sms));
+    int per_sm = 0;
+    auto kfun = method == TITUS_PARALLEL_ADAPTIVE ? adaptive_batched_kernel<TITUS_PARALLEL_ADAPTIVE>
+                                                  : adaptive_batched_kernel<TITUS_BUG_ADAPTIVE>;
+    CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WSmem)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, wide::NT, sizeof(WSmem)));
+    if (per_sm < 1) return fail(TITUS_ERR_CUDA, "batched kernel does not fit on an SM");
+    const int T = std::max(1, std::min(nspots, per_sm * s->num_sms / G));
+    int rc = ensure_batch_states(s, T, G);
+    if (rc) return rc;
+    // per-spot tables, concatenated
+    size_t tot_e = 0;
+    for (int i = 0; i < nspots; ++i) tot_e += (size_t)spots[i].n_energies;
+    DevTemps tmp;
+    double *d_stop, *d_bce, *d_sig, *d_bcs, *d_dose;
+    int* d_res;
+    if ((rc = tmp.alloc(&d_stop, tot_e)) || (rc = tmp.alloc(&d_bce, tot_e)) ||
+        (rc = tmp.alloc(&d_sig, tot_e * npn1)) || (rc = tmp.alloc(&d_bcs, (size_t)nspots * n)) ||
+        (rc = tmp.alloc(&d_dose, (size_t)nspots * n)) || (rc = tmp.alloc(&d_res, (size_t)2 * nspots)))
+        return rc;
+    std::vector<SpotData> sd(nspots);
+    size_t off = 0;
+    for (int i = 0; i < nspots; ++i) {
+        const titus_spot_t& sp = spots[i];
+        const int nE = sp.n_energies;
+        CK(cudaMemcpy(d_stop + off, sp.stopping, nE * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_bce + off, sp.bc_energy, nE * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_sig + off * npn1, sp.sigma, (size_t)nE * npn1 * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_bcs + (size_t)i * n, sp.bc_space, n * sizeof(double), cudaMemcpyHostToDevice));
+        SpotData& d = sd[i];
+        d.nE = nE;
+        d.n_end = nE;
+        if (method == TITUS_PARALLEL_ADAPTIVE && opt && opt->max_steps > 0) d.n_end = std::min(nE, 1 + opt->max_steps);
+        d.dE = sp.d_e;
+        d.stopping = d_stop + off;
+        d.bc_energy = d_bce + off;
+        d.sigma = d_sig + off * npn1;
+        d.bc_space = d_bcs + (size_t)i * n;
+        d.dose = d_dose + (size_t)i * n;
+        d.result = d_res + 2 * i;
+        off += nE;
+    }
+    SpotData* d_sd;
+    if ((rc = tmp.alloc(&d_sd, (size_t)nspots, sd.data()))) return rc;
+    int max_iters = INT_MAX;
+    if (method == TITUS_BUG_ADAPTIVE && opt && opt->max_steps > 0) max_iters = opt->max_steps;
+    for (int t = 0; t < T; ++t) CK(cudaMemset(s->bst[t].bar, 0, (size_t)(G + 1) * sizeof(unsigned)));
+    CK(cudaMemset(s->bst[0].status, 0, sizeof(int)));
+    CK(cudaMemset(s->bst[0].diag, 0, 16 * sizeof(double)));
+    DevProblem P = s->P;
+    if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
+    P.prof = nullptr;
+    P.zero_smem = 0;
+    if (opt && opt->profile) {
+        CK(cudaMemset(s->prof, 0, PF_SLOTS * sizeof(unsigned long long)));
+        P.prof = s->prof;
+    }
+    WideState* dst = s->d_bst;
+    int Tl = T, Gl = G, ns = nspots, r0l = r0;
+    void* args[] = {&P, &dst, &Gl, &Tl, &d_sd, &ns, &r0l, &max_iters};
+    CK(cudaLaunchCooperativeKernel((void*)kfun, dim3(T * G), dim3(wide::NT), args, sizeof(WSmem), nullptr));
+    CK(cudaDeviceSynchronize());
+    int status = 0;
+    CK(cudaMemcpy(&status, s->bst[0].status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) return fail(status == ST_LIMIT ? TITUS_ERR_LIMIT : TITUS_ERR_DEVICE,
+                                 "batched solve: device status %d (teams %d x %d CTAs)", status, T, G);
+    CK(cudaMemcpy(dose_out, d_dose, (size_t)nspots * n * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int> res(2 * nspots);
+    CK(cudaMemcpy(res.data(), d_res, res.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nspots; ++i) {
+        if (rank_out) rank_out[i] = res[2 * i];
+        if (iters_out) iters_out[i] = res[2 * i + 1];
+    }
+    return TITUS_OK;
+}
+
 void titus_host::wide_free(titus_solver* s) {
     for (void* p : s->wide_allocs) cudaFree(p);
     s->wide_allocs.clear();
     s->d_wst = nullptr;
+    for (void* p : s->batch_allocs) cudaFree(p);
+    s->batch_allocs.clear();
+    s->d_bst = nullptr;
 }

@@ -417,6 +417,16 @@ extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_o
     return titus_fetch(s, res);
 }
 
+extern "C" int titus_solve_batched(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t nspots,
+                                   const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
+    if (!s || !spots || !dose_out) return fail(TITUS_ERR_ARG, "NULL argument");
+    if (method != TITUS_PARALLEL_ADAPTIVE && method != TITUS_BUG_ADAPTIVE)
+        return fail(TITUS_ERR_ARG, "batched solves run the adaptive integrators (method 1 or 2), got %d", method);
+    if (nspots < 1) return fail(TITUS_ERR_ARG, "nspots < 1");
+    s->last_method = method;
+    return titus_host::wide_solve_batched(s, method, opt, nspots, spots, dose_out, rank_out, iters_out);
+}
+
 extern "C" void titus_destroy(titus_solver_t* s) { delete s; }
 
 extern "C" int titus_last_error(char* buf, size_t len) {

@@ -36,6 +36,8 @@ int wide_fetch(titus_solver* s, titus_result_t* res);
 int wide_set_state(titus_solver* s, int rank, const double* X, const double* S, const double* W, const double* psi,
                    const double* dose, int n_next);
 void wide_free(titus_solver* s);
+int wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots, const titus_spot_t* spots,
+                       double* dose_out, int32_t* rank_out, int32_t* iters_out);
 
 }  // namespace titus_host
 
@@ -58,6 +60,11 @@ struct titus_solver {
     titus::wide::WideState wst{};
     titus::wide::WideState* d_wst = nullptr;
     std::vector<void*> wide_allocs;
+    // batched teams (allocated on first batched solve, grown on demand)
+    std::vector<titus::wide::WideState> bst;
+    titus::wide::WideState* d_bst = nullptr;
+    int b_teams = 0, b_G = 0;
+    std::vector<void*> batch_allocs;
     int wide_state_valid = 0;   // 1 after an adaptive solve or titus_set_state
 
     template <class T>

@@ -16,6 +16,7 @@ The energy loop itself always runs on the GPU; there is no CPU path.
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import math
 
@@ -80,6 +81,53 @@ class SolverCSD:
         self.dose = np.zeros(self.n)
         self._handle = None
         self._keep = None
+
+    def beam_tables(self, energy: float, y0: float):
+        """Energy grid and PsiBeam tables of a pencil beam entering at (x0, y0)
+        with energy ``energy`` on this solver's phantom (``CSD.jl:47-89``,
+        ``SolverCSD.jl:240-276``): (nE, dE, stopping, bc_energy, sigma, bc_space)."""
+        s2 = copy.copy(self.settings)
+        s2.eMax = float(energy)
+        s2.y0 = float(y0)
+        eGrid, eTrafo, S = ph.energy_grid(s2)
+        ang = np.exp(-s2.sigmaO1Inv * (s2.Omega1 - self.Q_points[:, 0]) ** 2) * \
+            np.exp(-s2.sigmaO3Inv * (s2.Omega3 - self.Q_points[:, 2]) ** 2)
+        scale = s2.psi_scale / ang.max() if s2.beam_peak_normalized else s2.psi_scale
+        bc_energy = scale * np.exp(-s2.sigmaEInv * (s2.eMax - eGrid) ** 2) * S * s2.densityMin
+        ny = s2.NCellsY
+        xm = s2.xMid[np.arange(self.n) // ny]
+        ym = s2.yMid[np.arange(self.n) % ny]
+        bc_space = np.exp(-s2.sigmaXInv * (xm - s2.x0) ** 2) * np.exp(-s2.sigmaYInv * (ym - s2.y0) ** 2)
+        sig = np.array([s2.sigmaT_hg * s2.hg_g**l for l in range(s2.nPN + 1)])
+        sigma = np.ascontiguousarray(np.tile(sig, (eTrafo.size, 1)))
+        return (eTrafo.size, float(eTrafo[1] - eTrafo[0]), np.ascontiguousarray(S), np.ascontiguousarray(bc_energy),
+                sigma, np.ascontiguousarray(bc_space))
+
+    def solve_batched(self, spots, method: int = _lib.TITUS_BUG_ADAPTIVE, team_ctas: int = 1, max_steps: int = 0):
+        """All pencil beams ``spots`` = [(energy, y0), ...] in one persistent
+        launch (titus_solve_batched). Returns (dose (nspots x n), rank, iterations)."""
+        lib = _lib.load()
+        h = self.handle()
+        ns = len(spots)
+        arr = (_lib.Spot * ns)()
+        keep = []
+        for i, (e, y) in enumerate(spots):
+            nE, dE, S, bce, sig, bcs = self.beam_tables(e, y)
+            keep += [S, bce, sig, bcs]
+            arr[i].n_energies = nE
+            arr[i].d_e = dE
+            arr[i].stopping = _lib.as_dp(S)
+            arr[i].bc_energy = _lib.as_dp(bce)
+            arr[i].sigma = _lib.as_dp(sig)
+            arr[i].bc_space = _lib.as_dp(bcs)
+        dose = np.zeros((ns, self.n))
+        rank = np.zeros(ns, dtype=np.int32)
+        iters = np.zeros(ns, dtype=np.int32)
+        opt = self.options(max_steps)
+        opt.team_ctas = team_ctas
+        _lib.check(lib.titus_solve_batched(h, method, C.byref(opt), ns, arr, _lib.as_dp(dose), _lib.as_ip(rank),
+                                           _lib.as_ip(iters)), "titus_solve_batched")
+        return dose, rank, iters
 
     # -------------------------------------------------------------- device
     def problem_struct(self):
@@ -278,6 +326,14 @@ def SolveFirstCollisionSourceDLRBUGRejection(solver: SolverCSD, recordGif: bool 
     eta_hist = np.column_stack([np.full(ne, np.nan), eta])
     bound_hist = np.column_stack([np.full(ne, np.nan), bound])
     return res[0], res[1], res[2], res[3], res[4], rank_hist, eta_hist, bound_hist, res[5]
+
+
+def SolveBatchedPencilBeams(solver: SolverCSD, spots, method: str = "bug", team_ctas: int = 1,
+                            max_steps: int = 0):
+    """Many pencil beams (energy, entry y0) on one phantom in one persistent
+    launch; returns (dose per spot (nspots x n), final rank, loop iterations)."""
+    mid = {"bug": _lib.TITUS_BUG_ADAPTIVE, "parallel": _lib.TITUS_PARALLEL_ADAPTIVE}[method]
+    return solver.solve_batched(spots, mid, team_ctas, max_steps)
 
 
 def scalar_flux(X, sigma, WV):
