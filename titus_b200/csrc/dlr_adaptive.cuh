@@ -653,25 +653,30 @@ static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, 
 
 // Materialise the new directions: A[:, k:2k] = [C RI | completion]; with
 // `with_q1` also A[:, :k] = Q1 = [A F1 | completion] (BUG). Row tile t holds
-// [old A (k) | Q1 (k) | X~ (k)] per row.
-static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q1) {
+// [old A (k) | Q1 (k) | X~ (k) | B (k)] per row (ld 4RA). With `acc`, the
+// parallel integrator's S blocks are accumulated on the way: X side
+// acc[0..k^2) += X~^T K, W side acc[k^2..2k^2) += L^T W~.
+static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q1, double* acc) {
     ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
     WSmem* sm = x.sm;
     SideBufs sb = side_bufs(x, s);
     const SideInfo& si = x.side[s];
-    double* F1 = sm->work;                   // k x k
+    constexpr int LT = 4 * RA;               // tile leading dimension
+    double* F1 = sm->work + 2 * RA * RA;     // k x k (after the 2k^2 accumulator)
     double* Ri = F1 + RA * RA;               // rho2 x rho2
-    const int tr = rows_fit(WORKD - 2 * RA * RA, 4 * RA);
-    double* t = Ri + RA * RA;                // tr x 3RA
-    double* cb = t + tr * 3 * RA;            // tr x RA (C rows)
+    const int tr = rows_fit(WORKD - 4 * RA * RA, LT + RA);
+    double* t = Ri + RA * RA;                // tr x 4RA
+    double* cb = t + tr * LT;                // tr x RA (C rows)
+    const GBlock blk = s == 0 ? GBlock{2 * k, k, 3 * k, k, 0} : GBlock{3 * k, k, 2 * k, k, k * k};
     g_copy(F1, RA, sside(x, s, SS_F1), RA, k, k);
     if (si.rho2 > 0) g_copy(Ri, RA, sside(x, s, SS_RI), RA, si.rho2, si.rho2);
     const double* wc = sside(x, 1, SS_WC);
     const int rho1 = si.rho1, rho2 = si.rho2;
     for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
         const int nr = min(tr, sb.r1 - r0);
-        wload(t, 3 * RA, 0, sb.A, KA, 0, r0, nr, k);
+        wload(t, LT, 0, sb.A, KA, 0, r0, nr, k);
+        if (acc) wload(t, LT, 3 * k, sb.B, RA, 0, r0, nr, k);
         if (rho2 > 0) wload(cb, RA, 0, sb.C, RA, 0, r0, nr, rho2);
         __syncthreads();
         // Q1 columns (range part A F1, then completion) and X~ range part C RI
@@ -681,12 +686,12 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
             double q1;
             if (j < rho1) {
                 q1 = 0.0;
-                for (int l = 0; l < k; ++l) q1 = fma(t[r * 3 * RA + l], F1[l * RA + j], q1);
+                for (int l = 0; l < k; ++l) q1 = fma(t[r * LT + l], F1[l * RA + j], q1);
             } else {
                 const int ci = j - rho1;   // X side only (W side has rho1 == k)
                 q1 = (s == 0 && ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
             }
-            t[r * 3 * RA + k + j] = q1;
+            t[r * LT + k + j] = q1;
             double xt = 0.0;
             if (j < rho2) {
                 for (int l = 0; l <= j; ++l) xt = fma(cb[r * RA + l], Ri[l * RA + j], xt);
@@ -694,15 +699,15 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
                 const int ci = si.cand0 + (j - rho2);
                 xt = (ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
             }
-            t[r * 3 * RA + 2 * k + j] = xt;
+            t[r * LT + 2 * k + j] = xt;
         }
         __syncthreads();
         if (s == 1 && si.need2 > 0) {
             // completion vectors v_a[m] = (delta_{m,c_a} - P[m,:] w_a) / nrm_a, P = [Q1 | Q2 | v_1..]
             for (int r = threadIdx.x; r < nr; r += NT) {
                 const int m = r0 + r;
-                double* q1r = t + r * 3 * RA + k;       // Q1 row (k)
-                double* q2r = t + r * 3 * RA + 2 * k;   // [Q2 (rho2) | v_1 ..]
+                double* q1r = t + r * LT + k;           // Q1 row (k)
+                double* q2r = t + r * LT + 2 * k;       // [Q2 (rho2) | v_1 ..]
                 for (int a = 0; a < si.need2; ++a) {
                     const double* w = wc + a * WCS;
                     double v = (m == sm->wcand[a]) ? 1.0 : 0.0;
@@ -713,8 +718,9 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
             }
             __syncthreads();
         }
-        if (with_q1) wstore(sb.A, KA, 0, t, 3 * RA, k, r0, nr, k);
-        wstore(sb.A, KA, k, t, 3 * RA, 2 * k, r0, nr, k);
+        if (with_q1) wstore(sb.A, KA, 0, t, LT, k, r0, nr, k);
+        wstore(sb.A, KA, k, t, LT, 2 * k, r0, nr, k);
+        if (acc) gram_blocks(acc, t, LT, nr, &blk, 1);
         __syncthreads();
     }
 }
@@ -722,7 +728,7 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
 // Whole augmentation of both sides after the [A B] Grams were reduced at
 // offsets 0 (X) and 3k^2 (W). Leaves the new directions in columns [k, 2k)
 // (and Q1 in [0, k) with with_q1), without a closing barrier.
-static __device__ __noinline__ bool augment(WCtx& x, bool with_q1) {
+static __device__ __noinline__ bool augment(WCtx& x, bool with_q1, bool par_blocks) {
     const int k = x.r;
     if (2 * k > KA) {
         if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
@@ -746,8 +752,15 @@ static __device__ __noinline__ bool augment(WCtx& x, bool with_q1) {
         // the completion read W[c, :k] of other CTAs' rows; Q1 overwrites those columns
         if (with_q1 && !wsync(x)) return false;
     }
-    materialize_side(x, 0, with_q1);
-    materialize_side(x, 1, with_q1);
+    double* acc = par_blocks ? x.sm->work : nullptr;
+    if (acc) w_acc_zero(acc, 2 * k * k);
+    materialize_side(x, 0, with_q1, acc);
+    materialize_side(x, 1, with_q1, acc);
+    if (par_blocks) {
+        // red [X~^T K (k^2) | L^T W~ (k^2)]
+        wpublish_chunk(x, acc, 0, 2 * k * k);
+        return wreduce(x, 2 * k * k);
+    }
     return true;
 }
 
@@ -1063,37 +1076,6 @@ __device__ inline void w_zero_bnd(WCtx& x) {
     __syncthreads();
 }
 
-// Grams over the new directions for the parallel integrator's augmented S:
-// red [X~^T K (k^2) | L^T W~ (k^2)]
-static __device__ __noinline__ bool w_parallel_blocks(WCtx& x) {
-    ProfScope ps_(x.prof, PF_ROWS_SCATTER);
-    const int k = x.r;
-    double* acc = x.sm->work;
-    double* t = x.sm->work + 2 * RA * RA;   // tr x 2RA, after the 2k^2 accumulator
-    const int tr = rows_fit(WORKD - 2 * RA * RA, 2 * RA);
-    w_acc_zero(acc, 2 * k * k);
-    const GBlock bx{0, k, k, k, 0};        // X~^T K
-    const GBlock bw{k, k, 0, k, k * k};    // L^T W~
-    for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
-        const int nr = min(tr, x.c1 - r0);
-        wload(t, 2 * RA, 0, x.st.X, KA, k, r0, nr, k);
-        wload(t, 2 * RA, k, x.st.K, RA, 0, r0, nr, k);
-        __syncthreads();
-        gram_blocks(acc, t, 2 * RA, nr, &bx, 1);
-        __syncthreads();
-    }
-    for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
-        const int nr = min(tr, x.m1 - r0);
-        wload(t, 2 * RA, 0, x.st.W, KA, k, r0, nr, k);
-        wload(t, 2 * RA, k, x.st.L, RA, 0, r0, nr, k);
-        __syncthreads();
-        gram_blocks(acc, t, 2 * RA, nr, &bw, 1);
-        __syncthreads();
-    }
-    wpublish_chunk(x, acc, 0, 2 * k * k);
-    return wreduce(x, 2 * k * k);
-}
-
 // Build the parallel integrator's augmented S (:1881-1885) in transposed
 // storage at work[0]: S_new = [[Sbar, L^T W~], [X~^T K, 0]].
 static __device__ __noinline__ void w_parallel_snew(WCtx& x) {
@@ -1174,8 +1156,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
             w_stream_small(x, METHOD == TITUS_PARALLEL_ADAPTIVE);
             if (!w_phase_C(x)) { aborted = true; break; }
             if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
-                if (!augment(x, false)) { aborted = true; break; }
-                if (!w_parallel_blocks(x)) { aborted = true; break; }
+                if (!augment(x, false, true)) { aborted = true; break; }
                 w_parallel_snew(x);
                 const int kk = w_truncate_svd(x, 2 * k);
                 w_truncate_apply(x, 2 * k, kk, -1, nullptr);
@@ -1186,7 +1167,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 }
             } else {
                 // BUG streaming: X1 = [Q1 X~], W1 = [Q1_W W~]; S = Mu S Nu^T
-                if (!augment(x, true)) { aborted = true; break; }
+                if (!augment(x, true, false)) { aborted = true; break; }
                 if (!wsync(x)) { aborted = true; break; }
                 const int m = 2 * k;
                 // S2 = blockdiag(M1 S N1^T, 0) in shared S (ld KA)
@@ -1288,8 +1269,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
             const int k = x.r;
             if (!w_inscatter_KL(x, sig, METHOD == TITUS_PARALLEL_ADAPTIVE, n - 1)) { aborted = true; break; }
             if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
-                if (!augment(x, false)) { aborted = true; break; }
-                if (!w_parallel_blocks(x)) { aborted = true; break; }
+                if (!augment(x, false, true)) { aborted = true; break; }
                 w_parallel_snew(x);
                 const int kk = w_truncate_svd(x, 2 * k);
                 w_truncate_apply(x, 2 * k, kk, -1, nullptr);
@@ -1307,7 +1287,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 t += dE;
             } else {
                 const int m = 2 * k;
-                if (!augment(x, true)) { aborted = true; break; }
+                if (!augment(x, true, false)) { aborted = true; break; }
                 // Grams X1^T psi (m x q) and MRed^T D W1 (q x m) over the new bases
                 double* acc = sm->work;
                 const int ldt = KA + QW;

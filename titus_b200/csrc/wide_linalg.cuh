@@ -130,12 +130,14 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                     const double app = A[p * ld + p], aqq = A[q * ld + q];
                     // a rotation whose angle is below eps changes nothing (|a_pq| <= eps max|a|):
                     // skipping it keeps the sweep count finite on rounding-level entries
-                    if (fabs(apq) > afloor && fabs(apq) > rel_tol * sqrt(fabs(app * aqq)) &&
+                    if (fabs(apq) > afloor && apq * apq > rel_tol * rel_tol * fabs(app * aqq) &&
                         fabs(apq) > 4.4e-16 * fmax(fabs(app), fabs(aqq))) {
-                        const double th = (aqq - app) / (2.0 * apq);
-                        const double tt = fabs(th) > 1e150 ? 0.5 / th
-                                                           : copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0));
-                        c = rsqrt(tt * tt + 1.0);
+                        // t = tan of the rotation angle, the smaller root of
+                        // t^2 + 2 th t - 1 = 0 with th = (aqq - app) / (2 apq), in the
+                        // form t = 2 apq sgn(d) / (|d| + sqrt(d^2 + 4 apq^2)), d = aqq - app
+                        const double d = aqq - app;
+                        const double tt = 2.0 * apq * copysign(1.0, d) / (fabs(d) + sqrt(fma(d, d, 4.0 * apq * apq)));
+                        c = rsqrt(fma(tt, tt, 1.0));
                         s = tt * c;
                         s_rot[par] = 1;
                     }
@@ -261,11 +263,13 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
                         g += __shfl_xor_sync(0xffffffffu, g, o);
                     }
                     // skip rotations with an angle below eps (no effect on the columns)
-                    if (valid && g != 0.0 && fmin(a, bq) > nfloor && fabs(g) > ctol * sqrt(a * bq) &&
+                    if (valid && g != 0.0 && fmin(a, bq) > nfloor && g * g > ctol * ctol * a * bq &&
                         fabs(g) > 2.2e-16 * fmax(a, bq)) {
-                        const double z = (bq - a) / (2.0 * g);
-                        const double tt = fabs(z) > 1e150 ? 0.5 / z : copysign(1.0, z) / (fabs(z) + sqrt(1.0 + z * z));
-                        const double c = rsqrt(1.0 + tt * tt), sn = c * tt;
+                        // t = tan of the angle orthogonalising the two columns:
+                        // t = 2 g sgn(d) / (|d| + sqrt(d^2 + 4 g^2)), d = |y|^2 - |x|^2
+                        const double d = bq - a;
+                        const double tt = 2.0 * g * copysign(1.0, d) / (fabs(d) + sqrt(fma(d, d, 4.0 * g * g)));
+                        const double c = rsqrt(fma(tt, tt, 1.0)), sn = c * tt;
                         for (int i = gl; i < m; i += LP) {
                             const double u = At[p * ld + i], v = At[q * ld + i];
                             At[p * ld + i] = c * u - sn * v;
