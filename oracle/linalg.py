@@ -47,7 +47,8 @@ def svd_jacobi(A: np.ndarray):
     return u[:, :m], sva[:m] * scale, v[:, :m]
 
 
-def svd_det(A: np.ndarray, tol: float | None = None):
+def svd_det(A: np.ndarray, tol: float | None = None, basis_u: np.ndarray | None = None,
+            basis_v: np.ndarray | None = None):
     """Thin SVD (U, s, V) with the deterministic null-space rule.
 
     Computed by the one-sided Jacobi SVD (``svd_jacobi``) for relative accuracy.
@@ -63,9 +64,52 @@ def svd_det(A: np.ndarray, tol: float | None = None):
     m = s.size
     rho = int(np.sum(s > tol * s[0])) if m and s[0] > 0 else 0
     if rho < m:
-        U = np.column_stack([U[:, :rho], _complete(U[:, :rho], m - rho, U.shape[0])])
-        V = np.column_stack([V[:, :rho], _complete(V[:, :rho], m - rho, V.shape[0])])
+        if basis_u is not None:
+            U = np.column_stack([U[:, :rho], _complete_rows(U[:, :rho], m - rho, basis_u)])
+            V = np.column_stack([V[:, :rho], _complete_rows(V[:, :rho], m - rho, basis_v)])
+        else:
+            U = np.column_stack([U[:, :rho], _complete(U[:, :rho], m - rho, U.shape[0])])
+            V = np.column_stack([V[:, :rho], _complete(V[:, :rho], m - rho, V.shape[0])])
     return U, s, V
+
+
+def _complete_rows(Keep: np.ndarray, need: int, basis: np.ndarray, min_norm: float = 1e-6) -> np.ndarray:
+    """Gauge-free completion for the SVD of a small matrix S expressed in the
+    columns of ``basis`` (n x m): candidate c is u_c = basis[c, :] (the cell
+    indicator e_c projected into span(basis), in basis coordinates), c in index
+    order; it is Gram-Schmidt'ed twice against Keep and the vectors accepted so
+    far and accepted when ||u_c|| > min_norm and the residual keeps at least half
+    of ||u_c||. Rotating the basis rotates the result with it, so basis @ result
+    does not depend on the basis chosen for the span. Falls back to canonical
+    vectors of R^m if the rows run out."""
+    m = Keep.shape[0]
+    cols = []
+    c = 0
+    cands = list(range(basis.shape[0]))
+    while len(cols) < need:
+        if c < len(cands):
+            u = np.array(basis[cands[c], :], dtype=np.float64)
+            nu = np.linalg.norm(u)
+            c += 1
+            if not nu > min_norm:
+                continue
+        else:
+            i = c - len(cands)
+            if i >= m:
+                raise RuntimeError("basis completion ran out of candidates")
+            u = np.zeros(m)
+            u[i] = 1.0
+            nu = 1.0
+            c += 1
+        Bc = np.column_stack([Keep] + cols) if (Keep.shape[1] + len(cols)) else np.zeros((m, 0))
+        v = u.copy()
+        for _ in range(2):
+            if Bc.shape[1]:
+                v = v - Bc @ (Bc.T @ v)
+        nv = np.linalg.norm(v)
+        if nv > 0.5 * nu:
+            cols.append(v / nv)
+    return np.column_stack(cols) if cols else np.zeros((m, 0))
 
 
 def _complete(B: np.ndarray, need: int, n: int, order=None) -> np.ndarray:

@@ -187,7 +187,9 @@ class SolverCSD:
     def truncate(self, X, S, W):
         """``truncate!`` (``SolverCSD.jl:3369-3399``): l1 tail test, clamp [2, r]."""
         s = self.settings
-        U, D, V = la.svd_det(S) if self.basis_mode == "det" else la.svd_full(S)
+        # det mode: null directions completed from the rows of X and W (cells,
+        # moments in index order), which does not depend on the bases chosen
+        U, D, V = la.svd_det(S, basis_u=X, basis_v=W) if self.basis_mode == "det" else la.svd_full(S)
         rMaxTotal = s.r
         rMinTotal = 2
         tol = s.theta * np.linalg.norm(D) ** s.thetaIndex

@@ -65,6 +65,38 @@ def test_svd_det_completion():
     np.testing.assert_allclose(s0, 0.0)
 
 
+def test_svd_det_row_completion_is_gauge_free():
+    """truncate!'s null directions completed from the rows of X and W: rotating
+    the bases (X -> X Q, S -> Q^T S R, W -> W R) leaves X U and W V unchanged."""
+    rng = np.random.default_rng(3)
+    n, N, m = 40, 12, 5
+    X = np.linalg.qr(rng.standard_normal((n, m)))[0]
+    W = np.linalg.qr(rng.standard_normal((N, m)))[0]
+    S = np.zeros((m, m))
+    S[:2, :2] = rng.standard_normal((2, 2))       # rank 2: three null directions
+    U, s, V = la.svd_det(S, basis_u=X, basis_v=W)
+    assert np.allclose(U.T @ U, np.eye(m), atol=1e-14) and np.allclose(V.T @ V, np.eye(m), atol=1e-14)
+    Q = np.linalg.qr(rng.standard_normal((m, m)))[0]
+    R = np.linalg.qr(rng.standard_normal((m, m)))[0]
+    U2, s2, V2 = la.svd_det(Q.T @ S @ R, basis_u=X @ Q, basis_v=W @ R)
+    np.testing.assert_allclose(s2, s, rtol=1e-13, atol=1e-15)
+    # range directions up to sign, null directions exactly
+    for j in range(m):
+        a, b = X @ U[:, j], X @ Q @ U2[:, j]
+        sg = 1.0 if j >= 2 else np.sign(a @ b)
+        np.testing.assert_allclose(sg * b, a, atol=1e-12)
+        a, b = W @ V[:, j], W @ R @ V2[:, j]
+        sg = 1.0 if j >= 2 else np.sign(a @ b)
+        np.testing.assert_allclose(sg * b, a, atol=1e-12)
+    # rows that vanish in the basis are skipped: first accepted candidate is row 2
+    Xz = X.copy()
+    Xz[:2] = 0.0
+    Xz = np.linalg.qr(Xz)[0]
+    Uz, _, _ = la.svd_det(S, basis_u=Xz, basis_v=W)
+    r2 = Xz[2] - Uz[:, :2] @ (Uz[:, :2].T @ Xz[2])
+    np.testing.assert_allclose(Uz[:, 2], r2 / np.linalg.norm(r2), atol=1e-12)
+
+
 def test_svd_jacobi_relative_accuracy():
     rng = np.random.default_rng(1)
     d = np.array([1.0, 1e-4, 1e-8, 1e-11])

@@ -341,29 +341,74 @@ static __device__ __noinline__ void aug_prepare(WCtx& x, int s, int goff) {
         g_copy(M1, RA, R, RA, k, k);
     } else {
         si.fast1 = 0;
-        // G11 is still intact (w_chol copies); Jacobi destroys it
-        prof_count(x.prof, PF_EIG_SWEEPS, (unsigned long long)w_eig(G11, T, RA, lam, k, x.st.status, raw_gram_floor(k)));
+        // G11 is still intact (w_chol copies). This Jacobi only separates the
+        // scales (V0) for the graded Gram of A V0 that aug_q1_graded reduces;
+        // G12 waits in SS_R0 for T1.
+        prof_count(x.prof, PF_EIG_SWEEPS, (unsigned long long)w_eig(G11, T, RA, lam, k, x.st.status, raw_gram_floor(k), 1e-8));
         prof_count(x.prof, PF_EIG_CALLS, 1ull);
-        int rho = 0;
-        for (int j = 0; j < k; ++j) {
-            if (sqrt(fmax(lam[j], 0.0)) > tol * si.scale) rho = j + 1;
-            else break;
-        }
-        si.rho1 = rho;
-        for (int e = threadIdx.x; e < k * k; e += NT) {
-            const int i = e / k, j = e - (e / k) * k;
-            const double sq = j < rho ? sqrt(lam[j]) : 0.0;
-            F1[i * RA + j] = j < rho ? T[i * RA + j] / sq : 0.0;
-            M1[i * RA + j] = i < rho ? sqrt(lam[i]) * T[j * RA + i] : 0.0;   // Lambda^{1/2} V^T
-        }
-        __syncthreads();
-        if (s == 1 && rho < k && threadIdx.x == 0) set_status(x.st.status, ST_UNSUPPORTED);
+        g_copy(sside(x, s, SS_V0), RA, T, RA, k, k);
+        g_copy(sside(x, s, SS_R0), RA, G12, RA, k, k);
+        return;
     }
     __syncthreads();
     // P1 = F1 F1^T (only the first rho1 columns of F1 are nonzero)
     g_mm(P1, RA, F1, RA, false, F1, RA, true, k, si.rho1, k);
     // T1 = P1 G12
     g_mm(sside(x, s, SS_T), RA, P1, RA, false, G12, RA, false, k, k, k);
+}
+
+static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, double* acc, int off);
+
+// Rank-revealing Q1 after aug_prepare left V0 (Jacobi of A^T A) on a side:
+// the Gram of A V0 is reduced from the rows, so its Jacobi (V2, lambda) resolves
+// singular values of A far below sqrt(eps) ||A|| against the cut tol * scale,
+// as the SVD of A does; a Gram of A alone carries rounding of eps ||A||^2 there.
+// Q1 = A V diag(lambda^-1/2) on the rho1 values above the cut, V = V0 V2;
+// M1 = Q1^T A = diag(lambda^1/2) V^T; P1 = F1 F1^T; T1 = P1 G12.
+static __device__ __noinline__ bool aug_q1_graded(WCtx& x) {
+    const int k = x.r;
+    const bool slow[2] = {x.side[0].fast1 == 0, x.side[1].fast1 == 0};
+    if (!slow[0] && !slow[1]) return true;
+    double* acc = x.sm->work;
+    w_acc_zero(acc, 2 * k * k);
+    for (int s = 0; s < 2; ++s)
+        if (slow[s]) rf_pass(x, s, 3, k, acc, s * k * k);
+    wpublish_chunk(x, acc, 0, 2 * k * k);
+    if (!wreduce(x, 2 * k * k)) return false;
+    ProfScope ps_(x.prof, PF_SMALL);
+    for (int s = 0; s < 2; ++s) {
+        if (!slow[s]) continue;
+        SideInfo& si = x.side[s];
+        double* G = x.sm->work;
+        double* V2 = G + RA * RA;
+        double* V0 = V2 + RA * RA;
+        double* lam = x.sm->vec;
+        load_red(x, s * k * k, k, k, G, RA);
+        prof_count(x.prof, PF_EIG_SWEEPS, (unsigned long long)w_eig(G, V2, RA, lam, k, x.st.status, kGradedFloor));
+        prof_count(x.prof, PF_EIG_CALLS, 1ull);
+        g_copy(V0, RA, sside(x, s, SS_V0), RA, k, k);
+        const double cut = x.P.rank_tol * si.scale;
+        int rho = 0;
+        for (int j = 0; j < k; ++j) {
+            if (sqrt(fmax(lam[j], 0.0)) > cut) rho = j + 1;
+            else break;
+        }
+        si.rho1 = rho;
+        g_mm(G, RA, V0, RA, false, V2, RA, false, k, k, k);   // V (G is free after the Jacobi)
+        double* F1 = sside(x, s, SS_F1);
+        double* M1 = sside(x, s, SS_M1);
+        for (int e = threadIdx.x; e < k * k; e += NT) {
+            const int i = e / k, j = e - (e / k) * k;
+            F1[i * RA + j] = j < rho ? G[i * RA + j] / sqrt(lam[j]) : 0.0;
+            M1[i * RA + j] = i < rho ? sqrt(lam[i]) * G[j * RA + i] : 0.0;
+        }
+        __syncthreads();
+        if (s == 1 && rho < k && threadIdx.x == 0) set_status(x.st.status, ST_UNSUPPORTED);
+        double* P1 = sside(x, s, SS_P1);
+        g_mm(P1, RA, F1, RA, false, F1, RA, true, k, rho, k);
+        g_mm(sside(x, s, SS_T), RA, P1, RA, false, sside(x, s, SS_R0), RA, false, k, k, k);
+    }
+    return true;
 }
 
 // BP = B - A T (T = SS_T) for own rows; acc[off..] += A^T BP (second=false) or BP^T BP (second=true)
@@ -431,8 +476,8 @@ __device__ __forceinline__ void w_rsolve(double* t, int ldt, const double* R, in
 }
 
 // C = BP M (mode 0: M = R0 by row solves; mode 1: M = T (k x rho), product) for
-// own rows; acc[off..] += C^T C (rho x rho), or (mode 2) (BP V)^T (BP V) without
-// storing C.
+// own rows; acc[off..] += C^T C (rho x rho), or (mode 2) (BP V0)^T (BP V0) and
+// (mode 3) (A V0)^T (A V0) without storing C.
 static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, double* acc, int off) {
     ProfScope ps_(x.prof, PF_RF_PASSES);
     const int k = x.r;
@@ -445,7 +490,8 @@ static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, d
     const GBlock bl{k, w, k, w, off};
     for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
         const int nr = min(tr, sb.r1 - r0);
-        wload(F, 2 * RA, 0, sb.BP, RA, 0, r0, nr, k);
+        if (mode == 3) wload(F, 2 * RA, 0, sb.A, KA, 0, r0, nr, k);
+        else wload(F, 2 * RA, 0, sb.BP, RA, 0, r0, nr, k);
         __syncthreads();
         if (mode == 0) {
             for (int e = threadIdx.x; e < nr * k; e += NT) F[(e / k) * 2 * RA + k + e % k] = F[(e / k) * 2 * RA + e % k];
@@ -460,7 +506,7 @@ static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, d
             }
         }
         __syncthreads();
-        if (mode != 2) wstore(sb.C, RA, 0, F, 2 * RA, k, r0, nr, w);
+        if (mode < 2) wstore(sb.C, RA, 0, F, 2 * RA, k, r0, nr, w);
         gram_blocks(acc, F, 2 * RA, nr, &bl, 1);
         __syncthreads();
     }
@@ -736,6 +782,7 @@ static __device__ __noinline__ bool augment(WCtx& x, bool with_q1, bool par_bloc
     }
     aug_prepare(x, 0, 0);
     aug_prepare(x, 1, 3 * k * k);
+    if (!aug_q1_graded(x)) return false;
     if (!aug_project(x)) return false;
     const bool all[2] = {true, true};
     const bool aug[2] = {false, false};
@@ -768,7 +815,8 @@ static __device__ __noinline__ bool augment(WCtx& x, bool with_q1, bool par_bloc
 // truncate! of the m x m matrix given in transposed storage in work[0..):
 // SVD, l1 tail rank (clamped to [2, settings.r]), deterministic completion of
 // the kept null directions. Leaves U^T (rows perm[j]) at work[0], V^T at
-// work[KA*KA], sig/perm in shared memory; returns the kept rank.
+// work[KA*LDS], sig/perm in shared memory; returns the kept rank (-1 if the
+// team aborted).
 static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
     ProfScope ps_(x.prof, PF_JACOBI);
     WSmem* sm = x.sm;
@@ -803,7 +851,11 @@ static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
     kk = min(kk, x.P.r);
     kk = max(kk, 2);
     kk = min(kk, m);
-    w_svd_complete(At, Vt, LDS, m, sm->sig, sm->perm, kk, kNullSvd, x.st.status);
+    const int rho = w_svd_complete(At, Vt, LDS, m, sm->sig, sm->perm, kk, kNullSvd, x.st.status, x.st.X, x.P.n,
+                                   x.st.W, x.P.N, KA);
+    // the completion read rows of X and W owned by other CTAs, which the
+    // truncation then rewrites in place
+    if (rho < kk && !wsync(x)) return -1;
     return kk;
 }
 
@@ -1159,6 +1211,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 if (!augment(x, false, true)) { aborted = true; break; }
                 w_parallel_snew(x);
                 const int kk = w_truncate_svd(x, 2 * k);
+                if (kk < 0) { aborted = true; break; }
                 w_truncate_apply(x, 2 * k, kk, -1, nullptr);
                 if (kk > RA) {
                     if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
@@ -1229,6 +1282,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 }
                 __syncthreads();
                 const int kk = w_truncate_svd(x, m);
+                if (kk < 0) { aborted = true; break; }
                 bool repeat = false;
                 if (kk == 2 * k && 2 * k < P.r) {
                     repeat = true;   // accept the truncation, redo this energy (n = n-1 without continue)
@@ -1272,6 +1326,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 if (!augment(x, false, true)) { aborted = true; break; }
                 w_parallel_snew(x);
                 const int kk = w_truncate_svd(x, 2 * k);
+                if (kk < 0) { aborted = true; break; }
                 w_truncate_apply(x, 2 * k, kk, -1, nullptr);
                 if (kk > RA) {
                     if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
@@ -1356,6 +1411,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                     eta2 += a * a;
                 }
                 const int kk = w_truncate_svd(x, m);
+                if (kk < 0) { aborted = true; break; }
                 bool repeat = false;
                 if (kk == 2 * k && 2 * k < P.r) {
                     repeat = true;

@@ -314,16 +314,25 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
 }
 
 // Normalise the left singular vectors of the numerical range (sigma_j >
-// tol sigma_0, j < rho) and replace the directions j in [rho, kkeep) of both
-// factors by canonical vectors in index order, completed by two Gram-Schmidt
-// passes against the columns before them (accepted when the residual exceeds
-// 1/2) -- the rule of oracle.linalg.svd_det. Returns rho.
+// tol sigma_0, j < rho) and complete the directions j in [rho, kkeep) of both
+// factors, which the matrix does not determine, by a rule that does not depend
+// on the bases the small matrix is expressed in: candidate c is the row c of
+// that basis (rowsU: the n x m spatial basis for U, rowsV: the N x m angular
+// basis for V; global, ld ldr), i.e. the cell / moment indicator vector
+// projected into the basis, taken in index order (then canonical vectors of
+// R^m); rows with norm <= 1e-6 are skipped; two Gram-Schmidt passes against
+// the columns before it; accepted when the residual keeps at least half the
+// candidate's norm. Same rule as oracle.linalg._complete_rows. Returns rho.
 static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld, int m, const double* sig,
-                                                  const int* perm, int kkeep, double tol, int* status) {
+                                                  const int* perm, int kkeep, double tol, int* status,
+                                                  const double* rowsU, int nU, const double* rowsV, int nV,
+                                                  int ldr) {
     __shared__ double s_v[KA];
     __shared__ double s_d[KA];
-    __shared__ double s_nv;
+    __shared__ double s_nv, s_nu;
+    __shared__ double s_n8[NT / 32];
     __shared__ int s_acc;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int rho = 0;
     if (m > 0 && sig[0] > 0.0)
         for (int j = 0; j < m; ++j) {
@@ -337,25 +346,68 @@ static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld
     __syncthreads();
     for (int side = 0; side < 2; ++side) {
         double* B = side == 0 ? At : Vt;
-        int cand = 0;
+        const double* rows = side == 0 ? rowsU : rowsV;
+        const int nrows = side == 0 ? nU : nV;
+        int cand = 0;   // [0, nrows): basis rows; [nrows, nrows + m): canonical vectors
         for (int j = rho; j < kkeep; ++j) {
             bool done = false;
             while (!done) {
-                if (cand >= m) {
+                if (cand >= nrows + m) {
                     if (threadIdx.x == 0) set_status(status, ST_COMPLETION);
                     __syncthreads();
                     return rho;
                 }
-                for (int i = threadIdx.x; i < m; i += NT) s_v[i] = (i == cand) ? 1.0 : 0.0;
+                int found = -1;
+                if (cand < nrows) {
+                    // next row with norm > 1e-6, eight candidates at a time (one per warp)
+                    while (cand < nrows && found < 0) {
+                        const int c = cand + warp;
+                        double sq = 0.0;
+                        if (c < nrows)
+                            for (int i = lane; i < m; i += 32) {
+                                const double v = ldcg(rows + (size_t)c * ldr + i);
+                                sq = fma(v, v, sq);
+                            }
+                        sq = warp_sum(sq);
+                        if (lane == 0) s_n8[warp] = (c < nrows) ? sq : -1.0;
+                        __syncthreads();
+                        int f = -1;
+                        for (int w = 0; w < NT / 32; ++w)
+                            if (s_n8[w] > 1e-12) {
+                                f = w;
+                                break;
+                            }
+                        __syncthreads();
+                        if (f >= 0) {
+                            found = cand + f;
+                            cand = found + 1;
+                        } else {
+                            cand += NT / 32;
+                        }
+                    }
+                    if (found < 0) continue;   // rows exhausted: canonical vectors next
+                    for (int i = threadIdx.x; i < m; i += NT) s_v[i] = ldcg(rows + (size_t)found * ldr + i);
+                } else {
+                    const int i0 = cand - nrows;
+                    for (int i = threadIdx.x; i < m; i += NT) s_v[i] = (i == i0) ? 1.0 : 0.0;
+                    ++cand;
+                }
+                __syncthreads();
+                if (threadIdx.x < 32) {
+                    double sq = 0.0;
+                    for (int i = threadIdx.x; i < m; i += 32) sq = fma(s_v[i], s_v[i], sq);
+                    sq = warp_sum(sq);
+                    if (threadIdx.x == 0) s_nu = sqrt(sq);
+                }
                 __syncthreads();
                 for (int pass = 0; pass < 2; ++pass) {
                     // d_a = B_a . v for a < j, then v -= sum_a d_a B_a
-                    for (int a = threadIdx.x >> 5; a < j; a += NT / 32) {
+                    for (int a = warp; a < j; a += NT / 32) {
                         const double* ba = B + perm[a] * ld;
-                        double s = 0.0;
-                        for (int i = threadIdx.x & 31; i < m; i += 32) s = fma(ba[i], s_v[i], s);
-                        s = warp_sum(s);
-                        if ((threadIdx.x & 31) == 0) s_d[a] = s;
+                        double sdot = 0.0;
+                        for (int i = lane; i < m; i += 32) sdot = fma(ba[i], s_v[i], sdot);
+                        sdot = warp_sum(sdot);
+                        if (lane == 0) s_d[a] = sdot;
                     }
                     __syncthreads();
                     for (int i = threadIdx.x; i < m; i += NT) {
@@ -366,16 +418,15 @@ static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld
                     __syncthreads();
                 }
                 if (threadIdx.x < 32) {
-                    double s = 0.0;
-                    for (int i = threadIdx.x; i < m; i += 32) s = fma(s_v[i], s_v[i], s);
-                    s = warp_sum(s);
+                    double sq = 0.0;
+                    for (int i = threadIdx.x; i < m; i += 32) sq = fma(s_v[i], s_v[i], sq);
+                    sq = warp_sum(sq);
                     if (threadIdx.x == 0) {
-                        s_acc = (sqrt(s) > 0.5) ? 1 : 0;
-                        s_nv = sqrt(s);
+                        s_nv = sqrt(sq);
+                        s_acc = (s_nv > 0.5 * s_nu) ? 1 : 0;
                     }
                 }
                 __syncthreads();
-                ++cand;
                 if (s_acc) {
                     const double nv = s_nv;
                     for (int i = threadIdx.x; i < m; i += NT) B[perm[j] * ld + i] = s_v[i] / nv;
