@@ -21,7 +21,7 @@ constexpr int KA = 2 * RA;      // max augmented width
 constexpr int LDS = KA + 1;     // row stride of the truncation SVD's column arrays (odd: no bank conflicts)
 constexpr int QW = titus::QM;   // psi leading dimension (reduced ordinates <= QW)
 constexpr int TRW = 8;          // rows per staged tile (minimum layout)
-constexpr int TRMAX = 128;      // rows per staged tile when the phase's free shared memory allows
+constexpr int TRMAX = 512;      // rows per staged tile when the phase's free shared memory allows
 constexpr int PMAXW = 8 * KA * KA;   // largest reduction (BUG S-step Grams): 51200 doubles
 constexpr int WORKD = 20480;    // shared work area (doubles)
 constexpr int ACCW = 16384;     // accumulator chunk (doubles), inside the work area
@@ -256,16 +256,45 @@ __device__ __forceinline__ void wstore(double* A, int lda, int c0, const double*
 struct GBlock {
     int ca, wa, cb, wb, off;
 };
-// Accumulate a list of blocks over a tile of nr rows; 2x2 register blocking.
+// Accumulate a list of blocks over a tile of nr rows; 2x2 register tiles. The
+// tiles of all blocks are flattened; each warp holds 32/G tiles in G row
+// subgroups (subgroup s sums rows s, s+G, ...; lanes of a subgroup share rows,
+// so their loads broadcast), G in {1, 2, 4, 8} minimising rounds x rows per
+// lane. The G partial sums of a tile meet in a fixed xor butterfly: the result
+// depends only on (blocks, nr), not on timing.
 __device__ inline void gram_blocks(double* acc, const double* F, int ldf, int nr, const GBlock* bl, int nb) {
-    for (int q = 0; q < nb; ++q) {
-        const GBlock g = bl[q];
-        const int hi = (g.wa + 1) >> 1, hj = (g.wb + 1) >> 1;
-        for (int e = threadIdx.x; e < hi * hj; e += NT) {
-            const int i = 2 * (e / hj), j = 2 * (e - (e / hj) * hj);
-            const bool i1 = i + 1 < g.wa, j1 = j + 1 < g.wb;
-            double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
-            for (int r = 0; r < nr; ++r) {
+    int T = 0;
+    for (int q = 0; q < nb; ++q) T += ((bl[q].wa + 1) >> 1) * ((bl[q].wb + 1) >> 1);
+    int G = 1, best = 0x7fffffff;
+    for (int g = 1; g <= 8; g <<= 1) {
+        const int slots = (NT / 32) * (32 / g);
+        const int cost = ((T + slots - 1) / slots) * ((nr + g - 1) / g);
+        if (cost < best) {
+            best = cost;
+            G = g;
+        }
+    }
+    const int L = 32 / G, slots = (NT / 32) * L;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sg = lane / L, tl = lane - (lane / L) * L;
+    for (int base = 0; base < T; base += slots) {
+        int off = base + warp * L + tl;
+        const bool valid = off < T;
+        GBlock g{0, 2, 0, 2, 0};
+        int hj = 1;
+        if (valid)
+            for (int q = 0; q < nb; ++q) {
+                g = bl[q];
+                hj = (g.wb + 1) >> 1;
+                const int cnt = ((g.wa + 1) >> 1) * hj;
+                if (off < cnt) break;
+                off -= cnt;
+            }
+        const int i = 2 * (off / hj), j = 2 * (off - (off / hj) * hj);
+        const bool i1 = i + 1 < g.wa, j1 = j + 1 < g.wb;
+        double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+        if (valid)
+            for (int r = sg; r < nr; r += G) {
                 const double* row = F + r * ldf;
                 const double a0 = row[g.ca + i], a1 = i1 ? row[g.ca + i + 1] : 0.0;
                 const double b0 = row[g.cb + j], b1 = j1 ? row[g.cb + j + 1] : 0.0;
@@ -274,6 +303,13 @@ __device__ inline void gram_blocks(double* acc, const double* F, int ldf, int nr
                 s10 = fma(a1, b0, s10);
                 s11 = fma(a1, b1, s11);
             }
+        for (int o = L; o < 32; o <<= 1) {
+            s00 += __shfl_xor_sync(0xffffffffu, s00, o);
+            s01 += __shfl_xor_sync(0xffffffffu, s01, o);
+            s10 += __shfl_xor_sync(0xffffffffu, s10, o);
+            s11 += __shfl_xor_sync(0xffffffffu, s11, o);
+        }
+        if (valid && sg == 0) {
             double* o = acc + g.off + i * g.wb + j;
             o[0] += s00;
             if (j1) o[1] += s01;

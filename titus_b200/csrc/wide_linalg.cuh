@@ -93,7 +93,7 @@ static __device__ __noinline__ double w_chol(const double* G, int ldg, double* R
 // separated directions use a negligible floor.
 static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* lam, int k, int* status,
                                          double rel_floor, double rel_tol = 1e-15) {
-    __shared__ double rc[RA / 2 + 1], rs[RA / 2 + 1];
+    __shared__ double rc[RA / 2 + 1], rs[RA / 2 + 1], rdp[RA / 2 + 1], rdq[RA / 2 + 1];
     __shared__ int rp[RA / 2 + 1], rq[RA / 2 + 1];
     __shared__ int s_rot[2];
     __shared__ double s_lam[RA];
@@ -139,6 +139,11 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                         const double tt = 2.0 * apq * copysign(1.0, d) / (fabs(d) + sqrt(fma(d, d, 4.0 * apq * apq)));
                         c = rsqrt(fma(tt, tt, 1.0));
                         s = tt * c;
+                        // the rotated 2x2 block in closed form (a_pq -> 0 exactly):
+                        // two-sided updates leave a_pq at a few eps max|a_pp|, |a_qq|,
+                        // which the next sweep would rotate again without end
+                        rdp[threadIdx.x] = fma(-tt, apq, app);
+                        rdq[threadIdx.x] = fma(tt, apq, aqq);
                         s_rot[par] = 1;
                     }
                 } else {
@@ -166,8 +171,16 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                 if (p < 0 || rs[pi] == 0.0) continue;
                 const double c = rc[pi], s = rs[pi];
                 const double ap = A[i * ld + p], aq = A[i * ld + q];
-                A[i * ld + p] = c * ap - s * aq;
-                A[i * ld + q] = s * ap + c * aq;
+                if (i == p) {
+                    A[i * ld + p] = rdp[pi];
+                    A[i * ld + q] = 0.0;
+                } else if (i == q) {
+                    A[i * ld + p] = 0.0;
+                    A[i * ld + q] = rdq[pi];
+                } else {
+                    A[i * ld + p] = c * ap - s * aq;
+                    A[i * ld + q] = s * ap + c * aq;
+                }
                 const double vp = V[i * ld + p], vq = V[i * ld + q];
                 V[i * ld + p] = c * vp - s * vq;
                 V[i * ld + q] = s * vp + c * vq;
