@@ -1270,9 +1270,16 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                     }
                     __syncthreads();
                 }
-                double eta2 = 0.0, sup2 = 0.0;
-                for (int e = 0; e < k * k; ++e) eta2 += E[(e / k) * RA + e % k] * E[(e / k) * RA + e % k];
-                for (int e = 0; e < m * m; ++e) sup2 += Sup[(e / m) * KA + e % m] * Sup[(e / m) * KA + e % m];
+                double e2 = 0.0, s2p = 0.0;
+                for (int e = threadIdx.x; e < k * k; e += NT) {
+                    const double v = E[(e / k) * RA + e % k];
+                    e2 = fma(v, v, e2);
+                }
+                for (int e = threadIdx.x; e < m * m; e += NT) {
+                    const double v = Sup[(e / m) * KA + e % m];
+                    s2p = fma(v, v, s2p);
+                }
+                const double eta2 = cta_sum(e2), sup2 = cta_sum(s2p);
                 // truncate Sup
                 double* At = sm->work;
                 __syncthreads();
@@ -1403,13 +1410,14 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 }
                 __syncthreads();
                 // eta = ||Xtpsi[k:, :] MtDW[:, k:]||_F
-                double eta2 = 0.0;
-                for (int e = 0; e < k * k; ++e) {
+                double e2 = 0.0;
+                for (int e = threadIdx.x; e < k * k; e += NT) {
                     const int i = k + e / k, j = k + e % k;
                     double a = 0.0;
                     for (int l = 0; l < P.q; ++l) a = fma(Xp[i * QW + l], Mt[l * KA + j], a);
-                    eta2 += a * a;
+                    e2 = fma(a, a, e2);
                 }
+                const double eta2 = cta_sum(e2);
                 const int kk = w_truncate_svd(x, m);
                 if (kk < 0) { aborted = true; break; }
                 bool repeat = false;

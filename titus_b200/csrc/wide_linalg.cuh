@@ -16,6 +16,19 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Sum over the CTA of one value per thread, in a fixed order (warp butterflies,
+// then the warps in index order); every thread receives the same result.
+static __device__ __noinline__ double cta_sum(double v) {
+    __shared__ double s_w[NT / 32];
+    v = warp_sum(v);
+    __syncthreads();   // a previous call's readers are done with s_w
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < NT / 32; ++w) t += s_w[w];
+    return t;
+}
+
 // Upper Cholesky of G (k x k, ld ldg, any memory) into R (shared, ld) and its
 // inverse Ri (shared, ld). Returns ||R||_F ||R^{-1}||_F, or +inf on a
 // non-positive pivot; *ri_f receives ||R^{-1}||_F (a bound 1/sigma_min).
