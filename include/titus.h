@@ -194,6 +194,20 @@ int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* o
                         double* X, double* S, double* W, double* psi, int32_t* rank_out, void* stream,
                         char* err, size_t err_len);
 
+/* Second-order limited upwind transport flux of the uncollided ordinates,
+ * replacing solveFlux!(obj, phi, flux) (code/SolverCSD.jl:295-386, limiter
+ * minmod/slopefit :288-293). All arrays are DEVICE arrays: phi and flux hold
+ * nx*ny*q doubles with cell (i, j), ordinate l at (i*ny + j)*q + l (i along x,
+ * j along y); omega_x and omega_z hold the q ordinates' x and y components
+ * (qReduced[:,1] and qReduced[:,3]). flux is written on the interior cells
+ * 2 <= i < nx-2, 2 <= j < ny-2 only, like the reference's loops; its other
+ * entries are left as they were. phi and flux must not overlap. The call is
+ * asynchronous on `stream` (a cudaStream_t, NULL for the default stream).
+ * Returns TITUS_OK, TITUS_ERR_ARG (sizes, NULL, dx or dy <= 0, overlap),
+ * TITUS_ERR_LIMIT (ny*q >= 2^31) or TITUS_ERR_CUDA. */
+int titus_limited_flux(int32_t nx, int32_t ny, int32_t q, double dx, double dy, const double* omega_x,
+                       const double* omega_z, const double* phi, double* flux, void* stream);
+
 /* Build / capability queries. */
 int titus_max_rank(void);        /* largest settings.r accepted (adaptive rank cap) */
 int titus_max_ordinates(void);   /* largest q supported */

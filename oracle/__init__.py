@@ -26,4 +26,4 @@ here from its published definition:
   deterministic completion rule in ``oracle.linalg``.
 """
 
-__all__ = ["pn", "quadrature", "csd", "settings", "stencils", "solver", "linalg"]
+__all__ = ["pn", "quadrature", "csd", "settings", "stencils", "solver", "linalg", "flux"]

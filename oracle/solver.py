@@ -136,6 +136,13 @@ class SolverCSD:
         flux[1:-1, 1:-1, :] = (ox / s.dx) * ew + (oz / s.dy) * ns
         return flux
 
+    def flux_limited(self, phi, flux=None):
+        """``solveFlux!`` (``SolverCSD.jl:295-386``) with this solver's
+        ``qReduced`` and spacing; see ``oracle.flux.limited_flux``."""
+        from .flux import limited_flux
+
+        return limited_flux(phi, self.qReduced[:, 0], self.qReduced[:, 2], self.settings.dx, self.settings.dy, flux)
+
     def sweep(self, psi, dE, sigma0):
         """Uncollided update ``:1000-1005`` incl. the boundary-slab quirk.
 

@@ -76,6 +76,8 @@ SIGNATURES = [
     ("titus_profile", C.c_int, [C.c_void_p, _dp, C.c_int32]),
     ("titus_solve_noalloc", C.c_int, [C.POINTER(Problem), C.POINTER(Options), _dp, _dp, _dp, _dp, _dp, _ip,
                                       C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("titus_limited_flux", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("titus_max_rank", C.c_int, []),
     ("titus_max_ordinates", C.c_int, []),
     ("titus_version", C.c_char_p, []),
