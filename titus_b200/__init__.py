@@ -3,3 +3,4 @@ from .settings import Settings  # noqa: F401
 from .solver import (SolveBatchedPencilBeams, SolverCSD, SolveFirstCollisionSourceDLR,  # noqa: F401
                      SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel, scalar_flux)
 from .spots import partition, plan_dose, plan_objective  # noqa: F401
+from .output import write_dlm, write_dose_vtk, write_vtr  # noqa: F401
