@@ -160,7 +160,7 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                         s_rot[par] = 1;
                     }
                 } else {
-                    p = q = -1;
+                    q = -1;   // p is real, its partner the padding index: p stays put this round
                 }
                 rc[threadIdx.x] = c;
                 rs[threadIdx.x] = s;
@@ -168,35 +168,46 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                 rq[threadIdx.x] = q;
             }
             __syncthreads();
-            for (int e = threadIdx.x; e < npairs * k; e += NT) {
-                const int pi = e / k, j = e - (e / k) * k;
-                const int p = rp[pi], q = rq[pi];
-                if (p < 0 || rs[pi] == 0.0) continue;
-                const double c = rc[pi], s = rs[pi];
-                const double ap = A[p * ld + j], aq = A[q * ld + j];
-                A[p * ld + j] = c * ap - s * aq;
-                A[q * ld + j] = s * ap + c * aq;
-            }
-            __syncthreads();
-            for (int e = threadIdx.x; e < npairs * k; e += NT) {
-                const int pi = e / k, i = e - (e / k) * k;
-                const int p = rp[pi], q = rq[pi];
-                if (p < 0 || rs[pi] == 0.0) continue;
-                const double c = rc[pi], s = rs[pi];
-                const double ap = A[i * ld + p], aq = A[i * ld + q];
-                if (i == p) {
-                    A[i * ld + p] = rdp[pi];
-                    A[i * ld + q] = 0.0;
-                } else if (i == q) {
-                    A[i * ld + p] = 0.0;
-                    A[i * ld + q] = rdq[pi];
-                } else {
-                    A[i * ld + p] = c * ap - s * aq;
-                    A[i * ld + q] = s * ap + c * aq;
+            // Both rotations at once: the thread owning rows {p_a, q_a} x columns
+            // {p_b, q_b} reads the four entries, rotates the rows by pair a and the
+            // columns by pair b (the order of the two one-sided passes) and writes
+            // them back; no other thread touches them, so one barrier suffices.
+            // A rotated diagonal block takes the closed form.
+            for (int e = threadIdx.x; e < npairs * npairs; e += NT) {
+                const int a = e / npairs, b = e - (e / npairs) * npairs;
+                const double sa = rs[a], sb = rs[b];
+                if (sa == 0.0 && sb == 0.0) continue;
+                const int pa = rp[a], qa = rq[a], pb = rp[b], qb = rq[b];
+                if (a == b) {
+                    A[pa * ld + pa] = rdp[a];
+                    A[qa * ld + qa] = rdq[a];
+                    A[pa * ld + qa] = 0.0;
+                    A[qa * ld + pa] = 0.0;
+                    continue;
                 }
-                const double vp = V[i * ld + p], vq = V[i * ld + q];
-                V[i * ld + p] = c * vp - s * vq;
-                V[i * ld + q] = s * vp + c * vq;
+                const double ca = rc[a], cb = rc[b];
+                const double xpp = A[pa * ld + pb];
+                const double xpq = qb >= 0 ? A[pa * ld + qb] : 0.0;
+                const double xqp = qa >= 0 ? A[qa * ld + pb] : 0.0;
+                const double xqq = (qa >= 0 && qb >= 0) ? A[qa * ld + qb] : 0.0;
+                const double rpp = ca * xpp - sa * xqp, rpq = ca * xpq - sa * xqq;
+                const double rqp = sa * xpp + ca * xqp, rqq = sa * xpq + ca * xqq;
+                A[pa * ld + pb] = cb * rpp - sb * rpq;
+                if (qb >= 0) A[pa * ld + qb] = sb * rpp + cb * rpq;
+                if (qa >= 0) {
+                    A[qa * ld + pb] = cb * rqp - sb * rqq;
+                    if (qb >= 0) A[qa * ld + qb] = sb * rqp + cb * rqq;
+                }
+            }
+            for (int e = threadIdx.x; e < npairs * k; e += NT) {
+                const int b = e / k, i = e - (e / k) * k;
+                const double sb = rs[b];
+                if (sb == 0.0) continue;
+                const int pb = rp[b], qb = rq[b];
+                const double cb = rc[b];
+                const double vp = V[i * ld + pb], vq = V[i * ld + qb];
+                V[i * ld + pb] = cb * vp - sb * vq;
+                V[i * ld + qb] = sb * vp + cb * vq;
             }
             __syncthreads();
         }
