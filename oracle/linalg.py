@@ -77,59 +77,73 @@ def _complete_rows(Keep: np.ndarray, need: int, basis: np.ndarray, min_norm: flo
     """Gauge-free completion for the SVD of a small matrix S expressed in the
     columns of ``basis`` (n x m): candidate c is u_c = basis[c, :] (the cell
     indicator e_c projected into span(basis), in basis coordinates), c in index
-    order; it is Gram-Schmidt'ed twice against Keep and the vectors accepted so
-    far and accepted when ||u_c|| > min_norm and the residual keeps at least half
-    of ||u_c||. Rotating the basis rotates the result with it, so basis @ result
-    does not depend on the basis chosen for the span. Falls back to canonical
-    vectors of R^m if the rows run out."""
+    order, then the canonical vectors of R^m; rows with ||u_c|| <= min_norm are
+    skipped. A candidate is Gram-Schmidt'ed twice against Keep and the vectors
+    accepted so far and accepted when the residual keeps at least half of
+    ||u_c||. If the candidates run out first (many null directions in a wide
+    basis: the canonical vectors' residuals then average sqrt((m - r)/m)), a
+    second scan from the first candidate accepts residuals above 1e-3 ||u_c||.
+    Rotating the basis rotates the result with it, so basis @ result does not
+    depend on the basis chosen for the span."""
     m = Keep.shape[0]
     cols = []
-    c = 0
-    cands = list(range(basis.shape[0]))
-    while len(cols) < need:
-        if c < len(cands):
-            u = np.array(basis[cands[c], :], dtype=np.float64)
-            nu = np.linalg.norm(u)
-            c += 1
-            if not nu > min_norm:
-                continue
-        else:
-            i = c - len(cands)
-            if i >= m:
-                raise RuntimeError("basis completion ran out of candidates")
-            u = np.zeros(m)
-            u[i] = 1.0
-            nu = 1.0
-            c += 1
-        Bc = np.column_stack([Keep] + cols) if (Keep.shape[1] + len(cols)) else np.zeros((m, 0))
-        v = u.copy()
-        for _ in range(2):
-            if Bc.shape[1]:
-                v = v - Bc @ (Bc.T @ v)
-        nv = np.linalg.norm(v)
-        if nv > 0.5 * nu:
-            cols.append(v / nv)
+    nrows = basis.shape[0]
+    for frac in (0.5, 1e-3):
+        c = 0
+        while len(cols) < need and c < nrows + m:
+            if c < nrows:
+                u = np.array(basis[c, :], dtype=np.float64)
+                nu = np.linalg.norm(u)
+                c += 1
+                if not nu > min_norm:
+                    continue
+            else:
+                u = np.zeros(m)
+                u[c - nrows] = 1.0
+                nu = 1.0
+                c += 1
+            Bc = np.column_stack([Keep] + cols) if (Keep.shape[1] + len(cols)) else np.zeros((m, 0))
+            v = u.copy()
+            for _ in range(2):
+                if Bc.shape[1]:
+                    v = v - Bc @ (Bc.T @ v)
+            nv = np.linalg.norm(v)
+            if nv > frac * nu:
+                cols.append(v / nv)
+        if len(cols) >= need:
+            break
+    if len(cols) < need:
+        raise RuntimeError("basis completion ran out of candidates")
     return np.column_stack(cols) if cols else np.zeros((m, 0))
 
 
 def _complete(B: np.ndarray, need: int, n: int, order=None) -> np.ndarray:
+    """``need`` unit vectors completing the columns of B: canonical vectors
+    e_c, c in ``order``, Gram-Schmidt'ed twice against B and the vectors taken
+    so far, accepted when the residual keeps at least half the norm. If the
+    candidates run out first (B nearly fills the space), a second scan from the
+    first candidate accepts residuals above 1e-3 (the best canonical candidate
+    keeps at least sqrt((n - rank B)/n), so the scan always succeeds)."""
     cols = []
     order = np.arange(n) if order is None else order
-    it = 0
-    while len(cols) < need:
-        if it >= len(order):
-            raise RuntimeError("basis completion ran out of canonical vectors")
-        c = order[it]
-        Bc = np.column_stack([B] + cols) if (B.shape[1] + len(cols)) else np.zeros((n, 0))
-        v = np.zeros(n)
-        v[c] = 1.0
-        for _ in range(2):
-            if Bc.shape[1]:
-                v = v - Bc @ (Bc.T @ v)
-        nv = np.linalg.norm(v)
-        if nv > 0.5:
-            cols.append(v / nv)
-        it += 1
+    for frac in (0.5, 1e-3):
+        it = 0
+        while len(cols) < need and it < len(order):
+            c = order[it]
+            Bc = np.column_stack([B] + cols) if (B.shape[1] + len(cols)) else np.zeros((n, 0))
+            v = np.zeros(n)
+            v[c] = 1.0
+            for _ in range(2):
+                if Bc.shape[1]:
+                    v = v - Bc @ (Bc.T @ v)
+            nv = np.linalg.norm(v)
+            if nv > frac:
+                cols.append(v / nv)
+            it += 1
+        if len(cols) >= need:
+            break
+    if len(cols) < need:
+        raise RuntimeError("basis completion ran out of canonical vectors")
     return np.column_stack(cols) if cols else np.zeros((n, 0))
 
 

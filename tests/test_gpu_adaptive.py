@@ -175,3 +175,24 @@ def test_fixed_rank_cap_rejected_at_solve():
     g = gsolver(22, 25, 7)
     with pytest.raises(_lib.TitusError, match="rank"):
         g.run(_lib.TITUS_DLR_FIXED, max_steps=2)
+
+
+@pytest.mark.parametrize("method,theta,steps", [("bug", 1e-3, 30), ("parallel", 3e-5, 6)])
+def test_rank_cap_80_with_growing_rank(method, theta, steps):
+    """settings.r = 80 (the largest cap): rank 40 entering the first step
+    (augmented width 80), then a tighter truncation tolerance lets the rank grow
+    (BUG: to 26 through rejections within 30 steps)."""
+    nx, npn, r = 26, 9, 80
+    os_ = OSettings(nx, nx, r, "csdPhantom", nPN=npn)
+    os_.theta = theta
+    gs = Settings(nx, nx, r, "csdPhantom", nPN=npn)
+    gs.theta = theta
+    if method == "bug":
+        o = solve_dlr_bug(OSolver(os_), max_steps=steps)
+        g = SolveFirstCollisionSourceDLRBUGRejection(SolverCSD(gs), max_steps=steps)
+        assert o[5][1].max() >= 20
+    else:
+        o = solve_dlr_parallel(OSolver(os_), max_steps=steps)
+        g = SolveFirstCollisionSourceDLRParallel(SolverCSD(gs), max_steps=steps)
+    np.testing.assert_array_equal(g[5][1], o[5][1])
+    assert dose_ok(g[4], o[4], nx)

@@ -155,3 +155,22 @@ def test_bug_rejections_repeat_energies():
     assert np.any(energies[1:] == energies[:-1])
     ranks = out[5][1]
     assert ranks.max() <= s.r and ranks.min() >= 2
+
+
+def test_completion_second_scan_fills_a_nearly_full_space():
+    """With a wide basis the canonical candidates' residuals average
+    sqrt((n - r)/n): the first scan (keep half the norm) can run out, the second
+    (keep 1e-3 of it) completes the space."""
+    rng = np.random.default_rng(5)
+    n, r = 30, 24
+    B = np.linalg.qr(rng.standard_normal((n, r)))[0]
+    C = la._complete(B, n - r, n)
+    Q = np.column_stack([B, C])
+    np.testing.assert_allclose(Q.T @ Q, np.eye(n), atol=1e-12)
+    # the same basis through the row rule of truncate!'s completion
+    m = 8
+    W = np.linalg.qr(rng.standard_normal((m + 2, m)))[0]
+    keep = np.linalg.qr(rng.standard_normal((m, 6)))[0]
+    V = la._complete_rows(keep, m - 6, W)
+    Qv = np.column_stack([keep, V])
+    np.testing.assert_allclose(Qv.T @ Qv, np.eye(m), atol=1e-12)

@@ -634,7 +634,8 @@ static __device__ __noinline__ bool range_find(WCtx& x, const bool do_side[2], c
 }
 
 // W-side completion in the small space: candidates m = 0, 1, ... accepted when
-// 1 - ||P[m,:]||^2 > 1/4 with P = [Q1 (nq1 cols, rows W[m,:] F1), Q2 (rows
+// 1 - ||P[m,:]||^2 > 1/4 (a second scan, if the first runs out: > 1e-6)
+// with P = [Q1 (nq1 cols, rows W[m,:] F1), Q2 (rows
 // C[m,:] RI), v_1 .. v_a]; stores per accepted vector its candidate, norm and
 // coefficients in SS_WC (row a, length nq1 + rho2 + a).
 static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, int need) {
@@ -645,17 +646,29 @@ static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, 
     const double* Ri = sside(x, 1, SS_RI);
     double* wrow = sm->vec;             // W[c,:] (k) then C[c,:] (rho2)
     double* prow = sm->vec + 2 * KA;    // P[c,:] (nq1 + rho2 + a <= 3 RA)
-    __shared__ int s_acc, s_next;
+    __shared__ int s_acc, s_next, s_phase;
     const int k = x.r;
     if (threadIdx.x == 0) {
         s_acc = 0;
         s_next = 0;
+        s_phase = 0;
     }
     __syncthreads();
     while (true) {
         const int acc = s_acc, it = s_next;
         if (acc >= need) break;
         if (it >= x.P.nwcomp) {
+            // second scan from the first candidate with the relaxed threshold
+            // (the basis nearly fills the moment space)
+            if (s_phase == 0) {
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    s_phase = 1;
+                    s_next = 0;
+                }
+                __syncthreads();
+                continue;
+            }
             if (threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
             __syncthreads();
             break;
@@ -685,7 +698,7 @@ static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, 
             double ss = 0.0;
             for (int j = 0; j < nb + acc; ++j) ss += prow[j] * prow[j];
             const double nv2 = 1.0 - ss;
-            if (nv2 > 0.25) {
+            if (nv2 > (s_phase == 0 ? 0.25 : 1e-6)) {
                 for (int j = 0; j < nb + acc; ++j) wc[acc * WCS + j] = prow[j];
                 sm->wcand[acc] = c;
                 sm->wnrm[acc] = sqrt(nv2);

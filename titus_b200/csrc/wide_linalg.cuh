@@ -359,7 +359,10 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
 // projected into the basis, taken in index order (then canonical vectors of
 // R^m); rows with norm <= 1e-6 are skipped; two Gram-Schmidt passes against
 // the columns before it; accepted when the residual keeps at least half the
-// candidate's norm. Same rule as oracle.linalg._complete_rows. Returns rho.
+// candidate's norm. When the candidates run out before every direction is
+// filled (many null directions in a wide basis), a second scan from the first
+// candidate accepts residuals above 1e-3 of the norm. Same rule as
+// oracle.linalg._complete_rows. Returns rho.
 static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld, int m, const double* sig,
                                                   const int* perm, int kkeep, double tol, int* status,
                                                   const double* rowsU, int nU, const double* rowsV, int nV,
@@ -386,10 +389,16 @@ static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld
         const double* rows = side == 0 ? rowsU : rowsV;
         const int nrows = side == 0 ? nU : nV;
         int cand = 0;   // [0, nrows): basis rows; [nrows, nrows + m): canonical vectors
+        int phase = 0;  // 0: keep half the candidate's norm; 1 (second scan): 1e-3 of it
         for (int j = rho; j < kkeep; ++j) {
             bool done = false;
             while (!done) {
                 if (cand >= nrows + m) {
+                    if (phase == 0) {
+                        phase = 1;
+                        cand = 0;
+                        continue;
+                    }
                     if (threadIdx.x == 0) set_status(status, ST_COMPLETION);
                     __syncthreads();
                     return rho;
@@ -460,7 +469,7 @@ static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld
                     sq = warp_sum(sq);
                     if (threadIdx.x == 0) {
                         s_nv = sqrt(sq);
-                        s_acc = (s_nv > 0.5 * s_nu) ? 1 : 0;
+                        s_acc = (s_nv > (phase == 0 ? 0.5 : 1e-3) * s_nu) ? 1 : 0;
                     }
                 }
                 __syncthreads();
