@@ -196,3 +196,17 @@ def test_rank_cap_80_with_growing_rank(method, theta, steps):
         g = SolveFirstCollisionSourceDLRParallel(SolverCSD(gs), max_steps=steps)
     np.testing.assert_array_equal(g[5][1], o[5][1])
     assert dose_ok(g[4], o[4], nx)
+
+
+def test_rank_beyond_capacity_fails_cleanly():
+    """A BUG rejection that doubles the rank past 40 (26 -> 52 here, with a
+    tight tolerance on 100 moments) ends the solve with TITUS_ERR_LIMIT; the
+    context stays usable for the next solve."""
+    nx, npn, r = 26, 9, 80
+    gs = Settings(nx, nx, r, "csdPhantom", nPN=npn)
+    gs.theta = 1e-4
+    g = SolverCSD(gs)
+    with pytest.raises(_lib.TitusError, match="capacity"):
+        g.run(_lib.TITUS_BUG_ADAPTIVE, max_steps=120)
+    out = gsolver(23, 8, 3).run(_lib.TITUS_BUG_ADAPTIVE, max_steps=5)
+    assert np.isfinite(out["dose"]).all()
