@@ -172,7 +172,8 @@ int titus_last_error(char* buf, size_t len);
  * [9] everything else, [10] boundary inflow, dose half-step and sweep; then
  * event counts: [11] Jacobi SVD sweeps, [12] SVD calls, [13] eigensolver calls,
  * [14] eigensolver sweeps, [15] Cholesky calls, [16] rank-revealing and [17]
- * certified range-finder sides. Returns the number of entries written (<= n). */
+ * certified range-finder sides, [18] team barriers (adaptive integrators).
+ * Returns the number of entries written (<= n). */
 int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
 
 /* Fixed-rank solve (method TITUS_DLR_FIXED) that allocates nothing. No

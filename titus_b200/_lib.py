@@ -21,7 +21,8 @@ TITUS_BUG_ADAPTIVE = 2
 PROFILE_NAMES = ["barrier", "reduce", "jacobi", "cholesky", "completion", "rows_stream", "rows_scatter", "rf_passes",
                  "small", "other", "prologue"]
 # event counters titus_profile appends after the timers
-PROFILE_COUNTERS = ["svd_sweeps", "svd_calls", "eig_calls", "eig_sweeps", "chol_calls", "rf_slow", "rf_fast"]
+PROFILE_COUNTERS = ["svd_sweeps", "svd_calls", "eig_calls", "eig_sweeps", "chol_calls", "rf_slow", "rf_fast",
+                    "barriers"]
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

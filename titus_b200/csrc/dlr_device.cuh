@@ -60,7 +60,8 @@ enum ProfCat { PF_BARRIER = 0, PF_REDUCE, PF_JACOBI, PF_CHOL, PF_COMPLETE, PF_RO
                PF_RF_PASSES, PF_SMALL, PF_TOTAL, PF_PROLOGUE, PF_COUNT };
 // event counters in the timer buffer (profiled CTA only; the buffer has PF_SLOTS entries)
 constexpr int PF_SVD_SWEEPS = 12, PF_SVD_CALLS = 13;
-constexpr int PF_EIG_CALLS = 16, PF_EIG_SWEEPS = 17, PF_CHOL_CALLS = 18, PF_RF_SLOW = 19, PF_RF_FAST = 20;
+constexpr int PF_EIG_CALLS = 16, PF_EIG_SWEEPS = 17, PF_CHOL_CALLS = 18, PF_RF_SLOW = 19, PF_RF_FAST = 20,
+              PF_BARRIERS = 21;
 constexpr int PF_SLOTS = 32;
 __device__ __forceinline__ void prof_count(unsigned long long* p, int slot, unsigned long long v) {
     if (p && threadIdx.x == 0) p[slot] += v;

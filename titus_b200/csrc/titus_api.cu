@@ -441,9 +441,9 @@ extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
     CK(cudaMemcpy(cyc, s->prof, sizeof(cyc), cudaMemcpyDeviceToHost));
     // [0, PF_COUNT): phase times (ns); then event counts: SVD sweeps, SVD calls,
     // eigensolver calls, eigensolver sweeps, Cholesky calls, rank-revealing and
-    // certified range-finder sides
+    // certified range-finder sides, team barriers
     const int counters[] = {PF_SVD_SWEEPS, PF_SVD_CALLS, PF_EIG_CALLS, PF_EIG_SWEEPS, PF_CHOL_CALLS, PF_RF_SLOW,
-                            PF_RF_FAST};
+                            PF_RF_FAST, PF_BARRIERS};
     const int nc = (int)(sizeof(counters) / sizeof(counters[0]));
     int m = 0;
     for (int i = 0; i < PF_COUNT && m < n; ++i, ++m) ns[m] = (double)cyc[i] * 1e6 / (double)s->clock_khz;

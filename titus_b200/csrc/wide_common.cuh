@@ -142,6 +142,7 @@ __device__ __forceinline__ bool is_bnd_w(const DevProblem& P, int c) {
 
 __device__ __forceinline__ bool wsync(WCtx& x) {
     ProfScope ps(x.prof, PF_BARRIER);
+    prof_count(x.prof, PF_BARRIERS, 1ull);
     return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag);
 }
 

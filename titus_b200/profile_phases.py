@@ -44,6 +44,8 @@ def main():
         events["svd_sweeps_per_call"] = counters["svd_sweeps"] / counters["svd_calls"]
     if counters.get("eig_calls"):
         events["eig_sweeps_per_call"] = counters["eig_sweeps"] / counters["eig_calls"]
+    if counters.get("barriers") and "barrier" in prof:
+        events["us_per_barrier_wait"] = prof["barrier"] / 1e3 / counters["barriers"]
     hist = out["rank_history"]
     print(json.dumps({"workload": vars(a), "steps": out["steps"], "rank": out["rank"],
                       "rank_max": int(hist.max()), "wall_s": wall, "us_per_step": per_step,
