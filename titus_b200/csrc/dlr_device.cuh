@@ -131,15 +131,14 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
-// Team barrier without atomics: CTA b publishes its arrival generation in
-// flags[b]; CTA 0 polls all arrival flags (one thread per CTA) and then
-// publishes the release generation in flags[G]; the others poll that. Every
-// spin is bounded (about a second); on expiry the status flag is set and all
-// CTAs leave. Returns false if the team's status flag is set.
+// Team barrier, one hop through L2: after the CTA's writes, thread 0 fences and
+// adds 1 to the team's arrival counter flags[G], then waits (acquire loads)
+// until the counter reaches gen * G, i.e. every CTA of the team has arrived at
+// this generation. The counter runs modulo 2^32; the signed difference compares
+// correctly while fewer than 2^31 arrivals separate the two values. flags[0, G)
+// are not used. Every spin is bounded (about a second); on expiry the status
+// flag is set and all CTAs leave. Returns false if the team's status flag is set.
 __device__ inline bool team_sync(unsigned* flags, int* status, int G, int b, unsigned& gen, double* diag = nullptr) {
     __shared__ int s_ok;
     constexpr long long kSpinLimit = 1ll << 21;
@@ -147,45 +146,22 @@ __device__ inline bool team_sync(unsigned* flags, int* status, int G, int b, uns
     ++gen;
     if (threadIdx.x == 0) {
         __threadfence();
-        st_release(flags + b, gen);
-    }
-    if (b == 0) {
-        for (int t = threadIdx.x; t < G; t += NT) {
-            long long it = 0;
-            while (ld_acquire(flags + t) != gen) {
-                if (++it > kSpinLimit) {
-                    if (atomicCAS(status, 0, ST_BARRIER_TIMEOUT) == 0 && diag) {
-                        diag[8] = t;
-                        diag[9] = ld_acquire(flags + t);
-                        diag[10] = gen;
-                    }
-                    break;
-                }
-                if (it > 32) __nanosleep(200);
-                if ((it & 255) == 0 && ldcg(status) != 0) break;
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            st_release(flags + G, gen);
-        }
-    } else if (threadIdx.x == 0) {
+        const unsigned target = gen * (unsigned)G;
+        unsigned seen = atomicAdd(flags + G, 1u) + 1u;
         long long it = 0;
-        while (ld_acquire(flags + G) != gen) {
+        while ((int)(seen - target) < 0) {
             if (++it > kSpinLimit) {
                 if (atomicCAS(status, 0, ST_BARRIER_TIMEOUT) == 0 && diag) {
-                    diag[8] = 1000 + b;
-                    diag[9] = ld_acquire(flags + G);
-                    diag[10] = gen;
+                    diag[8] = b;
+                    diag[9] = seen;
+                    diag[10] = target;
                 }
                 break;
             }
             if (it > 32) __nanosleep(200);
             if ((it & 255) == 0 && ldcg(status) != 0) break;
+            seen = ld_acquire(flags + G);
         }
-    }
-    if (threadIdx.x == 0) {
         __threadfence();
         s_ok = (ldcg(status) == 0);
     }

@@ -280,12 +280,10 @@ static int check_status(titus_solver* s) {
         double d[16];
         CK(cudaMemcpy(d, s->st.diag, sizeof(d), cudaMemcpyDeviceToHost));
         if (status == ST_BARRIER_TIMEOUT) {
-            std::vector<unsigned> fl(s->num_sms + 1);
-            CK(cudaMemcpy(fl.data(), s->st.bar, fl.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
-            std::string arr;
-            for (int i = 0; i < s->last_G; ++i) arr += std::to_string(fl[i]) + " ";
-            return fail(TITUS_ERR_DEVICE, "device status %d: %s (waiter %g saw %g wanted %g; release %u; arrivals %s)",
-                        status, what, d[8], d[9], d[10], fl[s->last_G], arr.c_str());
+            unsigned counter = 0;
+            CK(cudaMemcpy(&counter, s->st.bar + s->last_G, sizeof(unsigned), cudaMemcpyDeviceToHost));
+            return fail(TITUS_ERR_DEVICE, "device status %d: %s (CTA %g saw %g arrivals, wanted %g; counter now %u)",
+                        status, what, d[8], d[9], d[10], counter);
         }
         if (status == ST_CHOL_BREAKDOWN)
             return fail(TITUS_ERR_DEVICE,
