@@ -38,6 +38,7 @@ __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0
                                  int fc) {
     const DevProblem& P = x.P;
     const double hx = 0.5 / P.dx, hy = 0.5 / P.dy;
+    const double ix = 1.0 / P.dx, iy = 1.0 / P.dy;
     for (int e = threadIdx.x; e < nr * k; e += NT) {
         const int r = e / k, j = e - (e / k) * k;
         const int c = r0 + r;
@@ -50,8 +51,8 @@ __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0
             const double ayp = ldcg(A + (size_t)(c + 1) * lda + j) * P.rinv[c + 1];
             l2x = (axp - axm) * hx;
             l2y = (ayp - aym) * hy;
-            l1x = a0 / P.dx - hx * axm - hx * axp;
-            l1y = a0 / P.dy - hy * aym - hy * ayp;
+            l1x = a0 * ix - hx * axm - hx * axp;
+            l1y = a0 * iy - hy * aym - hy * ayp;
         }
         double* row = F + r * ldf + fc;
         row[0 * k + j] = l2x;
@@ -128,6 +129,14 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
     const double dE = P.dE;
     const double den = 1.0 + dE * sigma0;
     const int q = P.q;
+    // the per-ordinate quotients Omega_x / dx, Omega_z / dy, formed once
+    __shared__ double s_cx[QW], s_cz[QW];
+    __syncthreads();   // a previous call's readers are done
+    for (int l = threadIdx.x; l < q; l += NT) {
+        s_cx[l] = P.omega[l * 3 + 0] / P.dx;
+        s_cz[l] = P.omega[l * 3 + 2] / P.dy;
+    }
+    __syncthreads();
     for (int e = threadIdx.x; e < (x.c1 - x.c0) * q; e += NT) {
         const int c = x.c0 + e / q, kq = e - (e / q) * q;
         const double pc = ldcg(x.psi_in + (size_t)c * QW + kq);
@@ -140,7 +149,7 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
             else ew = ldcg(x.psi_in + (size_t)(c + P.ny) * QW + kq) * P.rinv[c + P.ny] - f0;
             if (oz >= 0.0) ns = f0 - ldcg(x.psi_in + (size_t)(c - 1) * QW + kq) * P.rinv[c - 1];
             else ns = ldcg(x.psi_in + (size_t)(c + 1) * QW + kq) * P.rinv[c + 1] - f0;
-            flux = (ox / P.dx) * ew + (oz / P.dy) * ns;
+            flux = s_cx[kq] * ew + s_cz[kq] * ns;
         }
         double out = (pc - dE * flux) / den;
         if (kq == 0 && P.restore[c]) out = pc;
