@@ -48,7 +48,7 @@ ORACLE_SAMPLE_STEPS = 40
 # one ncu capture of the first energy steps (see profiles/); the per-launch
 # figure scales it to the launch's energy steps.
 DRAM_BYTES_PER_STEP_NCU = {"fixed": (5.010176e6 + 0.218112e6) / 20,
-                           "bug": (79.593472e6 + 194.938880e6) / 20, "parallel": None}
+                           "bug": (77.263616e6 + 193.732352e6) / 20, "parallel": None}
 
 
 def algorithmic_bytes_per_step(n, r, q, w=8):
