@@ -95,7 +95,8 @@ typedef struct titus_result {
                               index n at [n-1]; BUG: rank at the start of each loop iteration
                               (repeated energies included, first nE iterations); -1 if unused */
     double* eta_history;   /* optional (nE): BUG streaming eta of each rejection test, in order */
-    double* bound_history; /* optional (nE): the matching bound c_eta theta max(1e-7,||S||)/dE */
+    double* bound_history; /* optional (nE): the matching bound
+                              c_eta * theta * max(1e-7, ||S||^theta_index) / dE (SolverCSD.jl:2224) */
     double* time_history;  /* optional (nE): parallel: pseudo-time t at [n-1];
                               BUG: energy index n (1-based) of each iteration */
 } titus_result_t;
@@ -134,6 +135,14 @@ int titus_set_state(titus_solver_t* solver, int32_t rank, const double* X, const
                     const double* W, const double* psi, const double* dose, int32_t n_next);
 int titus_solve_from(titus_solver_t* solver, int32_t method, const titus_options_t* options,
                      int32_t n_stop, titus_result_t* result);
+
+/* Where the last solve on this handle stopped: the 1-based energy index the
+ * loop would process next (the reference loop variable n; a rejected BUG step
+ * repeats its n) and, for the adaptive integrators, the pseudo-time t of
+ * SolverCSD.jl:1763 / :2100 (fixed rank: (n_next - 2) dE). With
+ * titus_fetch's factors this is a complete checkpoint for titus_set_state.
+ * `t` may be NULL. */
+int titus_resume_point(titus_solver_t* solver, int32_t* n_next, double* t);
 
 /* One pencil beam of a batched solve: its own energy grid (5 MeV -> cutoff
  * grid of the base problem replaced by this spot's) and entry profile. All
@@ -208,6 +217,19 @@ int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* o
  * TITUS_ERR_LIMIT (ny*q >= 2^31) or TITUS_ERR_CUDA. */
 int titus_limited_flux(int32_t nx, int32_t ny, int32_t q, double dx, double dy, const double* omega_x,
                        const double* omega_z, const double* phi, double* flux, void* stream);
+
+/* Test hooks (no counterpart in the reference), for failure-detection tests
+ * that fault nothing.
+ * titus_debug_barrier_fault: the NEXT launch on this handle bounds every team
+ * barrier wait by `spin_limit` polls (0 = default, about a second), and CTA 1
+ * of the team does not arrive at barrier number `barrier` (1-based, counted from
+ * the start of the launch; <= 0 = every CTA arrives). The waits run out, the
+ * kernel leaves, the solve returns TITUS_ERR_DEVICE naming the barrier, and the
+ * handle stays usable. Needs a team of >= 2 CTAs; applies to one launch only.
+ * titus_debug_fail_alloc: the `after`-th device allocation from now (any handle)
+ * fails as if cudaMalloc had returned cudaErrorMemoryAllocation; 0 = off. */
+int titus_debug_barrier_fault(titus_solver_t* solver, int32_t barrier, int64_t spin_limit);
+int titus_debug_fail_alloc(int32_t after);
 
 /* Build / capability queries. */
 int titus_max_rank(void);        /* largest settings.r accepted (adaptive rank cap) */

@@ -40,3 +40,30 @@ def test_invalid_problem_is_rejected_without_gpu():
     rc = lib.titus_create(C.byref(p), C.byref(h))
     assert rc == 1
     assert "nx" in _lib.last_error()
+
+
+def _problem_with(field, index, value):
+    """A small valid problem (host arrays) with one entry set to `value`."""
+    from titus_b200 import Settings, SolverCSD
+    sv = SolverCSD(Settings(12, 12, 4, "csdWaterBeam", nPN=3))
+    p, keep = sv.problem_struct()
+    arr = getattr(p, field)
+    arr[index] = value
+    return p, keep
+
+
+@pytest.mark.parametrize("field,index", [("density", 5), ("stopping", 3), ("sigma", 2), ("bc_space", 0),
+                                         ("m_reduced", 7), ("omega", 4), ("e_trafo", 1)])
+@pytest.mark.parametrize("value", [float("nan"), float("inf")])
+def test_non_finite_inputs_are_rejected_without_gpu(field, index, value):
+    """titus_create validates every float input before touching the device."""
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libtitus.so not built")
+    import ctypes as C
+    lib = _lib.load()
+    p, keep = _problem_with(field, index, value)
+    h = C.c_void_p()
+    rc = lib.titus_create(C.byref(p), C.byref(h))
+    assert rc == 1
+    err = _lib.last_error()
+    assert ("not finite" in err or "density must be > 0" in err) and field.split("_")[0] in err, err

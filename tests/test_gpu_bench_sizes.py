@@ -1,0 +1,195 @@
+"""GPU parity at the benchmarked problem sizes, against the FP64 oracle.
+
+The benchmark solves the seeded 200 x 200 phantom at P29 (900 moments) with
+rank cap 80 over 29 695 BUG iterations; the batched benchmark runs pencil beams
+of 2-8 MeV on the 128 x 128 phantom at P21 with cap 60; the fixed-rank
+benchmark is the 100 x 100 water beam at P21, r = 20. A whole oracle sweep of
+these takes tens of minutes to hours, so they are compared in the pieces an
+oracle run finishes in seconds:
+
+* the first 200 BUG iterations of the 200 x 200 phantom as one whole run
+  (rank 40 entering, every rejection and truncation of the opening steps): rank
+  of every iteration exactly, dose and psi <= 1e-10, the streaming eta values
+  and their bounds;
+* the parallel integrator's first 5 steps on the same problem;
+* three windows from the middle of the BUG sweep (iterations 5 000, 15 000
+  and 25 000): the GPU's own state there (titus_fetch + titus_resume_point) is
+  handed to both paths, which then run 10 iterations each; the dose increment
+  over the window and psi at <= 1e-10, ranks exactly;
+* the fixed-rank water beam for 100 steps from its state after 1 500 steps;
+* three pencil beams of 2-8 MeV on the 128 x 128 phantom, first 200
+  iterations each, in one batched launch.
+
+Tolerances follow the conditioning measured on the oracle (the same rules as
+test_gpu_adaptive.py): factor products, the scalar flux and eta are bounded by
+max(1e-10, 4 x the oracle's own change under 1e-14 input noise) when they miss
+1e-10, because they depend on singular directions that rounding moves.
+"""
+import numpy as np
+import pytest
+
+from oracle.settings import Settings as OSettings
+from oracle.solver import SolverCSD as OSolver
+from oracle.solver import solve_dlr_bug, solve_dlr_fixed, solve_dlr_parallel
+from titus_b200 import (Settings, SolverCSD, SolveFirstCollisionSourceDLRBUGRejection,
+                        SolveFirstCollisionSourceDLRParallel, SolveBatchedPencilBeams, _lib, scalar_flux)
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+NX2, NPN2, CAP2 = 201, 29, 80          # 200 x 200 phantom, P29, rank cap 80
+NX1, NPN1, R1 = 101, 21, 20            # 100 x 100 water beam, P21, r = 20
+NX3, NPN3, CAP3 = 129, 21, 60          # 128 x 128 phantom, P21, cap 60
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def bnd_mask(nx):
+    i, j = np.divmod(np.arange((nx - 1) ** 2), nx - 1)
+    return (i == 0) | (j == 0) | (i == nx - 2) | (j == nx - 2)
+
+
+def dose_ok(gd, od, nx, tol=TOL):
+    """Interior relative L2 <= tol; ghost cells absolutely <= 1e-8 ||dose||."""
+    b = bnd_mask(nx)
+    return rel(gd[~b], od[~b]) <= tol and np.abs(gd[b] - od[b]).max() <= 1e-8 * np.linalg.norm(od)
+
+
+@pytest.fixture(scope="module")
+def phantom_gpu():
+    return SolverCSD(Settings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2), team_ctas=148)
+
+
+def test_phantom_200_bug_first_200_iterations(phantom_gpu):
+    steps = 200
+    o = solve_dlr_bug(OSolver(OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)), max_steps=steps)
+    g = SolveFirstCollisionSourceDLRBUGRejection(phantom_gpu, max_steps=steps)
+    np.testing.assert_array_equal(g[5][1], o[5][1])            # rank of every iteration
+    np.testing.assert_allclose(g[5][0], o[5][0], rtol=1e-12)   # energy of every iteration
+    assert o[5][1][0] == CAP2 // 2                             # entered at rank 40 (width 80)
+    assert dose_ok(g[4], o[4], NX2)
+    assert rel(g[8].ravel(), o[8].ravel()) <= TOL              # psi
+    assert g[6].shape[0] == o[6].shape[0]                      # one eta per rejection test
+    np.testing.assert_allclose(g[7][:, 1], o[7][:, 1], rtol=1e-10)
+    eerr = np.max(np.abs(g[6][:, 1] - o[6][:, 1]) / np.abs(o[6][:, 1]).max()) if o[6].size else 0.0
+    uerr = rel(scalar_flux(g[0], g[1], g[3]), scalar_flux(o[0], o[1], o[3]))
+    if eerr > 1e-8 or uerr > TOL:
+        # the oracle's own change under 1e-14 density noise
+        su = se = 0.0
+        for seed in (1, 2):
+            s = OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)
+            s.density = s.density * (1 + 1e-14 * np.random.default_rng(seed).standard_normal(s.density.shape))
+            p = solve_dlr_bug(OSolver(s), max_steps=steps)
+            su = max(su, rel(scalar_flux(p[0], p[1], p[3]), scalar_flux(o[0], o[1], o[3])))
+            if p[6].shape == o[6].shape:
+                se = max(se, np.max(np.abs(p[6][:, 1] - o[6][:, 1]) / np.abs(o[6][:, 1]).max()))
+        assert uerr <= max(TOL, 4 * su)
+        assert eerr <= max(1e-8, 4 * se)
+
+
+def test_phantom_200_parallel_first_steps():
+    steps = 5
+    o = solve_dlr_parallel(OSolver(OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)), max_steps=steps)
+    g = SolveFirstCollisionSourceDLRParallel(SolverCSD(Settings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2),
+                                                       team_ctas=148), max_steps=steps)
+    np.testing.assert_array_equal(g[5][1], o[5][1])
+    assert dose_ok(g[4], o[4], NX2)
+    assert rel(g[6].ravel(), o[6].ravel()) <= TOL
+
+
+def _window(gsolver, osettings, method, fn, state, steps, nx):
+    """Both paths run `steps` iterations from the same state; returns the
+    oracle's and the GPU's end states."""
+    ref = fn(OSolver(osettings()), max_steps=steps, state=state, n_begin=state["n_next"], return_state=True)
+    n_stop = gsolver.nE if method != _lib.TITUS_PARALLEL_ADAPTIVE else state["n_next"] + steps - 1
+    got = gsolver.run_from(method, state, state["n_next"], n_stop, max_steps=steps)
+    return ref, got
+
+
+def test_phantom_200_bug_mid_sweep_windows(phantom_gpu):
+    """Iterations 5 000, 15 000 and 25 000 of the 29 695: 10 iterations each
+    from the GPU's own state, GPU against oracle."""
+    steps = 10
+    osettings = lambda: OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)  # noqa: E731
+    mid = _lib.TITUS_BUG_ADAPTIVE
+    prev, done = None, 0
+    for at in (5000, 15000, 25000):
+        if prev is None:
+            cur = phantom_gpu.run(mid, max_steps=at)
+        else:
+            cur = phantom_gpu.run_from(mid, prev, prev["n_next"], phantom_gpu.nE, max_steps=at - done)
+        done = at
+        state = dict(X=cur["X"].copy(), S=cur["S"].copy(), W=cur["W"].copy(), psi=cur["psi"].copy(),
+                     dose=cur["dose"].copy(), t=cur["t"], n_next=cur["n_next"])
+        prev = state
+        ref, got = _window(phantom_gpu, osettings, mid, solve_dlr_bug, state, steps, NX2)
+        assert got["rank"] == ref["S"].shape[0], at
+        assert got["n_next"] == ref["n_next"], at
+        inc_ref = ref["dose"] - state["dose"]
+        inc_got = got["dose"] - state["dose"]
+        assert dose_ok(inc_got, inc_ref, NX2), (at, rel(inc_got, inc_ref))
+        assert rel(got["psi"].ravel(), ref["psi"].ravel()) <= TOL or np.abs(ref["psi"]).max() == 0.0
+        P_ref = ref["X"] @ ref["S"] @ ref["W"].T
+        perr = rel(got["X"] @ got["S"] @ got["W"].T, P_ref)
+        if perr > TOL:
+            sens = 0.0
+            for seed in (1, 2):
+                st2 = dict(state)
+                st2["S"] = state["S"] * (1 + 1e-14 * np.random.default_rng(seed).standard_normal(state["S"].shape))
+                o2 = solve_dlr_bug(OSolver(osettings()), max_steps=steps, state=st2, n_begin=state["n_next"],
+                                   return_state=True)
+                sens = max(sens, rel(o2["X"] @ o2["S"] @ o2["W"].T, P_ref))
+            assert perr <= max(TOL, 4 * sens), (at, perr, sens)
+
+
+def test_water_beam_100_fixed_rank_100_steps_mid_sweep():
+    """Fixed rank r = 20 on the 100 x 100 water beam: 100 steps from the GPU's
+    state after 1 500 of its 3 694 steps. The low-rank fixed-rank integrator
+    amplifies rounding (measured on the oracle), so the factor product and the
+    dose increment are held to max(1e-10, 4 x the oracle's own change under
+    1e-14 noise in the handed-over S)."""
+    steps = 100
+    g = SolverCSD(Settings(NX1, NX1, R1, "csdWaterBeam", nPN=NPN1))
+    cur = g.run(_lib.TITUS_DLR_FIXED, max_steps=1500)
+    state = dict(X=cur["X"].copy(), S=cur["S"].copy(), W=cur["W"].copy(), psi=cur["psi"].copy(),
+                 dose=cur["dose"].copy(), n_next=cur["n_next"])
+    assert state["n_next"] == 1502
+    mk = lambda: OSolver(OSettings(NX1, NX1, R1, "csdWaterBeam", nPN=NPN1))  # noqa: E731
+    ref = solve_dlr_fixed(mk(), max_steps=steps, state=state, n_begin=state["n_next"], return_state=True)
+    got = g.run_from(_lib.TITUS_DLR_FIXED, state, state["n_next"], state["n_next"] + steps - 1)
+    inc_ref = ref["dose"] - state["dose"]
+    inc_got = got["dose"] - state["dose"]
+    P_ref = ref["X"] @ ref["S"] @ ref["W"].T
+    derr = rel(inc_got, inc_ref)
+    perr = rel(got["X"] @ got["S"] @ got["W"].T, P_ref)
+    assert rel(got["psi"].ravel(), ref["psi"].ravel()) <= TOL or np.abs(ref["psi"]).max() == 0.0
+    if derr > TOL or perr > TOL:
+        sd = sp = 0.0
+        for seed in (1, 2):
+            st2 = dict(state)
+            st2["S"] = state["S"] * (1 + 1e-14 * np.random.default_rng(seed).standard_normal(state["S"].shape))
+            o2 = solve_dlr_fixed(mk(), max_steps=steps, state=st2, n_begin=state["n_next"], return_state=True)
+            sd = max(sd, rel(o2["dose"] - state["dose"], inc_ref))
+            sp = max(sp, rel(o2["X"] @ o2["S"] @ o2["W"].T, P_ref))
+        assert derr <= max(TOL, 4 * sd), (derr, sd)
+        assert perr <= max(TOL, 4 * sp), (perr, sp)
+
+
+def test_pencil_beams_2_to_8_MeV_on_128_phantom():
+    """Three spots of the batched benchmark's distribution (seeded energies in
+    [2, 8] MeV, entry y0 in [0.1, 0.9]), first 200 BUG iterations each, in one
+    batched launch of 1-CTA teams, against one oracle solve per spot."""
+    steps = 200
+    rng = np.random.default_rng(11)
+    spots = [(float(e), float(y)) for e, y in zip(rng.uniform(2.0, 8.0, 3), rng.uniform(0.1, 0.9, 3))]
+    g = SolverCSD(Settings(NX3, NX3, CAP3, "csdPhantom", nPN=NPN3))
+    dose, rank, iters = SolveBatchedPencilBeams(g, spots, "bug", team_ctas=1, max_steps=steps)
+    for i, (e, y) in enumerate(spots):
+        s = OSettings(NX3, NX3, CAP3, "csdPhantom", nPN=NPN3)
+        s.eMax, s.y0 = e, y
+        st = solve_dlr_bug(OSolver(s), max_steps=steps, return_state=True)
+        assert iters[i] == st["iters"] == steps
+        assert rank[i] == st["S"].shape[0], (i, rank[i], st["S"].shape[0])
+        assert dose_ok(dose[i], st["dose"], NX3), (i, rel(dose[i], st["dose"]))

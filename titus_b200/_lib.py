@@ -70,6 +70,7 @@ SIGNATURES = [
     ("titus_solve_problem", C.c_int, [C.POINTER(Problem), C.c_int32, C.POINTER(Options), C.POINTER(Result)]),
     ("titus_set_state", C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _dp, _dp, _dp, C.c_int32]),
     ("titus_solve_from", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_int32, C.POINTER(Result)]),
+    ("titus_resume_point", C.c_int, [C.c_void_p, _ip, _dp]),
     ("titus_solve_batched", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_int32, C.POINTER(Spot), _dp,
                                       _ip, _ip]),
     ("titus_destroy", None, [C.c_void_p]),
@@ -79,6 +80,8 @@ SIGNATURES = [
                                       C.c_void_p, C.c_char_p, C.c_size_t]),
     ("titus_limited_flux", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("titus_debug_barrier_fault", C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
+    ("titus_debug_fail_alloc", C.c_int, [C.c_int32]),
     ("titus_max_rank", C.c_int, []),
     ("titus_max_ordinates", C.c_int, []),
     ("titus_version", C.c_char_p, []),

@@ -53,6 +53,8 @@ struct DevProblem {
     const uint8_t* restore;   // n: 1 if ordinate-0 value is restored after the sweep
     unsigned long long* prof; // optional phase timers (SM cycles), recorded by CTA 0 of team 0
     int zero_smem;            // 1: clear the dynamic shared memory at kernel start
+    long long spin_limit;     // polls before a team barrier gives up (0 = default, about a second)
+    int fault_barrier;        // test hook: CTA 1 does not arrive at this barrier generation (<= 0: off)
 };
 
 // Phase-timer categories (titus_profile reports them in this order).
@@ -137,24 +139,38 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 // until the counter reaches gen * G, i.e. every CTA of the team has arrived at
 // this generation. The counter runs modulo 2^32; the signed difference compares
 // correctly while fewer than 2^31 arrivals separate the two values. flags[0, G)
-// are not used. Every spin is bounded (about a second); on expiry the status
-// flag is set and all CTAs leave. Returns false if the team's status flag is set.
-__device__ inline bool team_sync(unsigned* flags, int* status, int G, int b, unsigned& gen, double* diag = nullptr) {
+// are not used. Every spin is bounded (`spin_limit` polls, default 2^21 with
+// 200 ns sleeps: about a second); on expiry the status flag is set, the
+// diagnostics record the CTA, the counter it saw and the one it waited for, and
+// all CTAs leave. `fault_gen` >= 1 is a test hook: CTA 1 skips its arrival at
+// that generation, so the wait runs out (the host reads the status; nothing
+// faults). Returns false if the team's status flag is set.
+__device__ inline bool team_sync(unsigned* flags, int* status, int G, int b, unsigned& gen, double* diag = nullptr,
+                                 long long spin_limit = 0, int fault_gen = -1) {
     __shared__ int s_ok;
-    constexpr long long kSpinLimit = 1ll << 21;
+    const long long limit = spin_limit > 0 ? spin_limit : (1ll << 21);
     __syncthreads();
     ++gen;
+    if (G == 1) {
+        // a one-CTA team: __syncthreads already orders the block's global
+        // writes before its later reads; only the status flag is shared
+        if (threadIdx.x == 0) s_ok = (ldcg(status) == 0);
+        __syncthreads();
+        return s_ok;
+    }
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned target = gen * (unsigned)G;
-        unsigned seen = atomicAdd(flags + G, 1u) + 1u;
+        const bool skip = (b == 1 && (int)gen == fault_gen);
+        unsigned seen = skip ? ld_acquire(flags + G) : atomicAdd(flags + G, 1u) + 1u;
         long long it = 0;
         while ((int)(seen - target) < 0) {
-            if (++it > kSpinLimit) {
+            if (++it > limit) {
                 if (atomicCAS(status, 0, ST_BARRIER_TIMEOUT) == 0 && diag) {
                     diag[8] = b;
                     diag[9] = seen;
                     diag[10] = target;
+                    diag[14] = gen;
                 }
                 break;
             }

@@ -7,7 +7,7 @@ namespace titus {
 
 __device__ __forceinline__ bool tsync(Ctx& x) {
     ProfScope ps(x.prof, PF_BARRIER);
-    return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag);
+    return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag, x.P.spin_limit, x.P.fault_barrier);
 }
 
 // Publish this CTA's partial reduction of `count` entries and synchronise the

@@ -114,6 +114,7 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
     P.prof = nullptr;
     P.zero_smem = 0;
+    s->take_debug_hooks(P);
     if (opt && opt->profile) {
         CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));
         P.prof = s->prof;
@@ -148,6 +149,12 @@ int check_status(titus_solver* s) {
                        : status == ST_SVD            ? "Jacobi SVD did not converge"
                                                      : "device error";
     const int code = status == ST_LIMIT ? TITUS_ERR_LIMIT : TITUS_ERR_DEVICE;
+    if (status == ST_BARRIER_TIMEOUT) {
+        unsigned counter = 0;
+        CK(cudaMemcpy(&counter, s->wst.bar + s->last_G, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        return fail(code, "device status %d: %s (CTA %g at barrier %g saw %g arrivals, wanted %g; counter now %u)",
+                    status, what, d[8], d[14], d[9], d[10], counter);
+    }
     if (status == ST_SVD) {
         // statistics of the matrix handed to the SVD (CTA 0's copy)
         std::vector<double> a((size_t)KA * KA);
@@ -404,6 +411,7 @@ int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_opti
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
     P.prof = nullptr;
     P.zero_smem = 0;
+    s->take_debug_hooks(P);
     if (opt && opt->profile) {
         CK(cudaMemset(s->prof, 0, PF_SLOTS * sizeof(unsigned long long)));
         P.prof = s->prof;

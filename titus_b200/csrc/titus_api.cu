@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
@@ -17,7 +19,15 @@ using titus_host::fail;
 
 namespace {
 thread_local std::string g_last_error;
+std::atomic<int> g_alloc_fault{0};
 }  // namespace
+
+int titus_host::take_alloc_fault() {
+    int v = g_alloc_fault.load();
+    while (v > 0 && !g_alloc_fault.compare_exchange_weak(v, v - 1)) {
+    }
+    return v == 1;
+}
 
 int titus_host::fail(int code, const char* fmt, ...) {
     char buf[768];
@@ -48,11 +58,34 @@ static int validate(const titus_problem_t* pb) {
     if (pb->r > 2 * wide::RA)
         return fail(TITUS_ERR_LIMIT, "rank cap %d > %d supported by this build", pb->r, 2 * wide::RA);
     if (pb->r > pb->n_moments) return fail(TITUS_ERR_ARG, "r %d > n_moments %d", pb->r, pb->n_moments);
-    if (!(pb->dx > 0) || !(pb->dy > 0)) return fail(TITUS_ERR_ARG, "dx, dy must be > 0");
+    if (!(pb->dx > 0) || !(pb->dy > 0) || !std::isfinite(pb->dx) || !std::isfinite(pb->dy))
+        return fail(TITUS_ERR_ARG, "dx, dy must be finite and > 0");
+    if (!std::isfinite(pb->theta) || !std::isfinite(pb->theta_index) || !std::isfinite(pb->c_eta))
+        return fail(TITUS_ERR_ARG, "theta, theta_index and c_eta must be finite");
     const void* req[] = {pb->density, pb->e_trafo, pb->stopping, pb->bc_energy, pb->sigma,
                          pb->bc_space, pb->bc_angle, pb->omega, pb->m_reduced};
     for (const void* p : req)
         if (!p) return fail(TITUS_ERR_ARG, "a required problem array is NULL");
+    // non-finite inputs would propagate through the whole energy loop unnoticed
+    {
+        const int n = pb->nx * pb->ny, nE = pb->n_energies, q = pb->n_ordinates, N = pb->n_moments;
+        struct Arr {
+            const double* p;
+            size_t count;
+            const char* name;
+        } arrs[] = {{pb->density, (size_t)n, "density"},
+                    {pb->e_trafo, (size_t)nE, "e_trafo"},
+                    {pb->stopping, (size_t)nE, "stopping"},
+                    {pb->bc_energy, (size_t)nE, "bc_energy"},
+                    {pb->sigma, (size_t)nE * (pb->npn + 1), "sigma"},
+                    {pb->bc_space, (size_t)n, "bc_space"},
+                    {pb->bc_angle, (size_t)q, "bc_angle"},
+                    {pb->omega, (size_t)q * 3, "omega"},
+                    {pb->m_reduced, (size_t)N * q, "m_reduced"}};
+        for (const Arr& a : arrs)
+            for (size_t i = 0; i < a.count; ++i)
+                if (!std::isfinite(a.p[i])) return fail(TITUS_ERR_ARG, "%s[%zu] is not finite", a.name, i);
+    }
     for (int d = 0; d < 4; ++d)
         if (!pb->op_rowptr[d] || (!pb->op_col[d] && pb->op_rowptr[d][pb->n_moments] > 0) ||
             (!pb->op_val[d] && pb->op_rowptr[d][pb->n_moments] > 0))
@@ -74,28 +107,24 @@ static int validate(const titus_problem_t* pb) {
         if (rp[0] != 0) return fail(TITUS_ERR_ARG, "operator %d rowptr[0] != 0", d);
         for (int m = 0; m < pb->n_moments; ++m)
             if (rp[m + 1] < rp[m]) return fail(TITUS_ERR_ARG, "operator %d rowptr not monotone", d);
-        for (int p = 0; p < rp[pb->n_moments]; ++p)
+        for (int p = 0; p < rp[pb->n_moments]; ++p) {
             if (pb->op_col[d][p] < 0 || pb->op_col[d][p] >= pb->n_moments)
                 return fail(TITUS_ERR_ARG, "operator %d column index out of range", d);
+            if (!std::isfinite(pb->op_val[d][p])) return fail(TITUS_ERR_ARG, "operator %d value %d is not finite", d, p);
+        }
     }
     return TITUS_OK;
 }
 
-extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
-    if (!out) return fail(TITUS_ERR_ARG, "out is NULL");
-    *out = nullptr;
-    int rc = validate(pb);
-    if (rc) return rc;
-    auto* s = new titus_solver();
-    auto cleanup = [&](int code) {
-        delete s;
-        return code;
-    };
+// Uploads the problem into `s`; on any failure the caller deletes `s`, which
+// releases every allocation made so far.
+static int create_impl(const titus_problem_t* pb, titus_solver* s) {
+    int rc;
     CK(cudaGetDevice(&s->device));
     CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
     int coop = 0;
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device));
-    if (!coop) return cleanup(fail(TITUS_ERR_CUDA, "device does not support cooperative launch"));
+    if (!coop) return fail(TITUS_ERR_CUDA, "device does not support cooperative launch");
     const int n = pb->nx * pb->ny, N = pb->n_moments, q = pb->n_ordinates, nE = pb->n_energies;
     s->n = n;
     s->N = N;
@@ -145,7 +174,7 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
         (rc = s->alloc(&d_res, n, restore.data())) ||
         (rc = s->alloc(&d_xc, pb->n_x_completion, pb->x_completion)) ||
         (rc = s->alloc(&d_wc, pb->n_w_completion, pb->w_completion)))
-        return cleanup(rc);
+        return rc;
     P.rinv = d_rinv;
     P.stopping = d_stop;
     P.bc_energy = d_bce;
@@ -167,7 +196,7 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
         double* v = nullptr;
         if ((rc = s->alloc(&rp, N + 1, pb->op_rowptr[d])) || (rc = s->alloc(&ci, nnz, pb->op_col[d])) ||
             (rc = s->alloc(&v, nnz, pb->op_val[d])))
-            return cleanup(rc);
+            return rc;
         P.op[d].rowptr = rp;
         P.op[d].col = ci;
         P.op[d].val = v;
@@ -185,17 +214,30 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
         (rc = s->alloc(&st.red, PMAX)) ||
         (rc = s->alloc(&bar, s->num_sms + 1)) || (rc = s->alloc(&st.status, 1)) || (rc = s->alloc(&info, 4)) ||
         (rc = s->alloc(&st.rank_hist, nE)) || (rc = s->alloc(&st.diag, 16)))
-        return cleanup(rc);
+        return rc;
     st.bar = bar;
     st.info = info;
     st.eta_hist = st.bound_hist = st.time_hist = nullptr;
-    if ((rc = s->alloc(&s->d_st, 1))) return cleanup(rc);
-    if ((rc = s->alloc(&s->prof, PF_SLOTS))) return cleanup(rc);
+    if ((rc = s->alloc(&s->d_st, 1))) return rc;
+    if ((rc = s->alloc(&s->prof, PF_SLOTS))) return rc;
     CK(cudaMemset(s->prof, 0, PF_SLOTS * sizeof(unsigned long long)));
     CK(cudaDeviceGetAttribute(&s->clock_khz, cudaDevAttrClockRate, s->device));
     CK(cudaMemcpy(s->d_st, &st, sizeof(TeamState), cudaMemcpyHostToDevice));
     CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sizeof(SmemLayout)));
+    return TITUS_OK;
+}
+
+extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
+    if (!out) return fail(TITUS_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = validate(pb);
+    if (rc) return rc;
+    auto* s = new titus_solver();
+    if ((rc = create_impl(pb, s))) {
+        delete s;
+        return rc;
+    }
     *out = s;
     return TITUS_OK;
 }
@@ -252,6 +294,7 @@ static int launch(titus_solver* s, int method, const titus_options_t* opt, int n
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
     P.prof = nullptr;
     P.zero_smem = getenv("TITUS_ZERO_SMEM") ? 1 : 0;
+    s->take_debug_hooks(P);
     if (opt && opt->profile) {
         CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));
         P.prof = s->prof;
@@ -282,8 +325,9 @@ static int check_status(titus_solver* s) {
         if (status == ST_BARRIER_TIMEOUT) {
             unsigned counter = 0;
             CK(cudaMemcpy(&counter, s->st.bar + s->last_G, sizeof(unsigned), cudaMemcpyDeviceToHost));
-            return fail(TITUS_ERR_DEVICE, "device status %d: %s (CTA %g saw %g arrivals, wanted %g; counter now %u)",
-                        status, what, d[8], d[9], d[10], counter);
+            return fail(TITUS_ERR_DEVICE,
+                        "device status %d: %s (CTA %g at barrier %g saw %g arrivals, wanted %g; counter now %u)",
+                        status, what, d[8], d[14], d[9], d[10], counter);
         }
         if (status == ST_CHOL_BREAKDOWN)
             return fail(TITUS_ERR_DEVICE,
@@ -447,6 +491,39 @@ extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
     for (int i = 0; i < PF_COUNT && m < n; ++i, ++m) ns[m] = (double)cyc[i] * 1e6 / (double)s->clock_khz;
     for (int i = 0; i < nc && m < n; ++i, ++m) ns[m] = (double)cyc[counters[i]];
     return m;
+}
+
+extern "C" int titus_resume_point(titus_solver_t* s, int32_t* n_next, double* t) {
+    if (!s || !n_next) return fail(TITUS_ERR_ARG, "NULL argument");
+    CK(cudaDeviceSynchronize());
+    if (s->last_method == TITUS_PARALLEL_ADAPTIVE || s->last_method == TITUS_BUG_ADAPTIVE ||
+        (s->last_method < 0 && s->wide_state_valid)) {
+        if (!s->d_wst) return fail(TITUS_ERR_ARG, "no solver state yet");
+        int info[8];
+        CK(cudaMemcpy(info, s->wst.info, sizeof(info), cudaMemcpyDeviceToHost));
+        *n_next = info[3];
+        if (t) CK(cudaMemcpy(t, s->wst.tvar, sizeof(double), cudaMemcpyDeviceToHost));
+        return TITUS_OK;
+    }
+    int info[4];
+    CK(cudaMemcpy(info, s->st.info, sizeof(info), cudaMemcpyDeviceToHost));
+    *n_next = info[3];
+    if (t) *t = (info[3] - 2) * s->P.dE;
+    return TITUS_OK;
+}
+
+extern "C" int titus_debug_barrier_fault(titus_solver_t* s, int32_t barrier, int64_t spin_limit) {
+    if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (spin_limit < 0) return fail(TITUS_ERR_ARG, "spin_limit < 0");
+    s->dbg_fault_barrier = barrier > 0 ? barrier : 0;
+    s->dbg_spin_limit = spin_limit;
+    return TITUS_OK;
+}
+
+extern "C" int titus_debug_fail_alloc(int32_t after) {
+    if (after < 0) return fail(TITUS_ERR_ARG, "after < 0");
+    g_alloc_fault.store(after);
+    return TITUS_OK;
 }
 
 extern "C" int titus_max_rank(void) { return 2 * wide::RA; }

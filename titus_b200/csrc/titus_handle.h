@@ -20,10 +20,17 @@ int fail(int code, const char* fmt, ...);
         if (e_ != cudaSuccess) return titus_host::fail(TITUS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// Test hook (titus_debug_fail_alloc): when positive, the allocation that
+// brings it to zero fails as if cudaMalloc had returned cudaErrorMemoryAllocation.
+int take_alloc_fault();
+
 template <class T>
 int upload(T** dptr, const T* host, size_t count) {
     *dptr = nullptr;
     if (count == 0) return TITUS_OK;
+    if (take_alloc_fault())
+        return fail(TITUS_ERR_CUDA, "cudaMalloc(%zu bytes): %s (injected)", count * sizeof(T),
+                    cudaGetErrorString(cudaErrorMemoryAllocation));
     CK(cudaMalloc((void**)dptr, count * sizeof(T)));
     if (host) CK(cudaMemcpy(*dptr, host, count * sizeof(T), cudaMemcpyHostToDevice));
     return TITUS_OK;
@@ -66,6 +73,15 @@ struct titus_solver {
     int b_teams = 0, b_G = 0;
     std::vector<void*> batch_allocs;
     int wide_state_valid = 0;   // 1 after an adaptive solve or titus_set_state
+    // test hook (titus_debug_barrier_fault), consumed by the next launch
+    long long dbg_spin_limit = 0;
+    int dbg_fault_barrier = 0;
+    void take_debug_hooks(titus::DevProblem& P) {
+        P.spin_limit = dbg_spin_limit;
+        P.fault_barrier = dbg_fault_barrier;
+        dbg_spin_limit = 0;
+        dbg_fault_barrier = 0;
+    }
 
     template <class T>
     int alloc(T** p, size_t count, const T* host = nullptr) {

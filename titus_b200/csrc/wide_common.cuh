@@ -143,7 +143,7 @@ __device__ __forceinline__ bool is_bnd_w(const DevProblem& P, int c) {
 __device__ __forceinline__ bool wsync(WCtx& x) {
     ProfScope ps(x.prof, PF_BARRIER);
     prof_count(x.prof, PF_BARRIERS, 1ull);
-    return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag);
+    return team_sync(x.st.bar, x.st.status, x.G, x.b, x.gen, x.st.diag, x.P.spin_limit, x.P.fault_barrier);
 }
 
 __device__ __forceinline__ double* wpart(const WCtx& x, int g) {
@@ -166,6 +166,13 @@ template <class Hook>
 __device__ inline bool wreduce(WCtx& x, int count, Hook hook) {
     if (!wsync(x)) return false;
     hook();
+    if (x.G == 1) {
+        // one CTA: its partial is the sum; read it in place (the partial of
+        // this parity is next written two reductions later, like `red`)
+        x.redp = wpart(x, 0);
+        x.parity ^= 1;
+        return wsync(x);
+    }
     {
         ProfScope ps(x.prof, PF_REDUCE);
         // CTA b sums the slice [e0, e1) over the G partials. Blocks of RCH

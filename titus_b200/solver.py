@@ -240,10 +240,20 @@ class SolverCSD:
         opt = self.options(max_steps, rank_tol, profile)
         _lib.check(lib.titus_solve(h, method, C.byref(opt), C.byref(res)), "titus_solve")
         k = res.rank
+        n_next, t = self.resume_point()
         return dict(X=bufs["X"][:, :k], S=bufs["S"][:k, :k], W=bufs["W"][:, :k], dose=bufs["dose"],
                     psi=bufs["psi"], rank=k, steps=res.steps_done, rank_history=bufs["rank_history"],
                     time_history=bufs["time_history"], eta_history=bufs["eta_history"],
-                    bound_history=bufs["bound_history"])
+                    bound_history=bufs["bound_history"], n_next=n_next, t=t)
+
+    def resume_point(self):
+        """(n_next, t): the energy index the loop would process next and the
+        pseudo-time after the last solve (titus_resume_point)."""
+        nn = np.zeros(1, dtype=np.int32)
+        t = np.zeros(1)
+        _lib.check(_lib.load().titus_resume_point(self.handle(), _lib.as_ip(nn), _lib.as_dp(t)),
+                   "titus_resume_point")
+        return int(nn[0]), float(t[0])
 
     def run_from(self, method: int, state: dict, n_next: int, n_stop: int, rank_tol: float = 0.0, max_steps: int = 0):
         """Resume the loop from a given state (checkpoint restart)."""
@@ -262,8 +272,11 @@ class SolverCSD:
         opt = self.options(max_steps, rank_tol)
         _lib.check(lib.titus_solve_from(h, method, C.byref(opt), n_stop, C.byref(res)), "titus_solve_from")
         kk = res.rank
+        n_next, t = self.resume_point()
         return dict(X=bufs["X"][:, :kk], S=bufs["S"][:kk, :kk], W=bufs["W"][:, :kk], dose=bufs["dose"],
-                    psi=bufs["psi"], rank=kk, steps=res.steps_done, rank_history=bufs["rank_history"])
+                    psi=bufs["psi"], rank=kk, steps=res.steps_done, rank_history=bufs["rank_history"],
+                    time_history=bufs["time_history"], eta_history=bufs["eta_history"],
+                    bound_history=bufs["bound_history"], n_next=n_next, t=t)
 
     def outputs(self, out):
         """The reference's return tuple from raw factors (``SolverCSD.jl:1116-1118``)."""
