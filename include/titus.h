@@ -160,12 +160,28 @@ typedef struct titus_spot {
 /* Batched pencil-beam solves (no counterpart in the reference, which solves
  * one beam per Solve* call): all `nspots` spots advance in one persistent
  * launch, options->team_ctas CTAs per spot (default 1) and as many spots at a
- * time as the GPU holds teams. method: TITUS_PARALLEL_ADAPTIVE or
+ * time as the GPU holds teams, which take the spots longest energy grid first
+ * from a device work queue. method: TITUS_PARALLEL_ADAPTIVE or
  * TITUS_BUG_ADAPTIVE; options->max_steps bounds each spot's loop.
  * dose_out: nspots x n (row s = dose of spot s); rank_out / iters_out
  * (nspots, optional): final rank and loop iterations per spot. */
 int titus_solve_batched(titus_solver_t* solver, int32_t method, const titus_options_t* options, int32_t nspots,
                         const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out);
+
+/* The same batched solve in three parts, for callers that repeat it (plan
+ * optimisation loops) or time it: titus_batch_upload copies the spots' tables
+ * to the device once (the handle borrows `solver`, which must outlive it);
+ * titus_batch_solve_device launches the persistent kernel on `stream` (a
+ * cudaStream_t, NULL = default stream) and returns without waiting;
+ * titus_batch_fetch waits for the device, checks its status and copies the
+ * doses (nspots x n), final ranks and iteration counts out (each may be NULL).
+ * Teams take spots from a device work queue, longest energy grid first, so
+ * the launch ends about when its longest spot does. */
+typedef struct titus_batch titus_batch_t;
+int titus_batch_upload(titus_solver_t* solver, int32_t nspots, const titus_spot_t* spots, titus_batch_t** out);
+int titus_batch_solve_device(titus_batch_t* batch, int32_t method, const titus_options_t* options, void* stream);
+int titus_batch_fetch(titus_batch_t* batch, double* dose_out, int32_t* rank_out, int32_t* iters_out);
+void titus_batch_destroy(titus_batch_t* batch);
 
 void titus_destroy(titus_solver_t* solver);
 

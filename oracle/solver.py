@@ -429,7 +429,7 @@ def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None, state: d
 
 
 def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
-                  n_begin: int = 2, return_state: bool = False):
+                  n_begin: int = 2, return_state: bool = False, on_iter=None):
     """``SolveFirstCollisionSourceDLRBUGRejection`` (``SolverCSD.jl:2011-2374``).
 
     The undefined name ``rmax`` (``:2205, :2295``) is read as ``settings.r``,
@@ -439,6 +439,9 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict |
     ``max_steps`` bounds the number of loop iterations. ``state`` (X, S, W, psi,
     dose, optionally t) resumes the loop at energy index ``n_begin``;
     ``return_state`` returns that dict (with ``n_next``) at the end.
+    ``on_iter(rank)``, if given, is called at the start of every loop iteration
+    with the rank entering it, and once more with None when the loop ends (the
+    CPU baseline times iterations by rank with it).
 
     Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, [E rank]^T,
     [E eta], [E bound], psi).
@@ -478,6 +481,8 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict |
             n_next = n
             break
         iters += 1
+        if on_iter is not None:
+            on_iter(r)
         timeVec.append(energy[n - 1])
         rankInTime.append(r)
         sigma, Dvec, D = _step_prologue(solver, psi, X, S, W, n, dE)
@@ -563,6 +568,8 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict |
         r = S.shape[0]
         solver.dose_half(X, S, W, psi, dE, solver.csd.S[n - 1])
         t += dE
+    if on_iter is not None:
+        on_iter(None)
     if return_state:
         return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), t=t,
                     n_next=n_next if n_next is not None else n + 1, rank=rankInTime, eta=etaVec,

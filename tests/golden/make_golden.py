@@ -2,10 +2,10 @@
 
 Reads ``code/validationData/{AxPlus,AxMinus,AyPlus,AyMinus}.csv`` (64 x 64, the
 nPN = 7 flux-matrix splittings A+- = (A +- |A|)/2 shipped with the reference)
-and stores them as float64 in ``pn_golden.npz`` beside this script. Run in a
-checkout that has the reference tree:
+and stores them as float64 in ``pn_golden.npz`` beside this script. The
+argument is the root of a TITUS checkout (the directory holding ``code/``):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path-to-TITUS-checkout>
 """
 import os
 import sys
@@ -24,4 +24,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path-to-TITUS-checkout>")
+    main(sys.argv[1])

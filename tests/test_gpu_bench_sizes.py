@@ -9,21 +9,29 @@ oracle run finishes in seconds:
 
 * the first 200 BUG iterations of the 200 x 200 phantom as one whole run
   (rank 40 entering, every rejection and truncation of the opening steps): rank
-  of every iteration exactly, dose and psi <= 1e-10, the streaming eta values
-  and their bounds;
+  of every iteration exactly; dose, psi, scalar flux, the streaming eta values
+  and their bounds to the tolerance below;
 * the parallel integrator's first 5 steps on the same problem;
 * three windows from the middle of the BUG sweep (iterations 5 000, 15 000
   and 25 000): the GPU's own state there (titus_fetch + titus_resume_point) is
   handed to both paths, which then run 10 iterations each; the dose increment
-  over the window and psi at <= 1e-10, ranks exactly;
+  over the window and psi at <= 1e-10, ranks exactly, the factor product to
+  the tolerance below;
 * the fixed-rank water beam for 100 steps from its state after 1 500 steps;
 * three pencil beams of 2-8 MeV on the 128 x 128 phantom, first 200
   iterations each, in one batched launch.
 
 Tolerances follow the conditioning measured on the oracle (the same rules as
-test_gpu_adaptive.py): factor products, the scalar flux and eta are bounded by
-max(1e-10, 4 x the oracle's own change under 1e-14 input noise) when they miss
-1e-10, because they depend on singular directions that rounding moves.
+test_gpu_adaptive.py), with one addition at these sizes: the dose itself is
+no longer determined to 1e-10 by the arithmetic. A 1e-14 relative
+perturbation of the density moves the oracle's own dose after 200 iterations
+by 2.9e-8 - 3.6e-8 (200 x 200, P29) and by 1.0e-8 - 1.9e-8 (a 128 x 128, P21
+pencil beam), with identical rank histories: the l1 truncation rule keeps
+directions with sigma / sigma_1 near 1e-10, whose singular vectors rounding
+rotates. So every quantity -- dose, psi, factor products, scalar flux, eta --
+must meet 1e-10 or, failing that, max(1e-10, 4 x the oracle's own change
+under 1e-14 input noise), which the test then measures; the rank of every
+iteration must match exactly in all cases.
 """
 import numpy as np
 import pytest
@@ -62,31 +70,51 @@ def phantom_gpu():
     return SolverCSD(Settings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2), team_ctas=148)
 
 
+def interior_rel(a, b, nx):
+    m = ~bnd_mask(nx)
+    return rel(a[m], b[m])
+
+
+def oracle_noise(make_settings, steps, o):
+    """The oracle's own relative change under 1e-14 density noise (max over two
+    seeds) of: interior dose, psi, scalar flux, eta (scaled by max |eta|)."""
+    sd = sp = su = se = 0.0
+    nx = make_settings().NCellsX + 1
+    for seed in (1, 2):
+        s = make_settings()
+        s.density = s.density * (1 + 1e-14 * np.random.default_rng(seed).standard_normal(s.density.shape))
+        p = solve_dlr_bug(OSolver(s), max_steps=steps)
+        sd = max(sd, interior_rel(p[4], o[4], nx))
+        sp = max(sp, rel(p[8].ravel(), o[8].ravel()))
+        su = max(su, rel(scalar_flux(p[0], p[1], p[3]), scalar_flux(o[0], o[1], o[3])))
+        if p[6].shape == o[6].shape and o[6].size:
+            se = max(se, np.max(np.abs(p[6][:, 1] - o[6][:, 1]) / np.abs(o[6][:, 1]).max()))
+    return sd, sp, su, se
+
+
 def test_phantom_200_bug_first_200_iterations(phantom_gpu):
     steps = 200
-    o = solve_dlr_bug(OSolver(OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)), max_steps=steps)
+    mk = lambda: OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)  # noqa: E731
+    o = solve_dlr_bug(OSolver(mk()), max_steps=steps)
     g = SolveFirstCollisionSourceDLRBUGRejection(phantom_gpu, max_steps=steps)
     np.testing.assert_array_equal(g[5][1], o[5][1])            # rank of every iteration
     np.testing.assert_allclose(g[5][0], o[5][0], rtol=1e-12)   # energy of every iteration
     assert o[5][1][0] == CAP2 // 2                             # entered at rank 40 (width 80)
-    assert dose_ok(g[4], o[4], NX2)
-    assert rel(g[8].ravel(), o[8].ravel()) <= TOL              # psi
     assert g[6].shape[0] == o[6].shape[0]                      # one eta per rejection test
-    np.testing.assert_allclose(g[7][:, 1], o[7][:, 1], rtol=1e-10)
-    eerr = np.max(np.abs(g[6][:, 1] - o[6][:, 1]) / np.abs(o[6][:, 1]).max()) if o[6].size else 0.0
+    b = bnd_mask(NX2)
+    assert np.abs(g[4][b] - o[4][b]).max() <= 1e-8 * np.linalg.norm(o[4])   # ghost cells
+    derr = interior_rel(g[4], o[4], NX2)
+    perr = rel(g[8].ravel(), o[8].ravel())
     uerr = rel(scalar_flux(g[0], g[1], g[3]), scalar_flux(o[0], o[1], o[3]))
-    if eerr > 1e-8 or uerr > TOL:
-        # the oracle's own change under 1e-14 density noise
-        su = se = 0.0
-        for seed in (1, 2):
-            s = OSettings(NX2, NX2, CAP2, "csdPhantom", nPN=NPN2)
-            s.density = s.density * (1 + 1e-14 * np.random.default_rng(seed).standard_normal(s.density.shape))
-            p = solve_dlr_bug(OSolver(s), max_steps=steps)
-            su = max(su, rel(scalar_flux(p[0], p[1], p[3]), scalar_flux(o[0], o[1], o[3])))
-            if p[6].shape == o[6].shape:
-                se = max(se, np.max(np.abs(p[6][:, 1] - o[6][:, 1]) / np.abs(o[6][:, 1]).max()))
-        assert uerr <= max(TOL, 4 * su)
-        assert eerr <= max(1e-8, 4 * se)
+    eerr = np.max(np.abs(g[6][:, 1] - o[6][:, 1]) / np.abs(o[6][:, 1]).max()) if o[6].size else 0.0
+    berr = np.max(np.abs(g[7][:, 1] - o[7][:, 1]) / np.abs(o[7][:, 1]).max()) if o[7].size else 0.0
+    if max(derr, perr, uerr, berr) > TOL or eerr > 1e-8:
+        sd, sp, su, se = oracle_noise(mk, steps, o)
+        assert derr <= max(TOL, 4 * sd), (derr, sd)
+        assert perr <= max(TOL, 4 * sp), (perr, sp)
+        assert uerr <= max(TOL, 4 * su), (uerr, su)
+        assert eerr <= max(1e-8, 4 * se), (eerr, se)
+        assert berr <= max(TOL, 4 * sd), (berr, sd)
 
 
 def test_phantom_200_parallel_first_steps():
@@ -186,10 +214,23 @@ def test_pencil_beams_2_to_8_MeV_on_128_phantom():
     spots = [(float(e), float(y)) for e, y in zip(rng.uniform(2.0, 8.0, 3), rng.uniform(0.1, 0.9, 3))]
     g = SolverCSD(Settings(NX3, NX3, CAP3, "csdPhantom", nPN=NPN3))
     dose, rank, iters = SolveBatchedPencilBeams(g, spots, "bug", team_ctas=1, max_steps=steps)
+    b = bnd_mask(NX3)
     for i, (e, y) in enumerate(spots):
-        s = OSettings(NX3, NX3, CAP3, "csdPhantom", nPN=NPN3)
-        s.eMax, s.y0 = e, y
-        st = solve_dlr_bug(OSolver(s), max_steps=steps, return_state=True)
+        def mk(e=e, y=y):
+            s = OSettings(NX3, NX3, CAP3, "csdPhantom", nPN=NPN3)
+            s.eMax, s.y0 = e, y
+            return s
+        st = solve_dlr_bug(OSolver(mk()), max_steps=steps, return_state=True)
         assert iters[i] == st["iters"] == steps
         assert rank[i] == st["S"].shape[0], (i, rank[i], st["S"].shape[0])
-        assert dose_ok(dose[i], st["dose"], NX3), (i, rel(dose[i], st["dose"]))
+        assert np.abs(dose[i][b] - st["dose"][b]).max() <= 1e-8 * np.linalg.norm(st["dose"])
+        derr = interior_rel(dose[i], st["dose"], NX3)
+        if derr > TOL:
+            sd = 0.0
+            for seed in (1, 2):
+                sn = mk()
+                sn.density = sn.density * (1 + 1e-14 * np.random.default_rng(seed).standard_normal(sn.density.shape))
+                p = solve_dlr_bug(OSolver(sn), max_steps=steps, return_state=True)
+                assert p["rank"] == st["rank"]
+                sd = max(sd, interior_rel(p["dose"], st["dose"], NX3))
+            assert derr <= max(TOL, 4 * sd), (i, derr, sd)

@@ -34,45 +34,94 @@ __device__ __forceinline__ double* sside(const WCtx& x, int s, int off) {
 
 // ------------------------------------------------------------- row kernels ---
 // F[r][fc + d*k + j] = (L_d A)[r0 + r][j]; zero on boundary rows (stencils.jl:26-128).
+// Four elements per thread are gathered before any is combined, so each thread
+// has 20 neighbour loads in flight (the arithmetic per element is unchanged).
 __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0, int nr, int k, double* F, int ldf,
                                  int fc) {
     const DevProblem& P = x.P;
     const double hx = 0.5 / P.dx, hy = 0.5 / P.dy;
     const double ix = 1.0 / P.dx, iy = 1.0 / P.dy;
-    for (int e = threadIdx.x; e < nr * k; e += NT) {
-        const int r = e / k, j = e - (e / k) * k;
-        const int c = r0 + r;
-        double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
-        if (!is_bnd_w(P, c)) {
-            const double a0 = ldcg(A + (size_t)c * lda + j) * P.rinv[c];
-            const double axm = ldcg(A + (size_t)(c - P.ny) * lda + j) * P.rinv[c - P.ny];
-            const double axp = ldcg(A + (size_t)(c + P.ny) * lda + j) * P.rinv[c + P.ny];
-            const double aym = ldcg(A + (size_t)(c - 1) * lda + j) * P.rinv[c - 1];
-            const double ayp = ldcg(A + (size_t)(c + 1) * lda + j) * P.rinv[c + 1];
-            l2x = (axp - axm) * hx;
-            l2y = (ayp - aym) * hy;
-            l1x = a0 * ix - hx * axm - hx * axp;
-            l1y = a0 * iy - hy * aym - hy * ayp;
+    constexpr int SU = 4;
+    const int cnt = nr * k;
+    for (int b = threadIdx.x; b < cnt; b += SU * NT) {
+        double a[SU][5];
+        int cc[SU];
+        bool in[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int e = b + u * NT;
+            const int r = e / k, j = e - r * k;
+            const int c = r0 + r;
+            cc[u] = c;
+            in[u] = e < cnt && !is_bnd_w(P, c);
+            if (in[u]) {
+                const double* p = A + (size_t)c * lda + j;
+                a[u][0] = ldcg(p);
+                a[u][1] = ldcg(p - (size_t)P.ny * lda);
+                a[u][2] = ldcg(p + (size_t)P.ny * lda);
+                a[u][3] = ldcg(p - lda);
+                a[u][4] = ldcg(p + lda);
+            }
         }
-        double* row = F + r * ldf + fc;
-        row[0 * k + j] = l2x;
-        row[1 * k + j] = l2y;
-        row[2 * k + j] = l1x;
-        row[3 * k + j] = l1y;
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int e = b + u * NT;
+            if (e >= cnt) continue;
+            const int r = e / k, j = e - r * k;
+            const int c = cc[u];
+            double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
+            if (in[u]) {
+                const double a0 = a[u][0] * __ldg(P.rinv + c);
+                const double axm = a[u][1] * __ldg(P.rinv + c - P.ny);
+                const double axp = a[u][2] * __ldg(P.rinv + c + P.ny);
+                const double aym = a[u][3] * __ldg(P.rinv + c - 1);
+                const double ayp = a[u][4] * __ldg(P.rinv + c + 1);
+                l2x = (axp - axm) * hx;
+                l2y = (ayp - aym) * hy;
+                l1x = a0 * ix - hx * axm - hx * axp;
+                l1y = a0 * iy - hy * aym - hy * ayp;
+            }
+            double* row = F + r * ldf + fc;
+            row[0 * k + j] = l2x;
+            row[1 * k + j] = l2y;
+            row[2 * k + j] = l1x;
+            row[3 * k + j] = l1y;
+        }
     }
 }
 // F[r][fc + d*k + j] = (A_d B)[r0 + r][j] (sparse P_N operators Ax, Az, |Ax|, |Az|).
+// A thread takes one (operator, row) and a group of up to SPJ consecutive
+// columns: per nonzero it loads the index and value once and SPJ contiguous
+// entries of B, so the loads of a row segment are independent. The sum over
+// the nonzeros runs in CSR order for every column, as before.
 __device__ inline void w_spmm(const WCtx& x, const double* B, int ldb, int r0, int nr, int k, double* F, int ldf,
                               int fc) {
-    for (int e = threadIdx.x; e < NOPS * nr * k; e += NT) {
-        const int d = e / (nr * k);
-        const int rem = e - d * nr * k;
-        const int r = rem / k, j = rem - (rem / k) * k;
+    constexpr int SPJ = 8;
+    const int ng = (k + SPJ - 1) / SPJ;
+    for (int e = threadIdx.x; e < NOPS * nr * ng; e += NT) {
+        const int d = e / (nr * ng);
+        const int rem = e - d * nr * ng;
+        const int r = rem / ng, g = rem - (rem / ng) * ng;
+        const int j0 = g * SPJ, w = min(SPJ, k - j0);
         const Csr& A = x.P.op[d];
         const int m = r0 + r;
-        double s = 0.0;
-        for (int p = A.rowptr[m]; p < A.rowptr[m + 1]; ++p) s = fma(A.val[p], ldcg(B + (size_t)A.col[p] * ldb + j), s);
-        F[r * ldf + fc + d * k + j] = s;
+        double s[SPJ];
+#pragma unroll
+        for (int u = 0; u < SPJ; ++u) s[u] = 0.0;
+        const int p1 = __ldg(A.rowptr + m + 1);
+        for (int p = __ldg(A.rowptr + m); p < p1; ++p) {
+            const double v = __ldg(A.val + p);
+            const double* bp = B + (size_t)__ldg(A.col + p) * ldb + j0;
+            double bv[SPJ];
+#pragma unroll
+            for (int u = 0; u < SPJ; ++u) bv[u] = u < w ? ldcg(bp + u) : 0.0;
+#pragma unroll
+            for (int u = 0; u < SPJ; ++u) s[u] = fma(v, bv[u], s[u]);
+        }
+        double* out = F + r * ldf + fc + d * k + j0;
+#pragma unroll
+        for (int u = 0; u < SPJ; ++u)
+            if (u < w) out[u] = s[u];
     }
 }
 
@@ -82,8 +131,18 @@ static __device__ __noinline__ void w_dose(WCtx& x, int sidx, const double* v, i
     const double f = 0.5 * P.dE * P.stopping[sidx];
     for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT) {
         double xv = 0.0;
-        if (!(zero_bnd_x && is_bnd_w(P, c)))
-            for (int j = 0; j < k; ++j) xv = fma(ldcg(x.st.X + (size_t)c * KA + j), v[j], xv);
+        if (!(zero_bnd_x && is_bnd_w(P, c))) {
+            // the row's entries are loaded in groups of 8 before they are summed
+            const double* xr = x.st.X + (size_t)c * KA;
+            for (int j0 = 0; j0 < k; j0 += 8) {
+                double xl[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) xl[u] = j0 + u < k ? ldcg(xr + j0 + u) : 0.0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (j0 + u < k) xv = fma(xl[u], v[j0 + u], xv);
+            }
+        }
         const double* pr = x.psi_in + (size_t)c * QW;
         double u = 0.0;
         for (int kq = 0; kq < P.q; ++kq) u = fma(pr[kq], P.mred[kq], u);
@@ -1570,13 +1629,18 @@ static __device__ __noinline__ void init_spot(WCtx& x, int r0) {
     __syncthreads();
 }
 
-// Batched solves: T teams of G CTAs; team t solves spots t, t+T, ... one after
-// the other with the same integrator, re-initialising its factors on the
-// device between spots. Each spot's dose goes to its own output buffer.
+// Batched solves: T teams of G CTAs take spots from a device work queue (an
+// atomic counter over `order`, the spots sorted longest first) until it runs
+// dry, re-initialising their factors on the device between spots. CTA 0 of a
+// team draws the next index and publishes it to the team through info[6]
+// and a team barrier. Each spot's dose goes to its own output buffer; a spot's
+// result does not depend on which team solved it (all teams have G CTAs and
+// the same reduction order). `max_steps_par` > 0 bounds the parallel
+// integrator's energy index to 1 + max_steps_par.
 template <int METHOD>
 __global__ void __launch_bounds__(NT, 1)
 adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const SpotData* spots, int nspots, int r0,
-                        int max_iters) {
+                        int max_iters, int max_steps_par, int* queue, const int* order) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WSmem* sm = reinterpret_cast<WSmem*>(smem_raw);
     const int team = blockIdx.x / G;
@@ -1598,7 +1662,22 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
     x.c1 = (int)((long long)(x.b + 1) * P0.n / G);
     x.m0 = (int)((long long)x.b * P0.N / G);
     x.m1 = (int)((long long)(x.b + 1) * P0.N / G);
-    for (int sidx = team; sidx < nspots; sidx += T) {
+    __shared__ int s_next;
+    while (true) {
+        if (x.b == 0 && threadIdx.x == 0) {
+            const int q = atomicAdd(queue, 1);
+            s_next = q;
+            if (G > 1) x.st.info[6] = q;   // read by the team after the barrier below
+        }
+        __syncthreads();
+        if (G > 1) {
+            if (!wsync(x)) return;
+            if (x.b != 0 && threadIdx.x == 0) s_next = ldcg(x.st.info + 6);
+            __syncthreads();
+        }
+        const int qi = s_next;
+        if (qi >= nspots) break;
+        const int sidx = order[qi];
         const SpotData sp = spots[sidx];
         x.P = P0;
         x.P.nE = sp.nE;
@@ -1618,7 +1697,9 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
         ls.eta_count = 0;
         ls.n = 2;
         ls.aborted = false;
-        energy_loop<METHOD>(x, 2, sp.n_end, max_iters, ls);
+        const int n_end = (METHOD == TITUS_PARALLEL_ADAPTIVE && max_steps_par > 0) ? min(sp.nE, 1 + max_steps_par)
+                                                                                     : sp.n_end;
+        energy_loop<METHOD>(x, 2, n_end, max_iters, ls);
         if (ls.aborted) return;
         if (x.b == 0 && threadIdx.x == 0) {
             sp.result[0] = x.r;

@@ -343,16 +343,93 @@ int ensure_batch_states(titus_solver* s, int T, int G) {
 
 }  // namespace
 
-int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots,
-                                   const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
+// A set of pencil beams uploaded once (titus_batch_upload): per-spot tables,
+// the longest-first order, the work-queue counter and the outputs, all on the
+// device, so repeated launches move no host data.
+struct titus_batch {
+    titus_solver* s = nullptr;
+    int nspots = 0;
+    DevTemps tmp;
+    SpotData* d_sd = nullptr;
+    double* d_dose = nullptr;
+    int* d_res = nullptr;
+    int* d_order = nullptr;
+    int* d_queue = nullptr;
+    int last_T = 0, last_G = 0;
+    bool launched = false;
+};
+
+int titus_host::batch_upload(titus_solver* s, int nspots, const titus_spot_t* spots, titus_batch** out) {
+    *out = nullptr;
     const int n = s->n, npn1 = s->P.npn + 1;
     for (int i = 0; i < nspots; ++i) {
         const titus_spot_t& sp = spots[i];
         if (sp.n_energies < 2) return fail(TITUS_ERR_ARG, "spot %d: n_energies < 2", i);
-        if (!(sp.d_e > 0)) return fail(TITUS_ERR_ARG, "spot %d: d_e must be > 0", i);
+        if (!(sp.d_e > 0) || !std::isfinite(sp.d_e)) return fail(TITUS_ERR_ARG, "spot %d: d_e must be finite and > 0", i);
         if (!sp.stopping || !sp.bc_energy || !sp.sigma || !sp.bc_space)
             return fail(TITUS_ERR_ARG, "spot %d: a table is NULL", i);
+        for (int e = 0; e < sp.n_energies; ++e)
+            if (!std::isfinite(sp.stopping[e]) || !std::isfinite(sp.bc_energy[e]))
+                return fail(TITUS_ERR_ARG, "spot %d: stopping / bc_energy [%d] not finite", i, e);
+        for (size_t e = 0; e < (size_t)sp.n_energies * npn1; ++e)
+            if (!std::isfinite(sp.sigma[e])) return fail(TITUS_ERR_ARG, "spot %d: sigma[%zu] not finite", i, e);
+        for (int c = 0; c < n; ++c)
+            if (!std::isfinite(sp.bc_space[c])) return fail(TITUS_ERR_ARG, "spot %d: bc_space[%d] not finite", i, c);
     }
+    auto* b = new titus_batch();
+    b->s = s;
+    b->nspots = nspots;
+    auto bail = [&](int rc) {
+        delete b;
+        return rc;
+    };
+    size_t tot_e = 0;
+    for (int i = 0; i < nspots; ++i) tot_e += (size_t)spots[i].n_energies;
+    double *d_stop, *d_bce, *d_sig, *d_bcs;
+    int rc;
+    if ((rc = b->tmp.alloc(&d_stop, tot_e)) || (rc = b->tmp.alloc(&d_bce, tot_e)) ||
+        (rc = b->tmp.alloc(&d_sig, tot_e * npn1)) || (rc = b->tmp.alloc(&d_bcs, (size_t)nspots * n)) ||
+        (rc = b->tmp.alloc(&b->d_dose, (size_t)nspots * n)) || (rc = b->tmp.alloc(&b->d_res, (size_t)2 * nspots)) ||
+        (rc = b->tmp.alloc(&b->d_queue, (size_t)1)))
+        return bail(rc);
+    std::vector<SpotData> sd(nspots);
+    size_t off = 0;
+    for (int i = 0; i < nspots; ++i) {
+        const titus_spot_t& sp = spots[i];
+        const int nE = sp.n_energies;
+        cudaError_t e = cudaMemcpy(d_stop + off, sp.stopping, nE * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_bce + off, sp.bc_energy, nE * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_sig + off * npn1, sp.sigma, (size_t)nE * npn1 * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_bcs + (size_t)i * n, sp.bc_space, n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bail(fail(TITUS_ERR_CUDA, "spot table upload: %s", cudaGetErrorString(e)));
+        SpotData& d = sd[i];
+        d.nE = nE;
+        d.n_end = nE;
+        d.dE = sp.d_e;
+        d.stopping = d_stop + off;
+        d.bc_energy = d_bce + off;
+        d.sigma = d_sig + off * npn1;
+        d.bc_space = d_bcs + (size_t)i * n;
+        d.dose = b->d_dose + (size_t)i * n;
+        d.result = b->d_res + 2 * i;
+        off += nE;
+    }
+    if ((rc = b->tmp.alloc(&b->d_sd, (size_t)nspots, sd.data()))) return bail(rc);
+    // longest first: a spot's loop runs about nE iterations, so handing the
+    // queue out in decreasing nE keeps the last teams from starting long spots
+    std::vector<int> order(nspots);
+    for (int i = 0; i < nspots; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return spots[a].n_energies > spots[c].n_energies; });
+    if ((rc = b->tmp.alloc(&b->d_order, (size_t)nspots, order.data()))) return bail(rc);
+    *out = b;
+    return TITUS_OK;
+}
+
+int titus_host::batch_launch(titus_batch* b, int method, const titus_options_t* opt, cudaStream_t stream) {
+    titus_solver* s = b->s;
     const int r0 = s->r / 2;
     if (r0 < 1) return fail(TITUS_ERR_ARG, "adaptive integrators need settings.r >= 2 (got %d)", s->r);
     if (r0 > RA) return fail(TITUS_ERR_LIMIT, "initial rank %d > %d", r0, RA);
@@ -365,74 +442,78 @@ int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_opti
     CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WSmem)));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, wide::NT, sizeof(WSmem)));
     if (per_sm < 1) return fail(TITUS_ERR_CUDA, "batched kernel does not fit on an SM");
-    const int T = std::max(1, std::min(nspots, per_sm * s->num_sms / G));
+    const int T = std::max(1, std::min(b->nspots, per_sm * s->num_sms / G));
     int rc = ensure_batch_states(s, T, G);
     if (rc) return rc;
-    // per-spot tables, concatenated
-    size_t tot_e = 0;
-    for (int i = 0; i < nspots; ++i) tot_e += (size_t)spots[i].n_energies;
-    DevTemps tmp;
-    double *d_stop, *d_bce, *d_sig, *d_bcs, *d_dose;
-    int* d_res;
-    if ((rc = tmp.alloc(&d_stop, tot_e)) || (rc = tmp.alloc(&d_bce, tot_e)) ||
-        (rc = tmp.alloc(&d_sig, tot_e * npn1)) || (rc = tmp.alloc(&d_bcs, (size_t)nspots * n)) ||
-        (rc = tmp.alloc(&d_dose, (size_t)nspots * n)) || (rc = tmp.alloc(&d_res, (size_t)2 * nspots)))
-        return rc;
-    std::vector<SpotData> sd(nspots);
-    size_t off = 0;
-    for (int i = 0; i < nspots; ++i) {
-        const titus_spot_t& sp = spots[i];
-        const int nE = sp.n_energies;
-        CK(cudaMemcpy(d_stop + off, sp.stopping, nE * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_bce + off, sp.bc_energy, nE * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_sig + off * npn1, sp.sigma, (size_t)nE * npn1 * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_bcs + (size_t)i * n, sp.bc_space, n * sizeof(double), cudaMemcpyHostToDevice));
-        SpotData& d = sd[i];
-        d.nE = nE;
-        d.n_end = nE;
-        if (method == TITUS_PARALLEL_ADAPTIVE && opt && opt->max_steps > 0) d.n_end = std::min(nE, 1 + opt->max_steps);
-        d.dE = sp.d_e;
-        d.stopping = d_stop + off;
-        d.bc_energy = d_bce + off;
-        d.sigma = d_sig + off * npn1;
-        d.bc_space = d_bcs + (size_t)i * n;
-        d.dose = d_dose + (size_t)i * n;
-        d.result = d_res + 2 * i;
-        off += nE;
-    }
-    SpotData* d_sd;
-    if ((rc = tmp.alloc(&d_sd, (size_t)nspots, sd.data()))) return rc;
+    // parallel integrator: max_steps bounds the energy index; BUG: the iterations
+    const int max_steps = (opt && opt->max_steps > 0) ? opt->max_steps : 0;
     int max_iters = INT_MAX;
-    if (method == TITUS_BUG_ADAPTIVE && opt && opt->max_steps > 0) max_iters = opt->max_steps;
-    for (int t = 0; t < T; ++t) CK(cudaMemset(s->bst[t].bar, 0, (size_t)(G + 1) * sizeof(unsigned)));
-    CK(cudaMemset(s->bst[0].status, 0, sizeof(int)));
-    CK(cudaMemset(s->bst[0].diag, 0, 16 * sizeof(double)));
+    if (method == TITUS_BUG_ADAPTIVE && max_steps > 0) max_iters = max_steps;
+    for (int t = 0; t < T; ++t) CK(cudaMemsetAsync(s->bst[t].bar, 0, (size_t)(G + 1) * sizeof(unsigned), stream));
+    CK(cudaMemsetAsync(s->bst[0].status, 0, sizeof(int), stream));
+    CK(cudaMemsetAsync(s->bst[0].diag, 0, 16 * sizeof(double), stream));
+    CK(cudaMemsetAsync(b->d_queue, 0, sizeof(int), stream));
     DevProblem P = s->P;
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
     P.prof = nullptr;
     P.zero_smem = 0;
     s->take_debug_hooks(P);
     if (opt && opt->profile) {
-        CK(cudaMemset(s->prof, 0, PF_SLOTS * sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));
         P.prof = s->prof;
     }
     WideState* dst = s->d_bst;
-    int Tl = T, Gl = G, ns = nspots, r0l = r0;
-    void* args[] = {&P, &dst, &Gl, &Tl, &d_sd, &ns, &r0l, &max_iters};
-    CK(cudaLaunchCooperativeKernel((void*)kfun, dim3(T * G), dim3(wide::NT), args, sizeof(WSmem), nullptr));
+    SpotData* d_sd = b->d_sd;
+    int Tl = T, Gl = G, ns = b->nspots, r0l = r0, msl = (method == TITUS_PARALLEL_ADAPTIVE) ? max_steps : 0;
+    int* queue = b->d_queue;
+    const int* order = b->d_order;
+    void* args[] = {&P, &dst, &Gl, &Tl, &d_sd, &ns, &r0l, &max_iters, &msl, &queue, &order};
+    CK(cudaLaunchCooperativeKernel((void*)kfun, dim3(T * G), dim3(wide::NT), args, sizeof(WSmem), stream));
+    b->last_T = T;
+    b->last_G = G;
+    b->launched = true;
+    s->last_method = method;
+    return TITUS_OK;
+}
+
+int titus_host::batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
+    if (!b->launched) return fail(TITUS_ERR_ARG, "batch has not been solved yet");
+    titus_solver* s = b->s;
     CK(cudaDeviceSynchronize());
     int status = 0;
     CK(cudaMemcpy(&status, s->bst[0].status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (status != 0) return fail(status == ST_LIMIT ? TITUS_ERR_LIMIT : TITUS_ERR_DEVICE,
-                                 "batched solve: device status %d (teams %d x %d CTAs)", status, T, G);
-    CK(cudaMemcpy(dose_out, d_dose, (size_t)nspots * n * sizeof(double), cudaMemcpyDeviceToHost));
-    std::vector<int> res(2 * nspots);
-    CK(cudaMemcpy(res.data(), d_res, res.size() * sizeof(int), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < nspots; ++i) {
+    if (status != 0) {
+        double d[16];
+        CK(cudaMemcpy(d, s->bst[0].diag, sizeof(d), cudaMemcpyDeviceToHost));
+        if (status == ST_BARRIER_TIMEOUT)
+            return fail(TITUS_ERR_DEVICE,
+                        "batched solve: device status %d: team barrier timeout (CTA %g at barrier %g saw %g arrivals, "
+                        "wanted %g; teams %d x %d CTAs)", status, d[8], d[14], d[9], d[10], b->last_T, b->last_G);
+        return fail(status == ST_LIMIT ? TITUS_ERR_LIMIT : TITUS_ERR_DEVICE,
+                    "batched solve: device status %d (teams %d x %d CTAs)", status, b->last_T, b->last_G);
+    }
+    const int n = s->n;
+    if (dose_out) CK(cudaMemcpy(dose_out, b->d_dose, (size_t)b->nspots * n * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int> res(2 * b->nspots);
+    CK(cudaMemcpy(res.data(), b->d_res, res.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < b->nspots; ++i) {
         if (rank_out) rank_out[i] = res[2 * i];
         if (iters_out) iters_out[i] = res[2 * i + 1];
     }
     return TITUS_OK;
+}
+
+void titus_host::batch_free(titus_batch* b) { delete b; }
+
+int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots,
+                                   const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
+    titus_batch* b = nullptr;
+    int rc = batch_upload(s, nspots, spots, &b);
+    if (rc) return rc;
+    rc = batch_launch(b, method, opt, nullptr);
+    if (!rc) rc = batch_fetch(b, dose_out, rank_out, iters_out);
+    batch_free(b);
+    return rc;
 }
 
 void titus_host::wide_free(titus_solver* s) {

@@ -469,6 +469,30 @@ extern "C" int titus_solve_batched(titus_solver_t* s, int32_t method, const titu
     return titus_host::wide_solve_batched(s, method, opt, nspots, spots, dose_out, rank_out, iters_out);
 }
 
+extern "C" int titus_batch_upload(titus_solver_t* s, int32_t nspots, const titus_spot_t* spots,
+                                  titus_batch_t** out) {
+    if (!s || !spots || !out) return fail(TITUS_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    if (nspots < 1) return fail(TITUS_ERR_ARG, "nspots < 1");
+    return titus_host::batch_upload(s, nspots, spots, out);
+}
+
+extern "C" int titus_batch_solve_device(titus_batch_t* b, int32_t method, const titus_options_t* opt, void* stream) {
+    if (!b) return fail(TITUS_ERR_ARG, "batch is NULL");
+    if (method != TITUS_PARALLEL_ADAPTIVE && method != TITUS_BUG_ADAPTIVE)
+        return fail(TITUS_ERR_ARG, "batched solves run the adaptive integrators (method 1 or 2), got %d", method);
+    return titus_host::batch_launch(b, method, opt, (cudaStream_t)stream);
+}
+
+extern "C" int titus_batch_fetch(titus_batch_t* b, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
+    if (!b) return fail(TITUS_ERR_ARG, "batch is NULL");
+    return titus_host::batch_fetch(b, dose_out, rank_out, iters_out);
+}
+
+extern "C" void titus_batch_destroy(titus_batch_t* b) {
+    if (b) titus_host::batch_free(b);
+}
+
 extern "C" void titus_destroy(titus_solver_t* s) { delete s; }
 
 extern "C" int titus_last_error(char* buf, size_t len) {

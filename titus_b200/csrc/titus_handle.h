@@ -8,6 +8,7 @@
 #include "wide_common.cuh"
 
 struct titus_solver;
+struct titus_batch;
 
 namespace titus_host {
 
@@ -43,6 +44,10 @@ int wide_fetch(titus_solver* s, titus_result_t* res);
 int wide_set_state(titus_solver* s, int rank, const double* X, const double* S, const double* W, const double* psi,
                    const double* dose, int n_next);
 void wide_free(titus_solver* s);
+int batch_upload(titus_solver* s, int nspots, const titus_spot_t* spots, titus_batch** out);
+int batch_launch(titus_batch* b, int method, const titus_options_t* opt, cudaStream_t stream);
+int batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out, int32_t* iters_out);
+void batch_free(titus_batch* b);
 int wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots, const titus_spot_t* spots,
                        double* dose_out, int32_t* rank_out, int32_t* iters_out);
 

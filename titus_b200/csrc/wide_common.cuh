@@ -244,16 +244,73 @@ __device__ inline void g_zero(double* D, int ldd, int m, int n) {
 }
 
 // ----------------------------------------------------------- row helpers ---
+// Tile moves between global memory (L2, `.cg`: coherent across the team's
+// CTAs) and shared memory. Each thread first issues up to WU loads into
+// registers and only then writes them, so a tile keeps WU x NT loads in flight
+// instead of one load latency per element; with an even column count, offset
+// and leading dimensions the elements move as 16-byte pairs.
+constexpr int WU = 8;
+
+__device__ __forceinline__ double2 ldcg2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
+
 // rows [r0, r0+nr) x cols [c0, c0+k) of A (ld lda) -> t (ld ldt) at column tc
 __device__ __forceinline__ void wload(double* t, int ldt, int tc, const double* A, int lda, int c0, int r0, int nr,
                                       int k) {
-    for (int e = threadIdx.x; e < nr * k; e += NT) {
-        const int r = e / k, j = e - (e / k) * k;
-        t[r * ldt + tc + j] = ldcg(A + (size_t)(r0 + r) * lda + c0 + j);
+    if (((k | c0 | lda | ldt | tc) & 1) == 0 && ((reinterpret_cast<uintptr_t>(t) | reinterpret_cast<uintptr_t>(A)) & 15) == 0) {
+        const int h = k >> 1, cnt = nr * h;
+        for (int b = threadIdx.x; b < cnt; b += WU * NT) {
+            double2 v[WU];
+#pragma unroll
+            for (int u = 0; u < WU; ++u) {
+                const int e = b + u * NT;
+                if (e < cnt) {
+                    const int r = e / h, j = 2 * (e - r * h);
+                    v[u] = ldcg2(A + (size_t)(r0 + r) * lda + c0 + j);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < WU; ++u) {
+                const int e = b + u * NT;
+                if (e < cnt) {
+                    const int r = e / h, j = 2 * (e - r * h);
+                    *reinterpret_cast<double2*>(t + r * ldt + tc + j) = v[u];
+                }
+            }
+        }
+        return;
+    }
+    const int cnt = nr * k;
+    for (int b = threadIdx.x; b < cnt; b += WU * NT) {
+        double v[WU];
+#pragma unroll
+        for (int u = 0; u < WU; ++u) {
+            const int e = b + u * NT;
+            if (e < cnt) {
+                const int r = e / k, j = e - r * k;
+                v[u] = ldcg(A + (size_t)(r0 + r) * lda + c0 + j);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < WU; ++u) {
+            const int e = b + u * NT;
+            if (e < cnt) {
+                const int r = e / k, j = e - r * k;
+                t[r * ldt + tc + j] = v[u];
+            }
+        }
     }
 }
 __device__ __forceinline__ void wstore(double* A, int lda, int c0, const double* t, int ldt, int tc, int r0, int nr,
                                        int k) {
+    if (((k | c0 | lda | ldt | tc) & 1) == 0 && ((reinterpret_cast<uintptr_t>(t) | reinterpret_cast<uintptr_t>(A)) & 15) == 0) {
+        const int h = k >> 1;
+        for (int e = threadIdx.x; e < nr * h; e += NT) {
+            const int r = e / h, j = 2 * (e - r * h);
+            *reinterpret_cast<double2*>(A + (size_t)(r0 + r) * lda + c0 + j) =
+                *reinterpret_cast<const double2*>(t + r * ldt + tc + j);
+        }
+        return;
+    }
     for (int e = threadIdx.x; e < nr * k; e += NT) {
         const int r = e / k, j = e - (e / k) * k;
         A[(size_t)(r0 + r) * lda + c0 + j] = t[r * ldt + tc + j];
