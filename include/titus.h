@@ -181,6 +181,9 @@ typedef struct titus_batch titus_batch_t;
 int titus_batch_upload(titus_solver_t* solver, int32_t nspots, const titus_spot_t* spots, titus_batch_t** out);
 int titus_batch_solve_device(titus_batch_t* batch, int32_t method, const titus_options_t* options, void* stream);
 int titus_batch_fetch(titus_batch_t* batch, double* dose_out, int32_t* rank_out, int32_t* iters_out);
+/* After titus_batch_fetch: per spot, the sum over its loop iterations of the
+ * rank entering each (nspots entries): the work done, for throughput accounting. */
+int titus_batch_rank_sums(titus_batch_t* batch, int32_t* out);
 void titus_batch_destroy(titus_batch_t* batch);
 
 void titus_destroy(titus_solver_t* solver);

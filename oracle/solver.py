@@ -345,13 +345,15 @@ def _step_prologue(solver, psi, X, S, W, n, dE):
 
 
 def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
-                       n_begin: int = 2, return_state: bool = False):
+                       n_begin: int = 2, return_state: bool = False, on_iter=None):
     """``SolveFirstCollisionSourceDLRParallel`` (``SolverCSD.jl:1726-2008``).
 
     Returns (X U, 1/2 sqrt(gamma_0) Sigma, O W V, W V, dose, rVec, psi) with
     rVec (2 x nEnergies): row 0 the accumulated pseudo-time t, row 1 the rank.
     ``state`` (X, S, W, psi, dose, optionally t) resumes the loop at ``n_begin``;
     ``return_state`` returns that dict (with ``n_next``) for the end of the run.
+    ``on_iter(rank)`` is called at the start of every step with the rank
+    entering it and once with None after the last (timing hook).
     """
     s = solver.settings
     mode = solver.basis_mode
@@ -375,6 +377,8 @@ def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None, state: d
         t = state.get("t", (n_begin - 2) * dE)
     last = nE if max_steps is None else min(nE, n_begin - 1 + max_steps)
     for n in range(n_begin, last + 1):
+        if on_iter is not None:
+            on_iter(S.shape[0])
         sigma, Dvec, D = _step_prologue(solver, psi, X, S, W, n, dE)
         if n > 2:
             G = solver._x_grams(X, X)  # before X[bnd] = 0 (:1856-1859)
@@ -421,6 +425,8 @@ def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None, state: d
         rVec[0, n - 1] = t
         rVec[1, n - 1] = r
         t += dE
+    if on_iter is not None:
+        on_iter(None)
     if return_state:
         return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), t=t,
                     n_next=last + 1, rVec=rVec)

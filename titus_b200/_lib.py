@@ -76,6 +76,7 @@ SIGNATURES = [
     ("titus_batch_upload", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Spot), C.POINTER(C.c_void_p)]),
     ("titus_batch_solve_device", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_void_p]),
     ("titus_batch_fetch", C.c_int, [C.c_void_p, _dp, _ip, _ip]),
+    ("titus_batch_rank_sums", C.c_int, [C.c_void_p, _ip]),
     ("titus_batch_destroy", None, [C.c_void_p]),
     ("titus_destroy", None, [C.c_void_p]),
     ("titus_last_error", C.c_int, [C.c_char_p, C.c_size_t]),

@@ -1233,6 +1233,7 @@ struct LoopState {
     int psi_idx;
     double t;
     int iters;
+    int rank_sum;   // sum over the iterations of the rank entering each
     int eta_count;
     int n;          // on return: first energy index not processed
     bool aborted;
@@ -1247,6 +1248,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
     int psi_idx = ls.psi_idx;
     double t = ls.t;
     int iters = ls.iters;
+    int rank_sum = ls.rank_sum;
     int eta_count = ls.eta_count;
     const double dE = P.dE;
     const int nE = P.nE;
@@ -1271,6 +1273,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
             x.st.time_hist[iters] = (double)n;   // energy index (eGrid[n-1] on the host)
         }
         ++iters;
+        rank_sum += x.r;
         // ---- A, B
         w_phase_A(x, n);
         if (!wsync(x)) { aborted = true; break; }
@@ -1540,6 +1543,7 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
     ls.psi_idx = psi_idx;
     ls.t = t;
     ls.iters = iters;
+    ls.rank_sum = rank_sum;
     ls.eta_count = eta_count;
     ls.n = n;
     ls.aborted = aborted;
@@ -1575,6 +1579,7 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
     ls.psi_idx = ldcg(x.st.info + 2);
     ls.t = ldcg(x.st.tvar);
     ls.iters = 0;
+    ls.rank_sum = 0;
     ls.eta_count = ldcg(x.st.info + 4);
     ls.n = n_begin;
     ls.aborted = false;
@@ -1605,7 +1610,7 @@ struct SpotData {
     const double* sigma;       // nE x (npn+1)
     const double* bc_space;    // n
     double* dose;              // n (output)
-    int* result;               // [rank, iterations]
+    int* result;               // [final rank, iterations, sum of the ranks entering the iterations]
 };
 
 // Initial factors of one spot (SolverCSD.jl:1728-1760, :2013-2050) on this
@@ -1694,6 +1699,7 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
         ls.psi_idx = 0;
         ls.t = 0.0;
         ls.iters = 0;
+        ls.rank_sum = 0;
         ls.eta_count = 0;
         ls.n = 2;
         ls.aborted = false;
@@ -1704,6 +1710,7 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
         if (x.b == 0 && threadIdx.x == 0) {
             sp.result[0] = x.r;
             sp.result[1] = ls.iters;
+            sp.result[2] = ls.rank_sum;
         }
     }
 }

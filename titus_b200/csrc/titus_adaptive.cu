@@ -357,6 +357,7 @@ struct titus_batch {
     int* d_queue = nullptr;
     int last_T = 0, last_G = 0;
     bool launched = false;
+    std::vector<int> rank_sums;   // per spot, after the last fetch
 };
 
 int titus_host::batch_upload(titus_solver* s, int nspots, const titus_spot_t* spots, titus_batch** out) {
@@ -389,7 +390,7 @@ int titus_host::batch_upload(titus_solver* s, int nspots, const titus_spot_t* sp
     int rc;
     if ((rc = b->tmp.alloc(&d_stop, tot_e)) || (rc = b->tmp.alloc(&d_bce, tot_e)) ||
         (rc = b->tmp.alloc(&d_sig, tot_e * npn1)) || (rc = b->tmp.alloc(&d_bcs, (size_t)nspots * n)) ||
-        (rc = b->tmp.alloc(&b->d_dose, (size_t)nspots * n)) || (rc = b->tmp.alloc(&b->d_res, (size_t)2 * nspots)) ||
+        (rc = b->tmp.alloc(&b->d_dose, (size_t)nspots * n)) || (rc = b->tmp.alloc(&b->d_res, (size_t)3 * nspots)) ||
         (rc = b->tmp.alloc(&b->d_queue, (size_t)1)))
         return bail(rc);
     std::vector<SpotData> sd(nspots);
@@ -413,7 +414,7 @@ int titus_host::batch_upload(titus_solver* s, int nspots, const titus_spot_t* sp
         d.sigma = d_sig + off * npn1;
         d.bc_space = d_bcs + (size_t)i * n;
         d.dose = b->d_dose + (size_t)i * n;
-        d.result = b->d_res + 2 * i;
+        d.result = b->d_res + 3 * i;
         off += nE;
     }
     if ((rc = b->tmp.alloc(&b->d_sd, (size_t)nspots, sd.data()))) return bail(rc);
@@ -494,16 +495,24 @@ int titus_host::batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out,
     }
     const int n = s->n;
     if (dose_out) CK(cudaMemcpy(dose_out, b->d_dose, (size_t)b->nspots * n * sizeof(double), cudaMemcpyDeviceToHost));
-    std::vector<int> res(2 * b->nspots);
+    std::vector<int> res(3 * b->nspots);
     CK(cudaMemcpy(res.data(), b->d_res, res.size() * sizeof(int), cudaMemcpyDeviceToHost));
     for (int i = 0; i < b->nspots; ++i) {
-        if (rank_out) rank_out[i] = res[2 * i];
-        if (iters_out) iters_out[i] = res[2 * i + 1];
+        if (rank_out) rank_out[i] = res[3 * i];
+        if (iters_out) iters_out[i] = res[3 * i + 1];
     }
+    b->rank_sums.assign(b->nspots, 0);
+    for (int i = 0; i < b->nspots; ++i) b->rank_sums[i] = res[3 * i + 2];
     return TITUS_OK;
 }
 
 void titus_host::batch_free(titus_batch* b) { delete b; }
+
+int titus_host::batch_rank_sums(titus_batch* b, int32_t* out) {
+    if ((int)b->rank_sums.size() != b->nspots) return fail(TITUS_ERR_ARG, "fetch the batch first");
+    for (int i = 0; i < b->nspots; ++i) out[i] = b->rank_sums[i];
+    return TITUS_OK;
+}
 
 int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots,
                                    const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out) {

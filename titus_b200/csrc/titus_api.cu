@@ -489,6 +489,11 @@ extern "C" int titus_batch_fetch(titus_batch_t* b, double* dose_out, int32_t* ra
     return titus_host::batch_fetch(b, dose_out, rank_out, iters_out);
 }
 
+extern "C" int titus_batch_rank_sums(titus_batch_t* b, int32_t* out) {
+    if (!b || !out) return fail(TITUS_ERR_ARG, "NULL argument");
+    return titus_host::batch_rank_sums(b, out);
+}
+
 extern "C" void titus_batch_destroy(titus_batch_t* b) {
     if (b) titus_host::batch_free(b);
 }

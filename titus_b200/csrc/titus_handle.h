@@ -48,6 +48,7 @@ int batch_upload(titus_solver* s, int nspots, const titus_spot_t* spots, titus_b
 int batch_launch(titus_batch* b, int method, const titus_options_t* opt, cudaStream_t stream);
 int batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out, int32_t* iters_out);
 void batch_free(titus_batch* b);
+int batch_rank_sums(titus_batch* b, int32_t* out);
 int wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots, const titus_spot_t* spots,
                        double* dose_out, int32_t* rank_out, int32_t* iters_out);
 

@@ -103,11 +103,8 @@ class SolverCSD:
         return (eTrafo.size, float(eTrafo[1] - eTrafo[0]), np.ascontiguousarray(S), np.ascontiguousarray(bc_energy),
                 sigma, np.ascontiguousarray(bc_space))
 
-    def solve_batched(self, spots, method: int = _lib.TITUS_BUG_ADAPTIVE, team_ctas: int = 1, max_steps: int = 0):
-        """All pencil beams ``spots`` = [(energy, y0), ...] in one persistent
-        launch (titus_solve_batched). Returns (dose (nspots x n), rank, iterations)."""
-        lib = _lib.load()
-        h = self.handle()
+    def spot_array(self, spots):
+        """titus_spot_t array (and the host tables it points to) for [(energy, y0), ...]."""
         ns = len(spots)
         arr = (_lib.Spot * ns)()
         keep = []
@@ -120,6 +117,19 @@ class SolverCSD:
             arr[i].bc_energy = _lib.as_dp(bce)
             arr[i].sigma = _lib.as_dp(sig)
             arr[i].bc_space = _lib.as_dp(bcs)
+        return arr, keep
+
+    def batch(self, spots):
+        """Upload pencil beams once for repeated batched solves (PencilBeamBatch)."""
+        return PencilBeamBatch(self, spots)
+
+    def solve_batched(self, spots, method: int = _lib.TITUS_BUG_ADAPTIVE, team_ctas: int = 1, max_steps: int = 0):
+        """All pencil beams ``spots`` = [(energy, y0), ...] in one persistent
+        launch (titus_solve_batched). Returns (dose (nspots x n), rank, iterations)."""
+        lib = _lib.load()
+        h = self.handle()
+        ns = len(spots)
+        arr, keep = self.spot_array(spots)
         dose = np.zeros((ns, self.n))
         rank = np.zeros(ns, dtype=np.int32)
         iters = np.zeros(ns, dtype=np.int32)
@@ -286,6 +296,55 @@ class SolverCSD:
         nx, ny = self.settings.NCellsX, self.settings.NCellsY
         psi = out["psi"].reshape(nx, ny, self.q)
         return X @ U, 0.5 * math.sqrt(self.gamma[0]) * sig, self.O @ (W @ V), W @ V, out["dose"], psi
+
+
+class PencilBeamBatch:
+    """Pencil beams whose tables live on the device (titus_batch_upload), so
+    repeated batched solves move no host data: ``solve_device(stream)``
+    launches, ``fetch()`` waits and returns (dose (nspots x n), final rank,
+    iterations); ``rank_sums()`` gives the per-spot sum of the ranks entering
+    the iterations of the last fetched solve."""
+
+    def __init__(self, solver: SolverCSD, spots):
+        self.solver = solver
+        self.nspots = len(spots)
+        arr, keep = solver.spot_array(spots)
+        self.n_energies = np.array([arr[i].n_energies for i in range(self.nspots)], dtype=np.int64)
+        h = C.c_void_p()
+        _lib.check(_lib.load().titus_batch_upload(solver.handle(), self.nspots, arr, C.byref(h)), "titus_batch_upload")
+        self._h = h
+
+    def solve_device(self, method: int = _lib.TITUS_BUG_ADAPTIVE, team_ctas: int = 1, max_steps: int = 0,
+                     stream: int = 0):
+        opt = self.solver.options(max_steps)
+        opt.team_ctas = team_ctas
+        _lib.check(_lib.load().titus_batch_solve_device(self._h, method, C.byref(opt), C.c_void_p(stream)),
+                   "titus_batch_solve_device")
+
+    def fetch(self, want_dose: bool = True):
+        n = self.solver.n
+        dose = np.zeros((self.nspots, n)) if want_dose else None
+        rank = np.zeros(self.nspots, dtype=np.int32)
+        iters = np.zeros(self.nspots, dtype=np.int32)
+        _lib.check(_lib.load().titus_batch_fetch(self._h, _lib.as_dp(dose) if want_dose else None, _lib.as_ip(rank),
+                                                  _lib.as_ip(iters)), "titus_batch_fetch")
+        return dose, rank, iters
+
+    def rank_sums(self):
+        out = np.zeros(self.nspots, dtype=np.int32)
+        _lib.check(_lib.load().titus_batch_rank_sums(self._h, _lib.as_ip(out)), "titus_batch_rank_sums")
+        return out
+
+    def close(self):
+        if self._h is not None:
+            _lib.load().titus_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def SolveFirstCollisionSourceDLR(solver: SolverCSD, max_steps: int = 0):
