@@ -21,12 +21,13 @@ same problem is run for its first 200 iterations and compared with the FP64
 oracle's dose for them (``dose_rel_err_vs_oracle``, fixture
 ``tests/golden/phantom200_P29_bug200.npz``).
 
-``batched`` (also measured once after the timed steps of the default run,
-``--no-batched`` skips it): 256 pencil beams on the seeded 128 x 128 phantom,
-P_21, rank cap 60, energies U(2, 8) MeV, entry y0 U(0.1, 0.9) (seed 3), all in
-one persistent launch with one-CTA teams taking spots from a device work
-queue. Its ``plain`` companion is the same spots solved one at a time with all
-SMs, timed on the shortest spots and scaled by iteration counts.
+``batched``: 256 pencil beams on the seeded 128 x 128 phantom, P_21, rank cap
+60, energies U(2, 8) MeV, entry y0 U(0.1, 0.9) (seed 3), all in one persistent
+launch with small teams taking spots from a device work queue. Its ``plain``
+companion is the same spots solved one at a time with all SMs, timed on the
+shortest spots and scaled by iteration counts. The default run measures it
+once after the timed steps on every spot's first 600 iterations
+(``--no-batched`` skips it); ``--method batched`` times whole plans.
 
 Multi-GPU (``--gpus N``; without WORLD_SIZE in the environment the script
 re-launches itself under torch.distributed.run): the solve runs as N
@@ -59,9 +60,14 @@ WORKLOADS = {
                      method="parallel"),
     "fixed": dict(name="csd_water_beam_100x100_P21_r20_fixed", Nx=101, r=20, nPN=21, problem="csdWaterBeam",
                   method="fixed"),
+    "pn_full": dict(name="csd_water_beam_100x100_P21_full_rank", Nx=101, r=4, nPN=21, problem="csdWaterBeam",
+                    method="pn_full"),
 }
 BATCHED = dict(name="pencil_beams256_phantom_128x128_P21_cap60_bug", Nx=129, r=60, nPN=21, problem="csdPhantom",
                spots=256, seed=3, emin=2.0, emax=8.0, ymin=0.1, ymax=0.9)
+# the batched plan measured beside the default solve: every spot's first
+# BATCHED_SAMPLE_ITERS loop iterations (the whole plan takes minutes)
+BATCHED_SAMPLE_ITERS = 600
 FIXTURE = os.path.join(ROOT, "tests", "golden", "phantom200_P29_bug200.npz")
 RANKS_FIXTURE = os.path.join(ROOT, "tests", "golden", "phantom200_P29_bug_ranks.npz")
 # DRAM bytes (read + write) per energy step of each kernel on its workload, from
@@ -205,6 +211,16 @@ def cpu_cost_model(w, ranks, state200=None, head=40, tail=20):
     from oracle.solver import solve_dlr_bug, solve_dlr_fixed, solve_dlr_parallel
 
     mk = _oracle_setup(w)
+    if w["method"] == "pn_full":
+        from oracle.full_rank import solve_pn_full
+
+        o = mk()
+        t0 = time.perf_counter()
+        solve_pn_full(o, max_steps=head)
+        per = (time.perf_counter() - t0) / head
+        steps = o.csd.eTrafo.size - 1
+        return per * steps, (f"FP64 oracle, full-rank P_N: {head} energy steps timed, x {steps} steps "
+                             f"(constant cost per step)"), None
     fn = {"bug": solve_dlr_bug, "parallel": solve_dlr_parallel, "fixed": solve_dlr_fixed}[w["method"]]
     if w["method"] == "fixed":
         o = mk()
@@ -332,6 +348,76 @@ def run_gpu_solve(args, w, rank, world, local_rank, dist):
     return info
 
 
+# ------------------------------------------------------- full-rank P_N arm
+def run_gpu_pn_full(args, w, rank, world, local_rank, dist):
+    """Full-rank P_N solve (SolveFirstCollisionSource): one captured graph of
+    three kernels per energy step; value times the graph launch with CUDA events."""
+    import numpy as np
+    import torch
+
+    from titus_b200 import Settings, SolverCSD, _lib
+    from titus_b200.replicas import replica_throughput
+
+    s = Settings(w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"])
+    solver = SolverCSD(s)
+    lib = _lib.load()
+    h = solver.handle()
+    opt = solver.options()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def solve_once():
+        _lib.check(lib.titus_pn_full_solve_device(h, C.byref(opt), C.c_void_p(stream.cuda_stream)),
+                   "titus_pn_full_solve_device")
+
+    for _ in range(args.warmup):
+        solve_once()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    elapsed = 0.0
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solve_once()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            elapsed += e0.elapsed_time(e1) / 1e3
+    value, t_max = replica_throughput(args.steps, elapsed, world, device="cuda")
+    dose = np.zeros(solver.n)
+    _lib.check(lib.titus_pn_full_fetch(h, None, _lib.as_dp(dose), None), "titus_pn_full_fetch")
+    # end to end: upload, solve, u/dose/psi copy-out, free
+    p, keep = solver.problem_struct()
+    h2d = sum(a.nbytes for a in keep)
+    u = np.zeros((solver.n, solver.N))
+    psi = np.zeros((solver.n, solver.q))
+    d2h = u.nbytes + dose.nbytes + psi.nbytes
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2 = C.c_void_p()
+    _lib.check(lib.titus_create(C.byref(p), C.byref(h2)), "titus_create")
+    rc = lib.titus_pn_full_solve(h2, C.byref(opt), _lib.as_dp(u), _lib.as_dp(dose), _lib.as_dp(psi))
+    lib.titus_destroy(h2)
+    _lib.check(rc, "titus_pn_full_solve")
+    e2e_value, _ = replica_throughput(1, time.perf_counter() - t0, world, device="cuda")
+    steps = solver.nE - 1
+    nN = solver.n * solver.N
+    # per step: moments read u, write W (5 nN); stream reads u, W (4 nN), writes u' (6 nN);
+    # psi read + write (2 n q), dose read + write (2 n)
+    alg = steps * 8 * (11 * nN + 2 * solver.n * solver.q + 2 * solver.n)
+    peak, peak_kind = read_peaks()
+    achieved = alg / (t_max / args.steps) / 1e9
+    info = dict(value=value, ms_per_step=t_max / args.steps * 1e3, e2e_value=e2e_value, h2d=h2d, d2h=d2h,
+                alg=alg, achieved=achieved, peak=peak, peak_kind=peak_kind, clocks=clk.summary(),
+                dose_max=float(dose.max()), steps_per_solve=steps, q=solver.q, n=solver.n, N=solver.N)
+    solver.close()
+    return info
+
+
 # ------------------------------------------------------------ batched plan
 def batched_team(args, solver):
     """Team size (CTAs per spot) of the batched plan: --team-batched if given,
@@ -349,11 +435,13 @@ def batched_team(args, solver):
     return 1, "default"
 
 
-def run_gpu_batched(args, rank, world, local_rank, dist, steps, warmup, short_warmup=False):
+def run_gpu_batched(args, rank, world, local_rank, dist, steps, warmup, short_warmup=False, iters=0):
     """The 256-spot pencil-beam plan sharded by spot over the ranks: each step is
     one persistent launch of this rank's spots (device-resident tables), timed
     with CUDA events; e2e adds the host tables, upload, dose copy-back and the
-    SUM all-reduce of the weighted total dose (spots.plan_dose)."""
+    SUM all-reduce of the weighted total dose (spots.plan_dose). `iters` > 0
+    bounds every spot to its first `iters` loop iterations (the same bound for
+    batched and plain, so their ratio compares equal work)."""
     import numpy as np
     import torch
 
@@ -385,7 +473,7 @@ def run_gpu_batched(args, rank, world, local_rank, dist, steps, warmup, short_wa
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        batch.solve_device(_lib.TITUS_BUG_ADAPTIVE, team, stream=stream.cuda_stream)
+        batch.solve_device(_lib.TITUS_BUG_ADAPTIVE, team, max_steps=iters, stream=stream.cuda_stream)
         e1.record(stream)
         torch.cuda.synchronize()
         elapsed += e0.elapsed_time(e1) / 1e3
@@ -401,7 +489,7 @@ def run_gpu_batched(args, rank, world, local_rank, dist, steps, warmup, short_wa
     plain_it = 0
     max_rel = 0.0
     for i in order:
-        d, _, it = solver.solve_batched([local[i]], _lib.TITUS_BUG_ADAPTIVE, team_ctas=sms)
+        d, _, it = solver.solve_batched([local[i]], _lib.TITUS_BUG_ADAPTIVE, team_ctas=sms, max_steps=iters)
         plain_it += int(it[0])
         max_rel = max(max_rel, float(np.linalg.norm(d[0] - dose_b[i]) / np.linalg.norm(dose_b[i])))
     t_plain_sample = time.perf_counter() - t0
@@ -419,7 +507,7 @@ def run_gpu_batched(args, rank, world, local_rank, dist, steps, warmup, short_wa
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    total, _, _ = plan_dose(solver, spots, weights, "bug", team, device="cuda")
+    total, _, _ = plan_dose(solver, spots, weights, "bug", team, max_steps=iters, device="cuda")
     t_e2e = max_over_ranks(time.perf_counter() - t0, device="cuda")
     n, q = solver.n, solver.q
     alg = float(sum(algorithmic_bytes_per_step(n, 2.0 * rs / max(1, it), q) * it for rs, it in zip(rsum, it_b)))
@@ -430,12 +518,14 @@ def run_gpu_batched(args, rank, world, local_rank, dist, steps, warmup, short_wa
     peak, peak_kind = read_peaks()
     achieved = alg / t_max / 1e9
     out = {
-        "workload": cfg["name"], "spots": len(spots), "team_ctas": team, "team_source": team_src,
+        "workload": cfg["name"] + (f"_first{iters}iters" if iters else ""), "spots": len(spots),
+        "iterations_per_spot_bound": iters or None, "team_ctas": team, "team_source": team_src,
         "value": value, "unit": "solves/s", "seconds": t_max, "steps": nsteps,
         "iterations_total": int(tot_it), "spot_steps_per_s": tot_it / t_max,
         "plain": {"value": len(spots) / t_plain, "seconds_estimated": t_plain, "seconds_per_iteration": per_it,
                   "team_ctas": sms, "sample": f"{len(order)} shortest spots of each rank solved one at a time "
-                                              f"({plain_it} iterations), scaled by the plan's iterations"},
+                                              f"({plain_it} iterations, same bound), scaled by the plan's "
+                                              f"iterations"},
         "batched_over_plain": t_plain / t_max,
         "max_rel_dose_diff_batched_vs_plain": max_rel,
         "e2e": {"value": len(spots) / t_e2e, "unit": "solves/s", "seconds": t_e2e,
@@ -532,7 +622,7 @@ def run_reference(args, w, rank):
                      "config": batched_config(cfg, world=args.gpus)})
     else:
         ranks = _ranks_for(w)
-        if ranks is None and w["method"] != "fixed":
+        if ranks is None and w["method"] not in ("fixed", "pn_full"):
             print(json.dumps({"impl": "reference", "unavailable": "rank-history fixture missing: run "
                               "tests/golden/make_rank_history.py on a GPU"}), flush=True)
             return
@@ -600,11 +690,33 @@ def run_gpu(args, w, rank, world, local_rank):
                 t, sample = batched_reference_seconds(BATCHED)
                 line["cpu_baseline"] = {"value": BATCHED["spots"] / t, "unit": "solves/s",
                                         "cores": cores, "kind": "port", "sample": sample}
+    elif args.method == "pn_full":
+        info = run_gpu_pn_full(args, w, rank, world, local_rank, dist)
+        if rank == 0:
+            line = {"metric": "dose solves/s", "value": info["value"], "unit": "solves/s", "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["ms_per_step"],
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic",
+                    "config": dict(solve_config(w, info["steps_per_solve"], world), ordinates=info["q"]),
+                    "e2e": {"value": info["e2e_value"], "unit": "solves/s", "h2d_bytes_per_step": int(info["h2d"]),
+                            "d2h_bytes_per_step": int(info["d2h"])},
+                    "roofline": {"bound": "hbm", "achieved": info["achieved"], "peak": info["peak"], "unit": "GB/s",
+                                 "frac": info["achieved"] / info["peak"], "traffic": None,
+                                 "peak_kind": info["peak_kind"], "algorithmic_bytes_per_launch": info["alg"],
+                                 "note": "all three kernels of every energy step (one graph launch)"},
+                    "clocks": info["clocks"], "gpu_launches": 3 * info["steps_per_solve"] * args.steps,
+                    "dose_max": info["dose_max"], "cpu_baseline": None}
+            if world == 1 and not args.no_cpu_baseline:
+                cores = host_threads()
+                t, sample, _ = cpu_cost_model(w, None)
+                line["cpu_baseline"] = {"value": 1.0 / t, "unit": "solves/s", "cores": cores, "kind": "port",
+                                        "sample": sample}
     else:
         info = run_gpu_solve(args, w, rank, world, local_rank, dist)
         batched = None
         if not args.no_batched:
-            batched = run_gpu_batched(args, rank, world, local_rank, dist, 1, 1, short_warmup=True)
+            batched = run_gpu_batched(args, rank, world, local_rank, dist, 1, 1, short_warmup=True,
+                                      iters=BATCHED_SAMPLE_ITERS)
         if rank == 0:
             peak = info["peak"]
             line = {

@@ -69,6 +69,8 @@ typedef struct titus_problem {
     int32_t n_w_completion;
     const int32_t* sweep_restore;  /* cells whose ordinate-0 value is restored after the sweep */
     int32_t n_sweep_restore;
+    const double* stopping_mid;    /* nE-1: csd.SMid (stopping power at the energy midpoints, CSD.jl:88-89);
+                                      read by the full-rank P_N solver only, may be NULL otherwise */
 } titus_problem_t;
 
 typedef struct titus_options {
@@ -212,12 +214,15 @@ int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
  * host memory; dose (n), X (n x r), S (r x r), W (N x r) and psi (n x q) are
  * device output buffers owned by the caller (row-major). All intermediates live
  * in one static device array of 16 MiB that every GPU loading the library keeps
- * until the process exits; problems that need more are rejected with
- * TITUS_ERR_LIMIT (rank <= 24, q <= 24, at most 32 CTAs per solve). All calls
- * on a device share that array, so calls that overlap on the GPU race: issue
- * them one at a time per device. Each call clears what must start at zero. The
- * first call on a device looks up the array's address; make it before any
- * stream capture. The call returns after the solve has finished on `stream`.
+ * until the process exits. A problem fits when
+ *   913 n + 580 N + 4 nE + 73728 G + 48 KiB <= 16 MiB
+ * (n cells, N moments, nE energies, G <= 32 CTAs; about 16 700 cells at P21
+ * with G = 16); larger ones, rank > 24 or q > 24 are rejected with
+ * TITUS_ERR_LIMIT. All calls on a device share that array, so calls that
+ * overlap on the GPU race: issue them one at a time per device. Each call
+ * clears what must start at zero and looks the array's address up for the
+ * current device. The call is synchronous (it reads e_trafo[0..1] and the status
+ * words back and waits for `stream`), so it cannot run inside a stream capture.
  * Error text (if any) is written to err[0..err_len). */
 int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* options, double* dose,
                         double* X, double* S, double* W, double* psi, int32_t* rank_out, void* stream,
@@ -236,6 +241,24 @@ int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* o
  * TITUS_ERR_LIMIT (ny*q >= 2^31) or TITUS_ERR_CUDA. */
 int titus_limited_flux(int32_t nx, int32_t ny, int32_t q, double dx, double dy, const double* omega_x,
                        const double* omega_z, const double* phi, double* flux, void* stream);
+
+/* Full-rank P_N first-collision solver (SolveFirstCollisionSource,
+ * code/SolverCSD.jl:465-586): the collided flux as the whole moment matrix u
+ * (n x N, row-major, row i*ny + j), advanced with the reference's explicit
+ * step -- upwind sweep of the reduced ordinates with the beam inflow at
+ * energy[n], uTilde = u - dE (L2x u Ax + L2y u Az + L1x u |Ax| + L1y u |Az|),
+ * collision (I + dE D)^{-1}, in-scattering from psi, and the dose with csd.SMid
+ * (problem->stopping_mid must be set). It is the r -> N limit the DLR
+ * integrators approach. titus_pn_full_solve_device runs the whole sweep on
+ * `stream` (a cudaStream_t, NULL = default) as one captured CUDA graph of two
+ * kernels per energy step; options->max_steps bounds the steps (0 = all).
+ * titus_pn_full_fetch waits and copies u (n x N, raw: the reference returns
+ * 1/2 sqrt(gamma_0) u), the dose (n) and psi (n x q) to host buffers (each may
+ * be NULL). titus_pn_full_solve does both. */
+int titus_pn_full_solve_device(titus_solver_t* solver, const titus_options_t* options, void* stream);
+int titus_pn_full_fetch(titus_solver_t* solver, double* u_out, double* dose_out, double* psi_out);
+int titus_pn_full_solve(titus_solver_t* solver, const titus_options_t* options, double* u_out, double* dose_out,
+                        double* psi_out);
 
 /* Test hooks (no counterpart in the reference), for failure-detection tests
  * that fault nothing.

@@ -1,0 +1,86 @@
+"""Full-rank P_N first-collision solver (oracle restatement of
+``SolveFirstCollisionSource``, ``code/SolverCSD.jl:465-586``), FP64.
+
+Test infrastructure only: the GPU path (``titus_pn_full_*``) is checked
+against it. The collided flux is the full moment matrix u (n cells x N
+moments, row i*ny + j); per energy step n = 2..nE:
+
+* sigma = SigmaAtEnergy(energy[n]); Dvec[GlobalIndex(l,k)] = sigma_l;
+  D = sigma_0 - Dvec (``:530-538``);
+* boundary inflow at energy[n] with csd.S[n-1] (``PsiBeam(..., energy[n], ..., n-1)``,
+  ``:517-527``), upwind sweep, psi <- (psi - dE flux) / (1 + dE sigma_0)
+  (``:541-545``); the boundary cells' flux is zero, so they decay too;
+* uTilde = u - dE (L2x u Ax + L2y u Az + L1x u |Ax| + L1y u |Az|), boundary
+  rows zeroed (``:548-549``);
+* interior cells: uNew = (uTilde + dE Dvec . (MReduced psiNew)) / (1 + dE D),
+  uOUnc = psiNew . MReduced[0,:] (``:552-559``); boundary rows of uNew zero;
+* dose += dE (uNew[:,0] + uOUnc) SMid[n-1] / rho / (1 + (n == 2 or n == nE))
+  (``:575``).
+
+Returns (1/2 sqrt(gamma_0) u, dose, psi) like the reference (``:585``).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .solver import SolverCSD
+
+
+def sigma_vectors(solver: SolverCSD, n: int):
+    """sigma_l at energy[n] (1-based n, ``:530``) and the per-moment Dvec, D (``:533-540``)."""
+    sig = solver.csd.sigma_at_energy(solver.csd.eGrid[n - 1])
+    Dvec = solver.dvec(sig)
+    return sig, Dvec, sig[0] - Dvec
+
+
+def solve_pn_full(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None, n_begin: int = 2,
+                  return_state: bool = False):
+    s = solver.settings
+    eTrafo = solver.csd.eTrafo
+    energy = solver.csd.eGrid
+    nx, ny = s.NCellsX, s.NCellsY
+    n_cells = nx * ny
+    N = solver.N
+    psi = solver.setup_directions()
+    Mr = solver.MReduced
+    nE = eTrafo.size
+    dE = eTrafo[1] - eTrafo[0]
+    s.dE = dE
+    u = np.zeros((n_cells, N))
+    if state is not None:
+        u = state["u"].copy()
+        psi = state["psi"].reshape(psi.shape).copy()
+        solver.dose = state["dose"].copy()
+    st = solver.stencil
+    bnd = solver.boundaryIdx
+    inner = np.zeros((nx, ny), dtype=bool)
+    inner[1:-1, 1:-1] = True
+    inner = inner.ravel()
+    last = nE if max_steps is None else min(nE, n_begin - 1 + max_steps)
+    for n in range(n_begin, last + 1):
+        sig, Dvec, D = sigma_vectors(solver, n)
+        dE = eTrafo[n - 1] - eTrafo[n - 2]
+        solver.apply_bc(psi, energy[n - 1], n - 1)
+        flux = solver.flux_upwind(psi)
+        psi = psi - dE * flux
+        psi_new = psi / (1.0 + dE * sig[0])
+        # u A_d as (A_d^T u^T)^T: sparse times dense, the reference's u*Ax order of factors
+        uA = [np.asarray((A.T @ u.T).T) for A in (solver.Ax, solver.Az, solver.AbsAx, solver.AbsAz)]
+        uT = (u - dE * (st.L2x @ uA[0]) - dE * (st.L2y @ uA[1]) - dE * (st.L1x @ uA[2]) - dE * (st.L1y @ uA[3]))
+        uT[bnd, :] = 0.0
+        pv = psi_new.reshape(n_cells, -1)
+        u_new = np.zeros_like(u)
+        src = pv[inner] @ Mr.T                       # (MReduced psiNew) per interior cell
+        u_new[inner] = (uT[inner] + dE * Dvec[None, :] * src) / (1.0 + dE * D)[None, :]
+        u_unc = np.zeros(n_cells)
+        u_unc[inner] = pv[inner] @ Mr[0, :]
+        u_new[bnd, :] = 0.0
+        solver.dose += dE * (u_new[:, 0] + u_unc) * solver.csd.SMid[n - 2] / solver.densityVec / (
+            1 + (n == 2 or n == nE))
+        u = u_new
+        psi = psi_new
+    if return_state:
+        return dict(u=u.copy(), psi=psi.copy(), dose=solver.dose.copy(), n_next=last + 1)
+    return 0.5 * math.sqrt(solver.gamma[0]) * u, solver.dose, psi

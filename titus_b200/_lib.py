@@ -40,6 +40,7 @@ class Problem(C.Structure):
         ("x_completion", _ip), ("n_x_completion", C.c_int32),
         ("w_completion", _ip), ("n_w_completion", C.c_int32),
         ("sweep_restore", _ip), ("n_sweep_restore", C.c_int32),
+        ("stopping_mid", _dp),
     ]
 
 
@@ -85,6 +86,9 @@ SIGNATURES = [
                                       C.c_void_p, C.c_char_p, C.c_size_t]),
     ("titus_limited_flux", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("titus_pn_full_solve_device", C.c_int, [C.c_void_p, C.POINTER(Options), C.c_void_p]),
+    ("titus_pn_full_fetch", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    ("titus_pn_full_solve", C.c_int, [C.c_void_p, C.POINTER(Options), _dp, _dp, _dp]),
     ("titus_debug_barrier_fault", C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
     ("titus_debug_fail_alloc", C.c_int, [C.c_int32]),
     ("titus_max_rank", C.c_int, []),

@@ -34,59 +34,32 @@ __device__ __forceinline__ double* sside(const WCtx& x, int s, int off) {
 
 // ------------------------------------------------------------- row kernels ---
 // F[r][fc + d*k + j] = (L_d A)[r0 + r][j]; zero on boundary rows (stencils.jl:26-128).
-// Four elements per thread are gathered before any is combined, so each thread
-// has 20 neighbour loads in flight (the arithmetic per element is unchanged).
 __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0, int nr, int k, double* F, int ldf,
                                  int fc) {
     const DevProblem& P = x.P;
     const double hx = 0.5 / P.dx, hy = 0.5 / P.dy;
     const double ix = 1.0 / P.dx, iy = 1.0 / P.dy;
-    constexpr int SU = 4;
-    const int cnt = nr * k;
-    for (int b = threadIdx.x; b < cnt; b += SU * NT) {
-        double a[SU][5];
-        int cc[SU];
-        bool in[SU];
-#pragma unroll
-        for (int u = 0; u < SU; ++u) {
-            const int e = b + u * NT;
-            const int r = e / k, j = e - r * k;
-            const int c = r0 + r;
-            cc[u] = c;
-            in[u] = e < cnt && !is_bnd_w(P, c);
-            if (in[u]) {
-                const double* p = A + (size_t)c * lda + j;
-                a[u][0] = ldcg(p);
-                a[u][1] = ldcg(p - (size_t)P.ny * lda);
-                a[u][2] = ldcg(p + (size_t)P.ny * lda);
-                a[u][3] = ldcg(p - lda);
-                a[u][4] = ldcg(p + lda);
-            }
+    for (int e = threadIdx.x; e < nr * k; e += NT) {
+        const int r = e / k, j = e - (e / k) * k;
+        const int c = r0 + r;
+        double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
+        if (!is_bnd_w(P, c)) {
+            const double* p = A + (size_t)c * lda + j;
+            const double a0 = ldcg(p) * __ldg(P.rinv + c);
+            const double axm = ldcg(p - (size_t)P.ny * lda) * __ldg(P.rinv + c - P.ny);
+            const double axp = ldcg(p + (size_t)P.ny * lda) * __ldg(P.rinv + c + P.ny);
+            const double aym = ldcg(p - lda) * __ldg(P.rinv + c - 1);
+            const double ayp = ldcg(p + lda) * __ldg(P.rinv + c + 1);
+            l2x = (axp - axm) * hx;
+            l2y = (ayp - aym) * hy;
+            l1x = a0 * ix - hx * axm - hx * axp;
+            l1y = a0 * iy - hy * aym - hy * ayp;
         }
-#pragma unroll
-        for (int u = 0; u < SU; ++u) {
-            const int e = b + u * NT;
-            if (e >= cnt) continue;
-            const int r = e / k, j = e - r * k;
-            const int c = cc[u];
-            double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
-            if (in[u]) {
-                const double a0 = a[u][0] * __ldg(P.rinv + c);
-                const double axm = a[u][1] * __ldg(P.rinv + c - P.ny);
-                const double axp = a[u][2] * __ldg(P.rinv + c + P.ny);
-                const double aym = a[u][3] * __ldg(P.rinv + c - 1);
-                const double ayp = a[u][4] * __ldg(P.rinv + c + 1);
-                l2x = (axp - axm) * hx;
-                l2y = (ayp - aym) * hy;
-                l1x = a0 * ix - hx * axm - hx * axp;
-                l1y = a0 * iy - hy * aym - hy * ayp;
-            }
-            double* row = F + r * ldf + fc;
-            row[0 * k + j] = l2x;
-            row[1 * k + j] = l2y;
-            row[2 * k + j] = l1x;
-            row[3 * k + j] = l1y;
-        }
+        double* row = F + r * ldf + fc;
+        row[0 * k + j] = l2x;
+        row[1 * k + j] = l2y;
+        row[2 * k + j] = l1x;
+        row[3 * k + j] = l1y;
     }
 }
 // F[r][fc + d*k + j] = (A_d B)[r0 + r][j] (sparse P_N operators Ax, Az, |Ax|, |Az|).
@@ -196,23 +169,51 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
         s_cz[l] = P.omega[l * 3 + 2] / P.dy;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < (x.c1 - x.c0) * q; e += NT) {
-        const int c = x.c0 + e / q, kq = e - (e / q) * q;
-        const double pc = ldcg(x.psi_in + (size_t)c * QW + kq);
-        double flux = 0.0;
-        if (!is_bnd_w(P, c)) {
-            const double ox = P.omega[kq * 3 + 0], oz = P.omega[kq * 3 + 2];
-            const double f0 = pc * P.rinv[c];
-            double ew, ns;
-            if (ox >= 0.0) ew = f0 - ldcg(x.psi_in + (size_t)(c - P.ny) * QW + kq) * P.rinv[c - P.ny];
-            else ew = ldcg(x.psi_in + (size_t)(c + P.ny) * QW + kq) * P.rinv[c + P.ny] - f0;
-            if (oz >= 0.0) ns = f0 - ldcg(x.psi_in + (size_t)(c - 1) * QW + kq) * P.rinv[c - 1];
-            else ns = ldcg(x.psi_in + (size_t)(c + 1) * QW + kq) * P.rinv[c + 1] - f0;
-            flux = s_cx[kq] * ew + s_cz[kq] * ns;
+    // four entries per thread: their upwind neighbours are loaded before any is used
+    constexpr int SU = 4;
+    const int cnt = (x.c1 - x.c0) * q;
+    for (int b = threadIdx.x; b < cnt; b += SU * NT) {
+        double pcv[SU], nxv[SU], nyv[SU];
+        int cv[SU], kv[SU], ncx[SU], ncy[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int e = b + u * NT;
+            const int c = x.c0 + e / q, kq = e - (e / q) * q;
+            cv[u] = c;
+            kv[u] = kq;
+            pcv[u] = nxv[u] = nyv[u] = 0.0;
+            ncx[u] = ncy[u] = c;
+            if (e < cnt) {
+                pcv[u] = ldcg(x.psi_in + (size_t)c * QW + kq);
+                if (!is_bnd_w(P, c)) {
+                    ncx[u] = P.omega[kq * 3 + 0] >= 0.0 ? c - P.ny : c + P.ny;
+                    ncy[u] = P.omega[kq * 3 + 2] >= 0.0 ? c - 1 : c + 1;
+                    nxv[u] = ldcg(x.psi_in + (size_t)ncx[u] * QW + kq);
+                    nyv[u] = ldcg(x.psi_in + (size_t)ncy[u] * QW + kq);
+                }
+            }
         }
-        double out = (pc - dE * flux) / den;
-        if (kq == 0 && P.restore[c]) out = pc;
-        x.psi_out[(size_t)c * QW + kq] = out;
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const int e = b + u * NT;
+            if (e >= cnt) continue;
+            const int c = cv[u], kq = kv[u];
+            const double pc = pcv[u];
+            double flux = 0.0;
+            if (!is_bnd_w(P, c)) {
+                const double ox = P.omega[kq * 3 + 0], oz = P.omega[kq * 3 + 2];
+                const double f0 = pc * P.rinv[c];
+                double ew, ns;
+                if (ox >= 0.0) ew = f0 - nxv[u] * P.rinv[ncx[u]];
+                else ew = nxv[u] * P.rinv[ncx[u]] - f0;
+                if (oz >= 0.0) ns = f0 - nyv[u] * P.rinv[ncy[u]];
+                else ns = nyv[u] * P.rinv[ncy[u]] - f0;
+                flux = s_cx[kq] * ew + s_cz[kq] * ns;
+            }
+            double out = (pc - dE * flux) / den;
+            if (kq == 0 && P.restore[c]) out = pc;
+            x.psi_out[(size_t)c * QW + kq] = out;
+        }
     }
 }
 
@@ -322,14 +323,13 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
         wload(T, ldT, 0, x.st.X, KA, 0, r0, nr, k);
         w_stencil(x, x.st.X, KA, r0, nr, k, F, ldF, 0);
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * k; e += NT) {
-            const int r = e / k, j = e - (e / k) * k;
-            double s = 0.0;
-            for (int l = 0; l < k; ++l) s = fma(T[r * ldT + l], sm->S[l * KA + j], s);
-            double t = 0.0;
-            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * ldF + l], ST[l * k + j], t);
-            T[r * ldT + k + j] = s - dE * t;
-        }
+        // K = X S - dE (L_d X) (S C_d) stacked; the two chains of each entry are
+        // formed by the same thread (same micro-tile map in both calls)
+        const double* Sm = sm->S;
+        row_mm<4>(nr, k, k, T, ldT, [&](int l, int j) { return Sm[l * KA + j]; },
+                  [&](int r, int j, double v) { T[r * ldT + k + j] = v; });
+        row_mm<4>(nr, 4 * k, k, F, ldF, [&](int l, int j) { return ST[l * k + j]; },
+                  [&](int r, int j, double v) { T[r * ldT + k + j] = T[r * ldT + k + j] - dE * v; });
         __syncthreads();
         wstore(x.st.K, RA, 0, T, ldT, k, r0, nr, k);
         gram_blocks(acc, T, ldT, nr, bl, 3);
@@ -343,14 +343,12 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
         wload(T, ldT, 0, x.st.W, KA, 0, r0, nr, k);
         w_spmm(x, x.st.W, KA, r0, nr, k, F, ldF, 0);
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * k; e += NT) {
-            const int r = e / k, j = e - (e / k) * k;
-            double s = 0.0;  // (W S^T)[r][j]
-            for (int l = 0; l < k; ++l) s = fma(T[r * ldT + l], sm->S[j * KA + l], s);
-            double t = 0.0;
-            for (int l = 0; l < 4 * k; ++l) t = fma(F[r * ldF + l], ST[l * k + j], t);
-            T[r * ldT + k + j] = s - dE * t;
-        }
+        // L = W S^T - dE (A_d W) (S^T G_d^T) stacked
+        const double* Sm = sm->S;
+        row_mm<4>(nr, k, k, T, ldT, [&](int l, int j) { return Sm[j * KA + l]; },
+                  [&](int r, int j, double v) { T[r * ldT + k + j] = v; });
+        row_mm<4>(nr, 4 * k, k, F, ldF, [&](int l, int j) { return ST[l * k + j]; },
+                  [&](int r, int j, double v) { T[r * ldT + k + j] = T[r * ldT + k + j] - dE * v; });
         __syncthreads();
         wstore(x.st.L, RA, 0, T, ldT, k, r0, nr, k);
         gram_blocks(acc, T, ldT, nr, bw, 3);
@@ -495,12 +493,8 @@ static __device__ __noinline__ void aug_pass(WCtx& x, int s, bool second, double
         wload(F, 2 * RA, 0, sb.A, KA, 0, r0, nr, k);
         wload(F, 2 * RA, k, Bsrc, RA, 0, r0, nr, k);
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * k; e += NT) {
-            const int r = e / k, j = e - (e / k) * k;
-            double t = 0.0;
-            for (int l = 0; l < k; ++l) t = fma(F[r * 2 * RA + l], T[l * RA + j], t);
-            F[r * 2 * RA + k + j] -= t;
-        }
+        row_mm<4>(nr, k, k, F, 2 * RA, [&](int l, int j) { return T[l * RA + j]; },
+                  [&](int r, int j, double v) { F[r * 2 * RA + k + j] -= v; });
         __syncthreads();
         wstore(sb.BP, RA, 0, F, 2 * RA, k, r0, nr, k);
         gram_blocks(acc, F, 2 * RA, nr, &bl, 1);
@@ -566,12 +560,8 @@ static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, d
             __syncthreads();
             w_rsolve(F + k, 2 * RA, M, nr, k);
         } else {
-            for (int e = threadIdx.x; e < nr * w; e += NT) {
-                const int r = e / w, j = e - (e / w) * w;
-                double t = 0.0;
-                for (int l = 0; l < k; ++l) t = fma(F[r * 2 * RA + l], M[l * RA + j], t);
-                F[r * 2 * RA + k + j] = t;
-            }
+            row_mm<4>(nr, k, w, F, 2 * RA, [&](int l, int j) { return M[l * RA + j]; },
+                      [&](int r, int j, double v) { F[r * 2 * RA + k + j] = v; });
         }
         __syncthreads();
         if (mode < 2) wstore(sb.C, RA, 0, F, 2 * RA, k, r0, nr, w);
@@ -806,27 +796,27 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
         if (acc) wload(t, LT, 3 * k, sb.B, RA, 0, r0, nr, k);
         if (rho2 > 0) wload(cb, RA, 0, sb.C, RA, 0, r0, nr, rho2);
         __syncthreads();
-        // Q1 columns (range part A F1, then completion) and X~ range part C RI
+        // Q1 columns: range part A F1, then completion (X side only: the W side has rho1 == k)
+        row_mm<4>(nr, k, rho1, t, LT, [&](int l, int j) { return F1[l * RA + j]; },
+                  [&](int r, int j, double v) { t[r * LT + k + j] = v; });
+        // X~ range part C RI (RI upper triangular: the terms l > j add exact zeros)
+        row_mm<4>(nr, rho2, rho2, cb, RA, [&](int l, int j) { return l <= j ? Ri[l * RA + j] : 0.0; },
+                  [&](int r, int j, double v) { t[r * LT + 2 * k + j] = v; });
         for (int e = threadIdx.x; e < nr * k; e += NT) {
             const int r = e / k, j = e - (e / k) * k;
             const int row = r0 + r;
-            double q1;
-            if (j < rho1) {
-                q1 = 0.0;
-                for (int l = 0; l < k; ++l) q1 = fma(t[r * LT + l], F1[l * RA + j], q1);
-            } else {
-                const int ci = j - rho1;   // X side only (W side has rho1 == k)
-                q1 = (s == 0 && ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
+            if (j >= rho1) {
+                const int ci = j - rho1;
+                t[r * LT + k + j] = (s == 0 && ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
             }
-            t[r * LT + k + j] = q1;
-            double xt = 0.0;
-            if (j < rho2) {
-                for (int l = 0; l <= j; ++l) xt = fma(cb[r * RA + l], Ri[l * RA + j], xt);
-            } else if (s == 0) {
-                const int ci = si.cand0 + (j - rho2);
-                xt = (ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
+            if (j >= rho2) {
+                double xt = 0.0;
+                if (s == 0) {
+                    const int ci = si.cand0 + (j - rho2);
+                    xt = (ci < x.P.nxcomp && row == x.P.xcomp[ci]) ? 1.0 : 0.0;
+                }
+                t[r * LT + 2 * k + j] = xt;
             }
-            t[r * LT + 2 * k + j] = xt;
         }
         __syncthreads();
         if (s == 1 && si.need2 > 0) {
@@ -969,13 +959,9 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
             const int nr = min(tr, r1b - r0);
             wload(t, KA, 0, A, KA, 0, r0, nr, m);
             __syncthreads();
-            for (int e = threadIdx.x; e < nr * kk; e += NT) {
-                const int r = e / kk, j = e - (e / kk) * kk;
-                const double* bj = B + sm->perm[j] * LDS;
-                double a = 0.0;
-                for (int i = 0; i < m; ++i) a = fma(t[r * KA + i], bj[i], a);
-                o[r * KA + j] = a;
-            }
+            const int* perm = sm->perm;
+            row_mm<4>(nr, m, kk, t, KA, [&](int l, int j) { return B[perm[j] * LDS + l]; },
+                      [&](int r, int j, double v) { o[r * KA + j] = v; });
             __syncthreads();
             wstore(A, KA, 0, o, KA, 0, r0, nr, kk);
             __syncthreads();
@@ -1011,14 +997,11 @@ static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig
         const int nr = min(tr, x.m1 - r0);
         wload(t, ldt, 0, x.st.W, KA, 0, r0, nr, k);
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * k; e += NT) {
-            const int r = e / k, j = e - (e / k) * k;
-            double s = 0.0;
-            for (int l = 0; l < k; ++l) s = fma(t[r * ldt + l], sm->S[j * KA + l], s);
-            const int m = r0 + r;
-            const double D = sig[0] - sig[P.lof[m]];
-            t[r * ldt + k + j] = s / (1.0 + P.dE * D);
-        }
+        const double* Sm = sm->S;
+        row_mm<4>(nr, k, k, t, ldt, [&](int l, int j) { return Sm[j * KA + l]; }, [&](int r, int j, double v) {
+            const double D = sig[0] - sig[P.lof[r0 + r]];
+            t[r * ldt + k + j] = v / (1.0 + P.dE * D);
+        });
         __syncthreads();
         wstore(x.st.L, RA, 0, t, ldt, k, r0, nr, k);
         wstore(x.st.LP, RA, 0, t, ldt, k, r0, nr, k);
@@ -1067,12 +1050,8 @@ static __device__ __noinline__ bool w_outscatter_basis(WCtx& x, const double* si
             t[r * ldt + 3 * RA + kq] = P.mred[(size_t)m * P.q + kq] * sig[P.lof[m]];
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * rho; e += NT) {
-            const int r = e / rho, j = e - (e / rho) * rho;
-            double a = 0.0;
-            for (int l = 0; l <= j; ++l) a = fma(t[r * ldt + l], Ri[l * RA + j], a);
-            t[r * ldt + RA + j] = a;
-        }
+        row_mm<4>(nr, rho, rho, t, ldt, [&](int l, int j) { return l <= j ? Ri[l * RA + j] : 0.0; },
+                  [&](int r, int j, double v) { t[r * ldt + RA + j] = v; });
         __syncthreads();
         if (k > rho) {
             for (int r = threadIdx.x; r < nr; r += NT) {
@@ -1160,17 +1139,14 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
         wload(t, ldt, 0, x.st.X, KA, 0, r0, nr, k);
         wload(t, ldt, 2 * RA, x.psi_in, QW, 0, r0, nr, P.q);
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * k; e += NT) {
-            const int r = e / k, j = e - (e / k) * k;
-            double s = 0.0;
-            if (!is_bnd_w(P, r0 + r)) {
-                for (int l = 0; l < k; ++l) s = fma(t[r * ldt + l], sm->S[l * KA + j], s);
-                double a = 0.0;
-                for (int kq = 0; kq < P.q; ++kq) a = fma(t[r * ldt + 2 * RA + kq], Mt[kq * KA + j], a);
-                s += dE * a;
-            }
-            t[r * ldt + k + j] = s;
-        }
+        // K = X S + dE psi MtDW (zero on boundary rows), two chains per entry
+        const double* Sm = sm->S;
+        row_mm<4>(nr, k, k, t, ldt, [&](int l, int j) { return Sm[l * KA + j]; },
+                  [&](int r, int j, double v) { t[r * ldt + k + j] = is_bnd_w(P, r0 + r) ? 0.0 : v; });
+        row_mm<4>(nr, P.q, k, t + 2 * RA, ldt, [&](int l, int j) { return Mt[l * KA + j]; },
+                  [&](int r, int j, double v) {
+                      if (!is_bnd_w(P, r0 + r)) t[r * ldt + k + j] += dE * v;
+                  });
         __syncthreads();
         wstore(x.st.K, RA, 0, t, ldt, k, r0, nr, k);
         gram_blocks(acc, t, ldt, nr, bl, 3);

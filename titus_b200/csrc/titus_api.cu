@@ -40,6 +40,7 @@ int titus_host::fail(int code, const char* fmt, ...) {
 }
 
 titus_solver::~titus_solver() {
+    titus_host::pn_free(this);
     titus_host::wide_free(this);
     for (void* p : allocs) cudaFree(p);
 }
@@ -81,7 +82,8 @@ static int validate(const titus_problem_t* pb) {
                     {pb->bc_space, (size_t)n, "bc_space"},
                     {pb->bc_angle, (size_t)q, "bc_angle"},
                     {pb->omega, (size_t)q * 3, "omega"},
-                    {pb->m_reduced, (size_t)N * q, "m_reduced"}};
+                    {pb->m_reduced, (size_t)N * q, "m_reduced"},
+                    {pb->stopping_mid, pb->stopping_mid ? (size_t)nE - 1 : 0, "stopping_mid"}};
         for (const Arr& a : arrs)
             for (size_t i = 0; i < a.count; ++i)
                 if (!std::isfinite(a.p[i])) return fail(TITUS_ERR_ARG, "%s[%zu] is not finite", a.name, i);
@@ -175,6 +177,7 @@ static int create_impl(const titus_problem_t* pb, titus_solver* s) {
         (rc = s->alloc(&d_xc, pb->n_x_completion, pb->x_completion)) ||
         (rc = s->alloc(&d_wc, pb->n_w_completion, pb->w_completion)))
         return rc;
+    if (pb->stopping_mid && (rc = s->alloc(&s->smid, (size_t)nE - 1, pb->stopping_mid))) return rc;
     P.rinv = d_rinv;
     P.stopping = d_stop;
     P.bc_energy = d_bce;

@@ -9,6 +9,7 @@
 
 struct titus_solver;
 struct titus_batch;
+struct titus_pn_state;
 
 namespace titus_host {
 
@@ -49,6 +50,8 @@ int batch_launch(titus_batch* b, int method, const titus_options_t* opt, cudaStr
 int batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out, int32_t* iters_out);
 void batch_free(titus_batch* b);
 int batch_rank_sums(titus_batch* b, int32_t* out);
+// full-rank P_N solver state (titus_pn_full.cu)
+void pn_free(titus_solver* s);
 int wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots, const titus_spot_t* spots,
                        double* dose_out, int32_t* rank_out, int32_t* iters_out);
 
@@ -79,6 +82,9 @@ struct titus_solver {
     int b_teams = 0, b_G = 0;
     std::vector<void*> batch_allocs;
     int wide_state_valid = 0;   // 1 after an adaptive solve or titus_set_state
+    // full-rank P_N solver (allocated on first use) and csd.SMid
+    titus_pn_state* pn = nullptr;
+    double* smid = nullptr;
     // test hook (titus_debug_barrier_fault), consumed by the next launch
     long long dbg_spin_limit = 0;
     int dbg_fault_barrier = 0;

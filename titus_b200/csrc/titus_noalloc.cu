@@ -17,9 +17,15 @@
 //    with each other, so serialise them (one call at a time per device);
 //  * the array keeps the previous call's contents; everything that must start
 //    at zero is cleared at the start of each call;
-//  * the first call on each device looks the array's device address up
-//    (cudaGetSymbolAddress with that device current) and caches it; make that
-//    first call before any stream capture.
+//  * every call looks the array's device address up with the caller's device
+//    current (cudaGetSymbolAddress; nothing is cached, so concurrent first calls
+//    from several host threads and a cudaDeviceReset between calls are safe);
+//  * the call is synchronous: it reads e_trafo[0..1] back to the host before the
+//    launch and the status words after it, then waits for `stream`, so it cannot
+//    be recorded into a CUDA graph by stream capture;
+//  * a problem fits when 913 n + 580 N + 4 nE + 73 728 G + 48 KiB <= 16 MiB
+//    bytes (n cells, N moments, nE energies, G CTAs; 256-byte alignment of each
+//    piece included in the constant): about 16 700 cells at P21 with G = 16.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -35,13 +41,11 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = 16u << 20;  // 16 MiB per device
 constexpr int kNoAllocMaxTeam = 32;                 // CTAs per solve in this variant
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// device address of g_noalloc_scratch per device (looked up once per device);
-// the host-side symbol itself is only a stand-in and is never passed to a kernel
-unsigned char* g_scratch_addr[kMaxDevices] = {};
+// The host-side symbol g_noalloc_scratch is only a stand-in: kernels get the
+// device address that cudaGetSymbolAddress returns for the current device.
 
 // Error text goes to the caller's buffer (no library-side storage).
 struct ErrOut {
@@ -168,16 +172,12 @@ extern "C" int titus_solve_noalloc(const titus_problem_t* pb, const titus_option
 
     int dev = 0;
     NA_CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return eo.set(TITUS_ERR_LIMIT, "titus_solve_noalloc: device index too large");
-    if (!g_scratch_addr[dev]) {
-        // first call on this device: look up the array's device address with the device current
-        void* addr = nullptr;
-        NA_CK(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
-        if (!addr) return eo.set(TITUS_ERR_CUDA, "titus_solve_noalloc: scratch address lookup returned NULL");
-        NA_CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)sizeof(SmemLayout)));
-        g_scratch_addr[dev] = static_cast<unsigned char*>(addr);
-    }
+    // the array's device address on this device (neither call allocates)
+    void* scratch_addr = nullptr;
+    NA_CK(cudaGetSymbolAddress(&scratch_addr, g_noalloc_scratch));
+    if (!scratch_addr) return eo.set(TITUS_ERR_CUDA, "titus_solve_noalloc: scratch address lookup returned NULL");
+    NA_CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SmemLayout)));
     int num_sms = 0;
     NA_CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
     int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : 16;
@@ -186,7 +186,7 @@ extern "C" int titus_solve_noalloc(const titus_problem_t* pb, const titus_option
 
     const int n = pb->nx * pb->ny, N = pb->n_moments, q = pb->n_ordinates, nE = pb->n_energies;
     // carve the scratch array; reject problems that do not fit
-    Carve cv{g_scratch_addr[dev], 0};
+    Carve cv{static_cast<unsigned char*>(scratch_addr), 0};
     TeamState st{};
     TeamState* d_st = cv.take<TeamState>(1);
     st.X = cv.take<double>((size_t)n * KM);

@@ -244,65 +244,50 @@ __device__ inline void g_zero(double* D, int ldd, int m, int n) {
 }
 
 // ----------------------------------------------------------- row helpers ---
-// Tile moves between global memory (L2, `.cg`: coherent across the team's
-// CTAs) and shared memory. Each thread first issues up to WU loads into
-// registers and only then writes them, so a tile keeps WU x NT loads in flight
-// instead of one load latency per element; with an even column count, offset
-// and leading dimensions the elements move as 16-byte pairs.
-constexpr int WU = 8;
-
+// Tile moves between global memory and shared memory. Loads are asynchronous
+// copies (cp.async): a thread issues every copy of its share of the tile before
+// waiting once, so a tile costs about one memory latency instead of one per
+// element, and the data never passes through registers. Pairs of doubles move
+// as 16-byte copies that bypass L1 (.cg); single doubles use 8-byte copies
+// through L1 (.ca), which is safe because a CTA only loads rows that it wrote
+// itself in this launch (L1 holds no other SM's data for them).
 __device__ __forceinline__ double2 ldcg2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ bool pairs_ok(const double* t, const double* A, int k, int c0, int lda, int ldt, int tc) {
+    return ((k | c0 | lda | ldt | tc) & 1) == 0 &&
+           ((reinterpret_cast<uintptr_t>(t) | reinterpret_cast<uintptr_t>(A)) & 15) == 0;
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// rows [r0, r0+nr) x cols [c0, c0+k) of A (ld lda) -> t (ld ldt) at column tc
+// rows [r0, r0+nr) x cols [c0, c0+k) of A (ld lda) -> t (ld ldt) at column tc.
+// On return this thread's copies have landed; the caller's __syncthreads makes
+// the whole tile visible to the CTA.
 __device__ __forceinline__ void wload(double* t, int ldt, int tc, const double* A, int lda, int c0, int r0, int nr,
                                       int k) {
-    if (((k | c0 | lda | ldt | tc) & 1) == 0 && ((reinterpret_cast<uintptr_t>(t) | reinterpret_cast<uintptr_t>(A)) & 15) == 0) {
-        const int h = k >> 1, cnt = nr * h;
-        for (int b = threadIdx.x; b < cnt; b += WU * NT) {
-            double2 v[WU];
-#pragma unroll
-            for (int u = 0; u < WU; ++u) {
-                const int e = b + u * NT;
-                if (e < cnt) {
-                    const int r = e / h, j = 2 * (e - r * h);
-                    v[u] = ldcg2(A + (size_t)(r0 + r) * lda + c0 + j);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < WU; ++u) {
-                const int e = b + u * NT;
-                if (e < cnt) {
-                    const int r = e / h, j = 2 * (e - r * h);
-                    *reinterpret_cast<double2*>(t + r * ldt + tc + j) = v[u];
-                }
-            }
+    if (pairs_ok(t, A, k, c0, lda, ldt, tc)) {
+        const int h = k >> 1;
+        for (int e = threadIdx.x; e < nr * h; e += NT) {
+            const int r = e / h, j = 2 * (e - r * h);
+            cp_async16(t + r * ldt + tc + j, A + (size_t)(r0 + r) * lda + c0 + j);
         }
-        return;
-    }
-    const int cnt = nr * k;
-    for (int b = threadIdx.x; b < cnt; b += WU * NT) {
-        double v[WU];
-#pragma unroll
-        for (int u = 0; u < WU; ++u) {
-            const int e = b + u * NT;
-            if (e < cnt) {
-                const int r = e / k, j = e - r * k;
-                v[u] = ldcg(A + (size_t)(r0 + r) * lda + c0 + j);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < WU; ++u) {
-            const int e = b + u * NT;
-            if (e < cnt) {
-                const int r = e / k, j = e - r * k;
-                t[r * ldt + tc + j] = v[u];
-            }
+    } else {
+        for (int e = threadIdx.x; e < nr * k; e += NT) {
+            const int r = e / k, j = e - r * k;
+            cp_async8(t + r * ldt + tc + j, A + (size_t)(r0 + r) * lda + c0 + j);
         }
     }
+    cp_async_wait_all();
 }
 __device__ __forceinline__ void wstore(double* A, int lda, int c0, const double* t, int ldt, int tc, int r0, int nr,
                                        int k) {
-    if (((k | c0 | lda | ldt | tc) & 1) == 0 && ((reinterpret_cast<uintptr_t>(t) | reinterpret_cast<uintptr_t>(A)) & 15) == 0) {
+    if (pairs_ok(t, A, k, c0, lda, ldt, tc)) {
         const int h = k >> 1;
         for (int e = threadIdx.x; e < nr * h; e += NT) {
             const int r = e / h, j = 2 * (e - r * h);
@@ -312,8 +297,47 @@ __device__ __forceinline__ void wstore(double* A, int lda, int c0, const double*
         return;
     }
     for (int e = threadIdx.x; e < nr * k; e += NT) {
-        const int r = e / k, j = e - (e / k) * k;
+        const int r = e / k, j = e - r * k;
         A[(size_t)(r0 + r) * lda + c0 + j] = t[r * ldt + tc + j];
+    }
+}
+
+// Row products of a shared-memory tile: for rows r < nr and columns j < w,
+//   epi(r, j, sum_{l < kd} A[r * lda + l] * mget(l, j))
+// with one FMA chain per output in increasing l (the rounding of the plain
+// per-element loop). A thread owns a micro-tile of RB rows x 2 columns: per l it
+// reads RB entries of A and 2 of M for 2 RB independent FMAs, instead of two
+// shared loads per dependent FMA. Threads of a warp share rows (broadcast reads
+// of A) and take adjacent column pairs (consecutive entries of M).
+template <int RB, class MGet, class Epi>
+__device__ __forceinline__ void row_mm(int nr, int kd, int w, const double* A, int lda, MGet mget, Epi epi) {
+    const int cb = (w + 1) >> 1, rbn = (nr + RB - 1) / RB;
+    for (int tile = threadIdx.x; tile < rbn * cb; tile += NT) {
+        const int rb = tile / cb, c2 = tile - rb * cb;
+        const int r0 = rb * RB, j0 = 2 * c2;
+        const bool j1 = j0 + 1 < w;
+        double acc[RB][2];
+#pragma unroll
+        for (int i = 0; i < RB; ++i) acc[i][0] = acc[i][1] = 0.0;
+        const double* ap[RB];
+#pragma unroll
+        for (int i = 0; i < RB; ++i) ap[i] = A + min(r0 + i, nr - 1) * lda;
+        for (int l = 0; l < kd; ++l) {
+            const double m0 = mget(l, j0);
+            const double m1 = j1 ? mget(l, j0 + 1) : 0.0;
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+                const double a = ap[i][l];
+                acc[i][0] = fma(a, m0, acc[i][0]);
+                acc[i][1] = fma(a, m1, acc[i][1]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < RB; ++i)
+            if (r0 + i < nr) {
+                epi(r0 + i, j0, acc[i][0]);
+                if (j1) epi(r0 + i, j0 + 1, acc[i][1]);
+            }
     }
 }
 

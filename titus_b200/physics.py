@@ -167,8 +167,10 @@ def _interp(xt, yt, x):
     return yt[i] * (1.0 - t) + yt[i + 1] * t
 
 
-def energy_grid(settings):
-    """(eGrid, eTrafo, S) of ``CSD(settings)`` (``CSD.jl:47-89``) for analytic S(E)."""
+def energy_grid(settings, with_mid: bool = False):
+    """(eGrid, eTrafo, S) of ``CSD(settings)`` (``CSD.jl:47-89``) for analytic S(E);
+    with ``with_mid`` also SMid, the stopping power at the midpoints of the
+    transformed-energy steps (``CSD.jl:82-89``)."""
     s = settings
     E_tab = np.geomspace(0.5 * s.eMin, 2.0 * s.eMax, 4001)
     S_tab = stopping_power(s.stopping, E_tab)
@@ -191,4 +193,8 @@ def energy_grid(settings):
     eTrafo = np.linspace(0.0, eMaxT - eMinT, nE)
     eGrid = _interp(E_tr, E_tab, eMaxT - eTrafo)
     S = _interp(E_tab, S_tab, eGrid)
-    return eGrid, eTrafo, S
+    if not with_mid:
+        return eGrid, eTrafo, S
+    dE = eTrafo[1:] - eTrafo[:-1]
+    SMid = _interp(E_tab, S_tab, _interp(E_tr, E_tab, eMaxT - (eTrafo[:-1] + 0.5 * dE)))
+    return eGrid, eTrafo, S, SMid

@@ -40,7 +40,7 @@ class SolverCSD:
         self.ops = [ph.to_csr(A) for A in (Ax, Az, ph.roe(Ax), ph.roe(Az))]
         q = npn + 1
         self.Q_points, self.Q_weights, self.O, self.M = ph.quadrature(q, npn)
-        self.eGrid, self.eTrafo, self.S = ph.energy_grid(s)
+        self.eGrid, self.eTrafo, self.S, self.SMid = ph.energy_grid(s, with_mid=True)
         self.nE = self.eTrafo.size
         # separable PsiBeam (SolverCSD.jl:275): angular x spatial x energy factors
         ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - self.Q_points[:, 0]) ** 2) * \
@@ -178,6 +178,7 @@ class SolverCSD:
         p.n_w_completion = self.w_completion.size
         p.sweep_restore = ip(self.sweep_restore)
         p.n_sweep_restore = self.sweep_restore.size
+        p.stopping_mid = dp(self.SMid)
         return p, keep
 
     def handle(self):
@@ -345,6 +346,25 @@ class PencilBeamBatch:
             self.close()
         except Exception:
             pass
+
+
+def SolveFirstCollisionSource(solver: SolverCSD, max_steps: int = 0):
+    """Full-rank P_N first-collision solver (``SolverCSD.jl:465-586``) on the GPU.
+
+    Returns ``(1/2 sqrt(gamma_0) u, dose, psi)`` with u (n x N, row i*ny + j)
+    and psi (nx, ny, q) like the reference.
+    """
+    lib = _lib.load()
+    h = solver.handle()
+    u = np.zeros((solver.n, solver.N))
+    dose = np.zeros(solver.n)
+    psi = np.zeros((solver.n, solver.q))
+    opt = solver.options(max_steps)
+    _lib.check(lib.titus_pn_full_solve(h, C.byref(opt), _lib.as_dp(u), _lib.as_dp(dose), _lib.as_dp(psi)),
+               "titus_pn_full_solve")
+    solver.dose = dose
+    s = solver.settings
+    return 0.5 * math.sqrt(solver.gamma[0]) * u, dose, psi.reshape(s.NCellsX, s.NCellsY, solver.q)
 
 
 def SolveFirstCollisionSourceDLR(solver: SolverCSD, max_steps: int = 0):
