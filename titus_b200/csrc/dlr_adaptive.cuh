@@ -483,21 +483,22 @@ static __device__ __noinline__ void aug_pass(WCtx& x, int s, bool second, double
     const int k = x.r;
     SideBufs sb = side_bufs(x, s);
     double* T = x.sm->work + 2 * RA * RA;        // k x k (ld RA), after the 2k^2 accumulator
-    double* F = T + RA * RA;                     // tr x 2RA: [A | BP]
-    const int tr = rows_fit(WORKD - 3 * RA * RA, 2 * RA);
+    double* F = T + RA * RA;                     // tr x 2k: [A | BP]
+    const int ldF = 2 * k;
+    const int tr = rows_fit(WORKD - 3 * RA * RA, ldF);
     g_copy(T, RA, sside(x, s, SS_T), RA, k, k);
     const GBlock bl = second ? GBlock{k, k, k, k, off} : GBlock{0, k, k, k, off};
     const double* Bsrc = second ? sb.BP : sb.B;
     for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
         const int nr = min(tr, sb.r1 - r0);
-        wload(F, 2 * RA, 0, sb.A, KA, 0, r0, nr, k);
-        wload(F, 2 * RA, k, Bsrc, RA, 0, r0, nr, k);
+        wload(F, ldF, 0, sb.A, KA, 0, r0, nr, k);
+        wload(F, ldF, k, Bsrc, RA, 0, r0, nr, k);
         __syncthreads();
-        row_mm<4>(nr, k, k, F, 2 * RA, [&](int l, int j) { return T[l * RA + j]; },
-                  [&](int r, int j, double v) { F[r * 2 * RA + k + j] -= v; });
+        row_mm<4>(nr, k, k, F, ldF, [&](int l, int j) { return T[l * RA + j]; },
+                  [&](int r, int j, double v) { F[r * ldF + k + j] -= v; });
         __syncthreads();
-        wstore(sb.BP, RA, 0, F, 2 * RA, k, r0, nr, k);
-        gram_blocks(acc, F, 2 * RA, nr, &bl, 1);
+        wstore(sb.BP, RA, 0, F, ldF, k, r0, nr, k);
+        gram_blocks(acc, F, ldF, nr, &bl, 1);
         __syncthreads();
     }
 }
@@ -545,27 +546,28 @@ static __device__ __noinline__ void rf_pass(WCtx& x, int s, int mode, int rho, d
     const int k = x.r;
     SideBufs sb = side_bufs(x, s);
     double* M = x.sm->work + 2 * RA * RA;   // k x k (ld RA), after the 2k^2 accumulator
-    double* F = M + RA * RA;                // tr x 2RA: [BP | out]
-    const int tr = rows_fit(WORKD - 3 * RA * RA, 2 * RA);
+    double* F = M + RA * RA;                // tr x 2k: [BP | out]
+    const int ldF = 2 * k;
+    const int tr = rows_fit(WORKD - 3 * RA * RA, ldF);
     g_copy(M, RA, sside(x, s, mode == 0 ? SS_R0 : (mode == 1 ? SS_T : SS_V0)), RA, k, mode == 1 ? rho : k);
     const int w = (mode == 1) ? rho : k;
     const GBlock bl{k, w, k, w, off};
     for (int r0 = sb.r0; r0 < sb.r1; r0 += tr) {
         const int nr = min(tr, sb.r1 - r0);
-        if (mode == 3) wload(F, 2 * RA, 0, sb.A, KA, 0, r0, nr, k);
-        else wload(F, 2 * RA, 0, sb.BP, RA, 0, r0, nr, k);
+        if (mode == 3) wload(F, ldF, 0, sb.A, KA, 0, r0, nr, k);
+        else wload(F, ldF, 0, sb.BP, RA, 0, r0, nr, k);
         __syncthreads();
         if (mode == 0) {
-            for (int e = threadIdx.x; e < nr * k; e += NT) F[(e / k) * 2 * RA + k + e % k] = F[(e / k) * 2 * RA + e % k];
+            for (int e = threadIdx.x; e < nr * k; e += NT) F[(e / k) * ldF + k + e % k] = F[(e / k) * ldF + e % k];
             __syncthreads();
-            w_rsolve(F + k, 2 * RA, M, nr, k);
+            w_rsolve(F + k, ldF, M, nr, k);
         } else {
-            row_mm<4>(nr, k, w, F, 2 * RA, [&](int l, int j) { return M[l * RA + j]; },
-                      [&](int r, int j, double v) { F[r * 2 * RA + k + j] = v; });
+            row_mm<4>(nr, k, w, F, ldF, [&](int l, int j) { return M[l * RA + j]; },
+                      [&](int r, int j, double v) { F[r * ldF + k + j] = v; });
         }
         __syncthreads();
-        if (mode < 2) wstore(sb.C, RA, 0, F, 2 * RA, k, r0, nr, w);
-        gram_blocks(acc, F, 2 * RA, nr, &bl, 1);
+        if (mode < 2) wstore(sb.C, RA, 0, F, ldF, k, r0, nr, w);
+        gram_blocks(acc, F, ldF, nr, &bl, 1);
         __syncthreads();
     }
 }
@@ -779,12 +781,13 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
     WSmem* sm = x.sm;
     SideBufs sb = side_bufs(x, s);
     const SideInfo& si = x.side[s];
-    constexpr int LT = 4 * RA;               // tile leading dimension
+    const int LT = 4 * k;                    // tile leading dimension
+    const int LC = k + (k & 1);              // C-row leading dimension (even: 16-byte rows)
     double* F1 = sm->work + 2 * RA * RA;     // k x k (after the 2k^2 accumulator)
     double* Ri = F1 + RA * RA;               // rho2 x rho2
-    const int tr = rows_fit(WORKD - 4 * RA * RA, LT + RA);
-    double* t = Ri + RA * RA;                // tr x 4RA
-    double* cb = t + tr * LT;                // tr x RA (C rows)
+    const int tr = rows_fit(WORKD - 4 * RA * RA, LT + LC);
+    double* t = Ri + RA * RA;                // tr x 4k
+    double* cb = t + tr * LT;                // tr x LC (C rows)
     const GBlock blk = s == 0 ? GBlock{2 * k, k, 3 * k, k, 0} : GBlock{3 * k, k, 2 * k, k, k * k};
     g_copy(F1, RA, sside(x, s, SS_F1), RA, k, k);
     if (si.rho2 > 0) g_copy(Ri, RA, sside(x, s, SS_RI), RA, si.rho2, si.rho2);
@@ -794,13 +797,13 @@ static __device__ __noinline__ void materialize_side(WCtx& x, int s, bool with_q
         const int nr = min(tr, sb.r1 - r0);
         wload(t, LT, 0, sb.A, KA, 0, r0, nr, k);
         if (acc) wload(t, LT, 3 * k, sb.B, RA, 0, r0, nr, k);
-        if (rho2 > 0) wload(cb, RA, 0, sb.C, RA, 0, r0, nr, rho2);
+        if (rho2 > 0) wload(cb, LC, 0, sb.C, RA, 0, r0, nr, rho2);
         __syncthreads();
         // Q1 columns: range part A F1, then completion (X side only: the W side has rho1 == k)
         row_mm<4>(nr, k, rho1, t, LT, [&](int l, int j) { return F1[l * RA + j]; },
                   [&](int r, int j, double v) { t[r * LT + k + j] = v; });
         // X~ range part C RI (RI upper triangular: the terms l > j add exact zeros)
-        row_mm<4>(nr, rho2, rho2, cb, RA, [&](int l, int j) { return l <= j ? Ri[l * RA + j] : 0.0; },
+        row_mm<4>(nr, rho2, rho2, cb, LC, [&](int l, int j) { return l <= j ? Ri[l * RA + j] : 0.0; },
                   [&](int r, int j, double v) { t[r * LT + 2 * k + j] = v; });
         for (int e = threadIdx.x; e < nr * k; e += NT) {
             const int r = e / k, j = e - (e / k) * k;
@@ -939,9 +942,10 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
     WSmem* sm = x.sm;
     const double* Ut = sm->work;
     const double* Vt = sm->work + KA * LDS;
-    const int tr = rows_fit(WORKD - 2 * KA * LDS, 2 * KA);
-    double* t = sm->work + 2 * KA * LDS;    // tr x KA
-    double* o = t + tr * KA;                // tr x KA
+    const int ldt = m;                      // m = 2k, even: 16-byte rows
+    const int tr = rows_fit(WORKD - 2 * KA * LDS, 2 * ldt);
+    double* t = sm->work + 2 * KA * LDS;    // tr x m
+    double* o = t + tr * ldt;               // tr x m
     double* v = sm->vec;                    // diag(sig) W_new[0,:]^T
     if (dose_sidx >= 0) {
         for (int j = threadIdx.x; j < kk; j += NT) {
@@ -957,13 +961,13 @@ static __device__ __noinline__ void w_truncate_apply(WCtx& x, int m, int kk, int
         const int r0b = side == 0 ? x.c0 : x.m0, r1b = side == 0 ? x.c1 : x.m1;
         for (int r0 = r0b; r0 < r1b; r0 += tr) {
             const int nr = min(tr, r1b - r0);
-            wload(t, KA, 0, A, KA, 0, r0, nr, m);
+            wload(t, ldt, 0, A, KA, 0, r0, nr, m);
             __syncthreads();
             const int* perm = sm->perm;
-            row_mm<4>(nr, m, kk, t, KA, [&](int l, int j) { return B[perm[j] * LDS + l]; },
-                      [&](int r, int j, double v) { o[r * KA + j] = v; });
+            row_mm<4>(nr, m, kk, t, ldt, [&](int l, int j) { return B[perm[j] * LDS + l]; },
+                      [&](int r, int j, double v) { o[r * ldt + j] = v; });
             __syncthreads();
-            wstore(A, KA, 0, o, KA, 0, r0, nr, kk);
+            wstore(A, KA, 0, o, ldt, 0, r0, nr, kk);
             __syncthreads();
         }
     }
@@ -987,10 +991,11 @@ static __device__ __noinline__ bool w_outscatter_pass(WCtx& x, const double* sig
     const DevProblem& P = x.P;
     WSmem* sm = x.sm;
     double* acc = sm->work;
-    const int ldt = KA + QW;
+    int ldt = max(2 * k, k + P.q);
+    ldt += ldt & 1;                             // even: 16-byte rows
     const int tstart = 2 * RA * RA + RA * QW;   // after the largest accumulator
     const int tr = rows_fit(WORKD - tstart, ldt);
-    double* t = sm->work + tstart;   // tr x (KA + QW)
+    double* t = sm->work + tstart;   // tr x ldt: W side [W | L], X side [X | psi]
     w_acc_zero(acc, 2 * k * k + k * P.q);
     const GBlock bl{k, k, k, k, k * k};
     for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
@@ -1106,8 +1111,8 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
     double* acc = sm->work;                   // 6 k^2
     double* Mt = sm->work + 6 * RA * RA;      // q x k MtDW (ld KA)
     double* Xp = Mt + QW * KA;                // k x q Xtpsi (ld QW)
-    double* t = Xp + KA * QW;                 // tr x (2RA + QW)
-    const int ldt = 2 * RA + QW;
+    double* t = Xp + KA * QW;                 // tr x ldt: X side [X | K | psi], W side [W | L]
+    const int ldt = 2 * k + P.q + ((2 * k + P.q) & 1);
     const int tr = rows_fit(WORKD - (6 * RA * RA + 2 * KA * QW), ldt);
     g_copy(Mt, KA, x.scr + SO_MTDW, KA, P.q, k);
     g_copy(Xp, QW, x.scr + SO_XTPSI, QW, k, P.q);
@@ -1137,13 +1142,13 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
     for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
         const int nr = min(tr, x.c1 - r0);
         wload(t, ldt, 0, x.st.X, KA, 0, r0, nr, k);
-        wload(t, ldt, 2 * RA, x.psi_in, QW, 0, r0, nr, P.q);
+        wload(t, ldt, 2 * k, x.psi_in, QW, 0, r0, nr, P.q);
         __syncthreads();
         // K = X S + dE psi MtDW (zero on boundary rows), two chains per entry
         const double* Sm = sm->S;
         row_mm<4>(nr, k, k, t, ldt, [&](int l, int j) { return Sm[l * KA + j]; },
                   [&](int r, int j, double v) { t[r * ldt + k + j] = is_bnd_w(P, r0 + r) ? 0.0 : v; });
-        row_mm<4>(nr, P.q, k, t + 2 * RA, ldt, [&](int l, int j) { return Mt[l * KA + j]; },
+        row_mm<4>(nr, P.q, k, t + 2 * k, ldt, [&](int l, int j) { return Mt[l * KA + j]; },
                   [&](int r, int j, double v) {
                       if (!is_bnd_w(P, r0 + r)) t[r * ldt + k + j] += dE * v;
                   });
@@ -1412,29 +1417,29 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 if (!augment(x, true, false)) { aborted = true; break; }
                 // Grams X1^T psi (m x q) and MRed^T D W1 (q x m) over the new bases
                 double* acc = sm->work;
-                const int ldt = KA + QW;
+                const int ldt = m + P.q + (P.q & 1);     // [X1 | psi] or [W1 | MRed D]; m even
                 const int tstart = 2 * KA * QW + KA;   // after the largest accumulator
                 const int tr = rows_fit(WORKD - tstart, ldt);
                 double* tt = sm->work + tstart;
                 w_acc_zero(acc, 2 * m * P.q + m);
-                const GBlock bx{0, m, KA, P.q, 0};
+                const GBlock bx{0, m, m, P.q, 0};
                 for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
                     const int nr = min(tr, x.c1 - r0);
                     // own rows of X1 were just written by this CTA
                     wload(tt, ldt, 0, x.st.X, KA, 0, r0, nr, m);
-                    wload(tt, ldt, KA, x.psi_in, QW, 0, r0, nr, P.q);
+                    wload(tt, ldt, m, x.psi_in, QW, 0, r0, nr, P.q);
                     __syncthreads();
                     gram_blocks(acc, tt, ldt, nr, &bx, 1);
                     __syncthreads();
                 }
-                const GBlock bw{KA, P.q, 0, m, m * P.q};
+                const GBlock bw{m, P.q, 0, m, m * P.q};
                 for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
                     const int nr = min(tr, x.m1 - r0);
                     wload(tt, ldt, 0, x.st.W, KA, 0, r0, nr, m);
                     for (int e = threadIdx.x; e < nr * P.q; e += NT) {
                         const int r = e / P.q, kq = e - (e / P.q) * P.q;
                         const int mo = r0 + r;
-                        tt[r * ldt + KA + kq] = P.mred[(size_t)mo * P.q + kq] * sig[P.lof[mo]];
+                        tt[r * ldt + m + kq] = P.mred[(size_t)mo * P.q + kq] * sig[P.lof[mo]];
                     }
                     __syncthreads();
                     gram_blocks(acc, tt, ldt, nr, &bw, 1);

@@ -43,60 +43,20 @@ static __device__ __noinline__ double w_chol(const double* G, int ldg, double* R
     }
     if (threadIdx.x == 0) s_ok = 1;
     __syncthreads();
-    if (k <= 32) {
-        // Right-looking factorisation on warp 0 in registers: lane l keeps column
-        // l of R (entries a <= l) and row j travels by shuffles. Same operations
-        // as the CTA-wide loop below (division by the pivot, one fma per update),
-        // so R is bitwise the same; no barrier per column.
-        if (threadIdx.x < 32) {
-            const unsigned FULL = 0xffffffffu;
-            const int lane = threadIdx.x;
-            double col[32];
-#pragma unroll
-            for (int a = 0; a < 32; ++a) col[a] = (lane < k && a < k && a <= lane) ? R[a * ld + lane] : 0.0;
-            bool ok = true;
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                if (j < k) {
-                    const double d = __shfl_sync(FULL, col[j], j);
-                    const bool okp = d > 0.0;
-                    ok = ok && okp;
-                    const double piv = okp ? sqrt(d) : 1.0;
-                    if (lane == j) col[j] = piv;
-                    else if (lane > j) col[j] = col[j] / piv;
-#pragma unroll
-                    for (int i = j + 1; i < 32; ++i) {
-                        if (i < k) {
-                            const double rji = __shfl_sync(FULL, col[j], i);
-                            if (lane >= i) col[i] = fma(-rji, col[j], col[i]);
-                        }
-                    }
-                }
-            }
-            if (lane < k) {
-#pragma unroll
-                for (int a = 0; a < 32; ++a)
-                    if (a < k) R[a * ld + lane] = a <= lane ? col[a] : 0.0;
-            }
-            if (lane == 0 && !ok) s_ok = 0;
+    for (int j = 0; j < k; ++j) {
+        const double d = R[j * ld + j];
+        const bool okp = d > 0.0;
+        const double piv = okp ? sqrt(d) : 1.0;
+        __syncthreads();
+        for (int l = j + threadIdx.x; l < k; l += NT) R[j * ld + l] = (l == j) ? piv : R[j * ld + l] / piv;
+        if (!okp && threadIdx.x == 0) s_ok = 0;
+        __syncthreads();
+        const int m = k - j - 1;
+        for (int e = threadIdx.x; e < m * m; e += NT) {
+            const int i = j + 1 + e / m, l = j + 1 + (e - (e / m) * m);
+            if (l >= i) R[i * ld + l] = fma(-R[j * ld + i], R[j * ld + l], R[i * ld + l]);
         }
         __syncthreads();
-    } else {
-        for (int j = 0; j < k; ++j) {
-            const double d = R[j * ld + j];
-            const bool okp = d > 0.0;
-            const double piv = okp ? sqrt(d) : 1.0;
-            __syncthreads();
-            for (int l = j + threadIdx.x; l < k; l += NT) R[j * ld + l] = (l == j) ? piv : R[j * ld + l] / piv;
-            if (!okp && threadIdx.x == 0) s_ok = 0;
-            __syncthreads();
-            const int m = k - j - 1;
-            for (int e = threadIdx.x; e < m * m; e += NT) {
-                const int i = j + 1 + e / m, l = j + 1 + (e - (e / m) * m);
-                if (l >= i) R[i * ld + l] = fma(-R[j * ld + i], R[j * ld + l], R[i * ld + l]);
-            }
-            __syncthreads();
-        }
     }
     // R^{-1}: warp w solves columns c = w, w+8, ...; lanes split each dot product
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -168,26 +128,12 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
     }
     __syncthreads();
     const double afloor = s_floor;
-    // k <= 16 (at most 8 pairs): warp 0 alone runs the sweeps with warp
-    // barriers; every entry is computed by the same formula as with the whole
-    // CTA, so the result does not depend on which threads run it
-    const bool solo = k <= 16;
-    const int nthr = solo ? 32 : NT;
-    auto sync = [&]() {
-        if (solo) __syncwarp();
-        else __syncthreads();
-    };
-    __shared__ int s_conv, s_nsw;
-    if (threadIdx.x == 0) {
-        s_conv = 0;
-        s_nsw = 60;
-    }
-    __syncthreads();
-    if (!solo || threadIdx.x < 32)
+    bool conv = false;
+    int nsw = 60;
     for (int sweep = 0; sweep < 60; ++sweep) {
         const int par = sweep & 1;
         if (threadIdx.x == 0) s_rot[par] = 0;
-        sync();
+        __syncthreads();
         for (int t = 0; t < m - 1; ++t) {
             if (threadIdx.x < npairs) {
                 int p, q;
@@ -221,13 +167,13 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                 rp[threadIdx.x] = p;
                 rq[threadIdx.x] = q;
             }
-            sync();
+            __syncthreads();
             // Both rotations at once: the thread owning rows {p_a, q_a} x columns
             // {p_b, q_b} reads the four entries, rotates the rows by pair a and the
             // columns by pair b (the order of the two one-sided passes) and writes
             // them back; no other thread touches them, so one barrier suffices.
             // A rotated diagonal block takes the closed form.
-            for (int e = threadIdx.x; e < npairs * npairs; e += nthr) {
+            for (int e = threadIdx.x; e < npairs * npairs; e += NT) {
                 const int a = e / npairs, b = e - (e / npairs) * npairs;
                 const double sa = rs[a], sb = rs[b];
                 if (sa == 0.0 && sb == 0.0) continue;
@@ -253,7 +199,7 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                     if (qb >= 0) A[qa * ld + qb] = sb * rqp + cb * rqq;
                 }
             }
-            for (int e = threadIdx.x; e < npairs * k; e += nthr) {
+            for (int e = threadIdx.x; e < npairs * k; e += NT) {
                 const int b = e / k, i = e - (e / k) * k;
                 const double sb = rs[b];
                 if (sb == 0.0) continue;
@@ -263,19 +209,14 @@ static __device__ __noinline__ int w_eig(double* A, double* V, int ld, double* l
                 V[i * ld + pb] = cb * vp - sb * vq;
                 V[i * ld + qb] = sb * vp + cb * vq;
             }
-            sync();
+            __syncthreads();
         }
         if (!s_rot[par]) {
-            if (threadIdx.x == 0) {
-                s_conv = 1;
-                s_nsw = sweep + 1;
-            }
+            conv = true;
+            nsw = sweep + 1;
             break;
         }
     }
-    __syncthreads();
-    const bool conv = s_conv != 0;
-    const int nsw = s_nsw;
     if (!conv && threadIdx.x == 0) set_status(status, ST_JACOBI);
     __syncthreads();
     for (int i = threadIdx.x; i < k; i += NT) s_lam[i] = A[i * ld + i];
@@ -328,61 +269,7 @@ static __device__ __noinline__ int w_svd(double* At, double* Vt, int ld, int m, 
     }
     __syncthreads();
     const double nfloor = 1e-32 * s_fro;
-    if (m > 1 && m <= 32) {
-        // one warp, no CTA barrier per round: LP lanes per pair (npairs <= 16),
-        // rounds separated by __syncwarp; the other warps wait at the end
-        __shared__ int s_sweeps;
-        if (warp == 0) {
-            const int mm = m + (m & 1);
-            const int npairs = mm / 2;
-            const int LP = npairs <= 2 ? 16 : (npairs <= 4 ? 8 : (npairs <= 8 ? 4 : 2));
-            const int grp = lane / LP, gl = lane % LP;
-            int sw = -1;
-            for (int sweep = 0; sweep < 60; ++sweep) {
-                bool rotated = false;
-                for (int t = 0; t < mm - 1; ++t) {
-                    int p = 0, q = 0;
-                    const bool valid = grp < npairs && rr_pair(mm, t, grp, m, p, q);
-                    double a = 0.0, bq = 0.0, g = 0.0;
-                    if (valid)
-                        for (int i = gl; i < m; i += LP) {
-                            const double u = At[p * ld + i], v = At[q * ld + i];
-                            a = fma(u, u, a);
-                            bq = fma(v, v, bq);
-                            g = fma(u, v, g);
-                        }
-                    for (int o = LP / 2; o > 0; o >>= 1) {
-                        a += __shfl_xor_sync(0xffffffffu, a, o);
-                        bq += __shfl_xor_sync(0xffffffffu, bq, o);
-                        g += __shfl_xor_sync(0xffffffffu, g, o);
-                    }
-                    if (valid && g != 0.0 && fmin(a, bq) > nfloor && g * g > ctol * ctol * a * bq &&
-                        fabs(g) > 2.2e-16 * fmax(a, bq)) {
-                        const double d = bq - a;
-                        const double tt = 2.0 * g * copysign(1.0, d) / (fabs(d) + sqrt(fma(d, d, 4.0 * g * g)));
-                        const double c = rsqrt(fma(tt, tt, 1.0)), sn = c * tt;
-                        for (int i = gl; i < m; i += LP) {
-                            const double u = At[p * ld + i], v = At[q * ld + i];
-                            At[p * ld + i] = c * u - sn * v;
-                            At[q * ld + i] = sn * u + c * v;
-                            const double vu = Vt[p * ld + i], vv = Vt[q * ld + i];
-                            Vt[p * ld + i] = c * vu - sn * vv;
-                            Vt[q * ld + i] = sn * vu + c * vv;
-                        }
-                        rotated = true;
-                    }
-                    __syncwarp();
-                }
-                if (!__any_sync(0xffffffffu, rotated)) {
-                    sw = sweep + 1;
-                    break;
-                }
-            }
-            if (lane == 0) s_sweeps = sw;
-        }
-        __syncthreads();
-        sweeps = s_sweeps;
-    } else if (m > 1) {
+    if (m > 1) {
         const int mm = m + (m & 1);
         const int npairs = mm / 2;
         // LP lanes per pair (8 / 16 / 32), PPW = 32 / LP pairs per warp
