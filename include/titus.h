@@ -30,10 +30,15 @@ extern "C" {
 
 /* Integrators: SolverCSD.jl SolveFirstCollisionSourceDLR (:891-1120),
  * SolveFirstCollisionSourceDLRParallel (:1726-2008),
- * SolveFirstCollisionSourceDLRBUGRejection (:2011-2374). */
+ * SolveFirstCollisionSourceDLRBUGRejection (:2011-2374),
+ * SolveFirstCollisionSourceDLRHighOrder (:588-889: fixed rank, inflow on the
+ * two outer layers, second-order limited sweep, RK4 K/L/S streaming with the
+ * central operators; the reference never allocates its KUP buffer, this one
+ * does). TITUS_DLR_HIGH_ORDER needs nx, ny >= 5. */
 #define TITUS_DLR_FIXED 0
 #define TITUS_PARALLEL_ADAPTIVE 1
 #define TITUS_BUG_ADAPTIVE 2
+#define TITUS_DLR_HIGH_ORDER 3
 
 /* Assembled problem. Replaces the fields of `SolverCSD{T}` that the energy
  * loop reads (SolverCSD.jl:20-146) plus the per-step tables the loop derives
@@ -73,11 +78,22 @@ typedef struct titus_problem {
                                       read by the full-rank P_N solver only, may be NULL otherwise */
 } titus_problem_t;
 
+/* Arithmetic of the energy loop. FP64: every product in FP64 (the plain
+ * mode, parity with the FP64 restatement of the reference). MIXED: the
+ * operator Grams X^T L_d X and W^T A_d W of the rank-adaptive integrators
+ * (streaming and S-step, SolverCSD.jl:1856-1859, :2187-2199) run on the
+ * tensor cores in TF32 with a hi/lo split of each FP64 input and FP32
+ * accumulation wherever the basis width is >= 32; the QR / range finders, the
+ * truncation SVD, the small algebra and the dose stay FP64. MIXED applies to
+ * TITUS_PARALLEL_ADAPTIVE and TITUS_BUG_ADAPTIVE (plain and batched). */
+typedef enum titus_precision { TITUS_PRECISION_FP64 = 0, TITUS_PRECISION_MIXED = 1 } titus_precision_t;
+
 typedef struct titus_options {
     int32_t team_ctas;     /* CTAs cooperating on one solve (0 = library default) */
     int32_t max_steps;     /* stop after this many loop iterations (0 = full sweep) */
     double rank_tol;       /* relative singular-value cut for numerical rank (0 = 1e-12) */
     int32_t profile;       /* 1 = record per-phase device timers (read with titus_profile) */
+    int32_t precision;     /* a titus_precision_t value; 0 = FP64 */
 } titus_options_t;
 
 /* Host result buffers (caller-owned). Factors are returned raw: X (n x r_cap),
@@ -272,6 +288,13 @@ int titus_pn_full_solve(titus_solver_t* solver, const titus_options_t* options, 
  * fails as if cudaMalloc had returned cudaErrorMemoryAllocation; 0 = off. */
 int titus_debug_barrier_fault(titus_solver_t* solver, int32_t barrier, int64_t spin_limit);
 int titus_debug_fail_alloc(int32_t after);
+/* titus_debug_tc_gram: the MIXED mode's tensor-core Gram run on host data, for
+ * the unit test of its layouts. F (rows x (nops+1) nw, row-major) holds A in
+ * columns [0, nw) and nops operator images O_d A after it; out (nops x nw x nw)
+ * receives out[d][i][j] = sum_r (O_d A)[r][i] A[r][j], formed as the adaptive
+ * kernel forms it (hi/lo TF32 operands, tcgen05 MMAs, FP32 accumulation in
+ * TMEM). nw <= 80, nops in {1, 2, 4}. */
+int titus_debug_tc_gram(const double* F, int32_t rows, int32_t nw, int32_t nops, double* out);
 
 /* Build / capability queries. */
 int titus_max_rank(void);        /* largest settings.r accepted (adaptive rank cap) */

@@ -84,3 +84,91 @@ def solve_pn_full(solver: SolverCSD, max_steps: int | None = None, state: dict |
     if return_state:
         return dict(u=u.copy(), psi=psi.copy(), dose=solver.dose.copy(), n_next=last + 1)
     return 0.5 * math.sqrt(solver.gamma[0]) * u, solver.dose, psi
+
+
+def _pn_step_pieces(solver: SolverCSD, n: int):
+    """Per-step constants of ``solve_pn_full``'s step n: (dE_n, D, Dvec, c_n)
+    with c_n = dE SMid[n-1] / (1 + (n == 2 or n == nE)) the dose weight."""
+    eTrafo = solver.csd.eTrafo
+    nE = eTrafo.size
+    _, Dvec, D = sigma_vectors(solver, n)
+    dE = eTrafo[n - 1] - eTrafo[n - 2]
+    c = dE * solver.csd.SMid[n - 2] / (1 + (n == 2 or n == nE))
+    return dE, D, Dvec, c
+
+
+def pn_full_dose_adjoint(solver: SolverCSD, g, max_steps: int | None = None):
+    """Discrete adjoint of ``solve_pn_full``'s dose, density gradient.
+
+    For a dose objective J with dJ/d(dose) = g (n cells) this returns
+    (dose, dJ/drho) with rho the cell densities, at a fixed energy grid (the
+    tau step follows min(rho) when Settings is built and stays fixed here) and
+    a fixed PsiBeam scale (densityMin is a setting). It is the exact transpose
+    of the forward recursion, run from the last energy step back to the first:
+
+    * forward step n: V_d = u A_d, uT = u - dE sum_d L_d V_d with the stencils
+      L_d = Ltilde_d diag(1/rho) (stencils.jl: every entry carries 1/rho of its
+      column cell), boundary rows zero, u' = P_int (uT + src) / (1 + dE D),
+      dose += c_n (u'[:,0] + uOUnc) / rho; psi does not depend on rho or u;
+    * backward: lambda (adjoint of u') gets g c_n / rho in its moment 0;
+      mu = P_int lambda / (1 + dE D); Y_d = L_d^T mu;
+      dJ/drho += (dE / rho) sum_d rowsum(Y_d * V_d);
+      lambda <- mu - dE sum_d Y_d A_d^T (the adjoint of the previous u);
+    * the explicit 1/rho of the dose adds -g dose / rho.
+
+    The oracle keeps every step's V_d in memory, so it is for small cases
+    (the GPU path checkpoints u and recomputes). TEST INFRASTRUCTURE ONLY.
+    """
+    s = solver.settings
+    eTrafo = solver.csd.eTrafo
+    energy = solver.csd.eGrid
+    nx, ny = s.NCellsX, s.NCellsY
+    n_cells = nx * ny
+    N = solver.N
+    psi = solver.setup_directions()
+    Mr = solver.MReduced
+    nE = eTrafo.size
+    u = np.zeros((n_cells, N))
+    st = solver.stencil
+    ops = (solver.Ax, solver.Az, solver.AbsAx, solver.AbsAz)
+    Ls = (st.L2x, st.L2y, st.L1x, st.L1y)
+    bnd = solver.boundaryIdx
+    inner = np.zeros((nx, ny), dtype=bool)
+    inner[1:-1, 1:-1] = True
+    inner = inner.ravel()
+    rho = solver.densityVec
+    dose = np.zeros(n_cells)
+    last = nE if max_steps is None else min(nE, 1 + max_steps)
+    V_hist = {}
+    for n in range(2, last + 1):
+        sig, Dvec, D = sigma_vectors(solver, n)
+        dE = eTrafo[n - 1] - eTrafo[n - 2]
+        solver.apply_bc(psi, energy[n - 1], n - 1)
+        psi = psi - dE * solver.flux_upwind(psi)
+        psi_new = psi / (1.0 + dE * sig[0])
+        V = [np.asarray((A.T @ u.T).T) for A in ops]
+        V_hist[n] = V
+        uT = u - dE * sum(L @ Vd for L, Vd in zip(Ls, V))
+        uT[bnd, :] = 0.0
+        pv = psi_new.reshape(n_cells, -1)
+        u_new = np.zeros_like(u)
+        u_new[inner] = (uT[inner] + dE * Dvec[None, :] * (pv[inner] @ Mr.T)) / (1.0 + dE * D)[None, :]
+        u_unc = np.zeros(n_cells)
+        u_unc[inner] = pv[inner] @ Mr[0, :]
+        _, _, _, c = _pn_step_pieces(solver, n)
+        dose += c * (u_new[:, 0] + u_unc) / rho
+        u = u_new
+        psi = psi_new
+    g = np.asarray(g, dtype=np.float64)
+    lam = np.zeros((n_cells, N))
+    grad = np.zeros(n_cells)
+    for n in range(last, 1, -1):
+        dE, D, _, c = _pn_step_pieces(solver, n)
+        lam[:, 0] += g * c / rho
+        mu = lam / (1.0 + dE * D)[None, :]
+        mu[~inner, :] = 0.0
+        Y = [np.asarray(L.T @ mu) for L in Ls]
+        grad += (dE / rho) * sum(np.sum(Yd * Vd, axis=1) for Yd, Vd in zip(Y, V_hist[n]))
+        lam = mu - dE * sum(np.asarray((A @ Yd.T).T) for A, Yd in zip(ops, Y))
+    grad += -g * dose / rho
+    return dose, grad

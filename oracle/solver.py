@@ -158,6 +158,32 @@ class SolverCSD:
         psi[...] = (psi - dE * flux) / (1 + dE * sigma0)
         psi[a, b, 0] = psiBC
 
+    def apply_bc_two_layer(self, psi, E, n):
+        """Boundary inflow of ``SolveFirstCollisionSourceDLRHighOrder``
+        (``SolverCSD.jl:679-695``): the two outer layers on every side, the
+        second layer taking the coordinates of the first. The x-sides (first
+        index) are written last, so they win at the corners."""
+        s = self.settings
+        xm, ym = s.xMid, s.yMid
+        Om = self.qReduced
+        for jj, yy in ((0, ym[0]), (-1, ym[-1]), (1, ym[0]), (-2, ym[-1])):
+            psi[:, jj, :] = self.psi_beam(Om, E, xm[:, None], yy, n)
+        for ii, xx in ((0, xm[0]), (-1, xm[-1]), (1, xm[0]), (-2, xm[-1])):
+            psi[ii, :, :] = self.psi_beam(Om, E, xx, ym[:, None], n)
+
+    def sweep_limited(self, psi, dE, sigma0):
+        """Uncollided update of the HighOrder loop (``SolverCSD.jl:707-713``):
+        the second-order limited flux ``solveFlux!`` of psi/rho, which writes
+        interior cells 3:N-2 only (the flux buffer keeps zeros on the two outer
+        rings), then the same boundary-slab restore as ``sweep``."""
+        nx = self.settings.NCellsX
+        flux = self.flux_limited(psi / self.density[:, :, None])
+        L0 = self.boundaryIdx
+        a, b = L0 % nx, L0 // nx
+        psiBC = psi[a, b, 0].copy()
+        psi[...] = (psi - dE * flux) / (1 + dE * sigma0)
+        psi[a, b, 0] = psiBC
+
     def dvec(self, sigma):
         s = self.settings
         Dv = np.zeros(self.N)
@@ -239,6 +265,39 @@ def init_factors(solver, r):
     return X, S, W
 
 
+def _fixed_scatter(solver, X, S, W, psi, Dvec, D, dE):
+    """Out-scattering and the in-scattering K/L/S steps of the fixed-rank loops
+    (``SolverCSD.jl:1066-1102``; the HighOrder loop repeats them at ``:768-808``).
+    X's boundary rows are zeroed in place, as the reference does."""
+    s = solver.settings
+    mode = solver.basis_mode
+    bnd = solver.boundaryIdx
+    Mr = solver.MReduced
+    # out scattering
+    L = W @ S.T
+    L = L / (1.0 + dE * D)[:, None]
+    W, S = out_scatter_factor(L, mode, solver.w_completion)
+    # in scattering, K-step
+    X[bnd, :] = 0.0
+    K = X @ S
+    psiv = psi.reshape(s.NCellsX * s.NCellsY, -1)
+    K = K + dE * psiv @ (Mr.T @ (Dvec[:, None] * W))
+    K[bnd, :] = 0.0
+    XNew = la.orth(K, mode, order=solver.x_completion)
+    MUp = XNew.T @ X
+    # L-step
+    L = W @ S.T
+    L = L + dE * Dvec[:, None] * (Mr @ (psiv.T @ X))
+    WNew = la.orth(L, mode, order=solver.w_completion)
+    NUp = WNew.T @ W
+    W = WNew
+    X = XNew
+    # S-step
+    S = MUp @ S @ NUp.T
+    S = S + dE * (X.T @ psiv) @ Mr.T @ (Dvec[:, None] * W)
+    return X, S, W
+
+
 def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
                     n_begin: int = 2, return_state: bool = False):
     """``SolveFirstCollisionSourceDLR`` (``SolverCSD.jl:891-1120``).
@@ -295,33 +354,107 @@ def solve_dlr_fixed(solver: SolverCSD, max_steps: int | None = None, state: dict
             G = solver._x_grams(X, X)
             C = solver._w_grams(W, W)
             S = solver._s_stream(S, G, C, dE)
-        # out scattering
-        L = W @ S.T
-        L = L / (1.0 + dE * D)[:, None]
-        W, S = out_scatter_factor(L, mode, solver.w_completion)
-        # in scattering, K-step
-        X[bnd, :] = 0.0
-        K = X @ S
-        psiv = psi.reshape(nx * ny, -1)
-        K = K + dE * psiv @ (Mr.T @ (Dvec[:, None] * W))
-        K[bnd, :] = 0.0
-        XNew = la.orth(K, mode, order=solver.x_completion)
-        MUp = XNew.T @ X
-        # L-step
-        L = W @ S.T
-        L = L + dE * Dvec[:, None] * (Mr @ (psiv.T @ X))
-        WNew = la.orth(L, mode, order=solver.w_completion)
-        NUp = WNew.T @ W
-        W = WNew
-        X = XNew
-        # S-step
-        S = MUp @ S @ NUp.T
-        S = S + dE * (X.T @ psiv) @ Mr.T @ (Dvec[:, None] * W)
+        X, S, W = _fixed_scatter(solver, X, S, W, psi, Dvec, D, dE)
         solver.dose_half(X, S, W, psi, dE, Scsd[n - 1])
     if return_state:
         return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), n_next=last + 1)
     return solver.outputs(X, S, W, psi)
 
+
+def rk4_accumulated(Y, dE, f):
+    """One classical RK4 step of Y' = f(Y) in the K-step's form
+    (``SolverCSD.jl:731-739``): KUP grows stage by stage."""
+    k1 = f(Y)
+    up = Y + dE * k1 / 6
+    k2 = f(Y + 0.5 * dE * k1)
+    up = up + 2 * dE * k2 / 6
+    k3 = f(Y + 0.5 * dE * k2)
+    up = up + 2 * dE * k3 / 6
+    k4 = f(Y + dE * k3)
+    return up + dE * k4 / 6
+
+
+def rk4_summed(Y, dE, f):
+    """The same step in the L- and S-steps' form (``:751-756``, ``:783-788``)."""
+    k1 = f(Y)
+    k2 = f(Y + 0.5 * dE * k1)
+    k3 = f(Y + 0.5 * dE * k2)
+    k4 = f(Y + dE * k3)
+    return Y + dE * (k1 + 2 * k2 + 2 * k3 + k4) / 6
+
+
+def solve_dlr_high_order(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
+                         n_begin: int = 2, return_state: bool = False):
+    """``SolveFirstCollisionSourceDLRHighOrder`` (``SolverCSD.jl:588-889``).
+
+    The fixed-rank loop with a second-order uncollided part and RK4 streaming:
+    - inflow on the two outer layers (``:679-695``, ``apply_bc_two_layer``);
+    - the limited flux ``solveFlux!`` for the sweep (``:707``);
+    - K, L and S streaming with the central operators only (L2x/L2y with
+      Ax/Az; no Roe diffusion terms), each advanced by one classical RK4 step
+      of size dE (``:724-791``).
+    The reference assigns ``KUP .= ...`` without allocating it (an
+    UndefVarError when the loop reaches ``n = 3``); here KUP is a fresh array
+    of K's shape, the evident intent. The out- and in-scattering steps and the
+    dose half-steps are those of the fixed-rank loop. Arguments and return
+    value as ``solve_dlr_fixed``.
+    """
+    s = solver.settings
+    mode = solver.basis_mode
+    r = s.r
+    eTrafo = solver.csd.eTrafo
+    energy = solver.csd.eGrid
+    Scsd = solver.csd.S
+    psi = solver.setup_directions()
+    X, S, W = init_factors(solver, r)
+    if state is not None:
+        X, S, W = state["X"].copy(), state["S"].copy(), state["W"].copy()
+        psi = state["psi"].reshape(psi.shape).copy()
+        solver.dose = state["dose"].copy()
+    bnd = solver.boundaryIdx
+    st = solver.stencil
+    nE = eTrafo.size
+    dE = eTrafo[1] - eTrafo[0]
+    s.dE = dE
+    last = nE if max_steps is None else min(nE, n_begin - 1 + max_steps)
+
+    for n in range(n_begin, last + 1):
+        sigma = solver.csd.sigma_at_energy(energy[n - 1])
+        solver.apply_bc_two_layer(psi, energy[n - 2], n - 1)
+        solver.dose_half(X, S, W, psi, dE, Scsd[n - 2])
+        solver.sweep_limited(psi, dE, sigma[0])
+        Dvec = solver.dvec(sigma)
+        D = sigma[0] - Dvec
+        if n > 2:
+            # K-step
+            X[bnd, :] = 0.0
+            K = X @ S
+            WAzW = W.T @ (solver.Az @ W)
+            WAxW = W.T @ (solver.Ax @ W)
+            K = rk4_accumulated(K, dE, lambda Y: -(st.L2x @ Y) @ WAxW - (st.L2y @ Y) @ WAzW)
+            XNew = la.orth(K, mode, order=solver.x_completion)
+            MUp = XNew.T @ X
+            # L-step
+            L = W @ S.T
+            XL2xX = X.T @ (st.L2x @ X)
+            XL2yX = X.T @ (st.L2y @ X)
+            L = rk4_summed(L, dE, lambda Y: -(solver.Ax @ Y) @ XL2xX.T - (solver.Az @ Y) @ XL2yX.T)
+            WNew = la.orth(L, mode, order=solver.w_completion)
+            NUp = WNew.T @ W
+            W = WNew
+            X = XNew
+            # S-step
+            S = MUp @ S @ NUp.T
+            XL2xX = X.T @ (st.L2x @ X)
+            XL2yX = X.T @ (st.L2y @ X)
+            WAzW = W.T @ (solver.Az @ W)
+            WAxW = W.T @ (solver.Ax @ W)
+            S = rk4_summed(S, dE, lambda Y: -XL2xX @ Y @ WAxW - XL2yX @ Y @ WAzW)
+        X, S, W = _fixed_scatter(solver, X, S, W, psi, Dvec, D, dE)
+        solver.dose_half(X, S, W, psi, dE, Scsd[n - 1])
+    if return_state:
+        return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), n_next=last + 1)
+    return solver.outputs(X, S, W, psi)
 
 def _augment_tilde(solver, A_old, A_new, side):
     """``Xtmp,_ = py"qr"([X K]); X1Tilde = Xtmp[:, (r+1):end]`` and the full Q.

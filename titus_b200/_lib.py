@@ -17,6 +17,9 @@ LIB_PATH = os.path.join(HERE, "libtitus.so")
 TITUS_DLR_FIXED = 0
 TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
+TITUS_DLR_HIGH_ORDER = 3
+TITUS_PRECISION_FP64 = 0
+TITUS_PRECISION_MIXED = 1
 # exclusive device timers (titus_profile order); "other" is time outside every named phase
 PROFILE_NAMES = ["barrier", "reduce", "jacobi", "cholesky", "completion", "rows_stream", "rows_scatter", "rf_passes",
                  "small", "other", "prologue"]
@@ -46,7 +49,7 @@ class Problem(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("team_ctas", C.c_int32), ("max_steps", C.c_int32), ("rank_tol", C.c_double),
-                ("profile", C.c_int32)]
+                ("profile", C.c_int32), ("precision", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -91,6 +94,7 @@ SIGNATURES = [
     ("titus_pn_full_solve", C.c_int, [C.c_void_p, C.POINTER(Options), _dp, _dp, _dp]),
     ("titus_debug_barrier_fault", C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
     ("titus_debug_fail_alloc", C.c_int, [C.c_int32]),
+    ("titus_debug_tc_gram", C.c_int, [_dp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     ("titus_max_rank", C.c_int, []),
     ("titus_max_ordinates", C.c_int, []),
     ("titus_version", C.c_char_p, []),

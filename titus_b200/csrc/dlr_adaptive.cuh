@@ -245,6 +245,116 @@ static __device__ __noinline__ void w_grams_pass(WCtx& x, const double* A, const
     }
 }
 
+// ---- MIXED precision: the same eight operator Grams on the tensor cores
+// (umma.cuh). Per side, one run over the CTA's own rows stages the factor
+// (N operand) and its four operator images (M operand, stacked) chunk by
+// chunk straight from global memory -- the stencil / sparse products are
+// formed where they are staged, in FP64 exactly as w_stencil / w_spmm form
+// them -- and accumulates D[d cw + i][j] = sum_r (L_d A)[r][i] A[r][j] = G_d[j][i]
+// in TMEM (FP32). The sums are written as this CTA's partial at the FP64
+// layout [G_0..G_3 | C_0..C_3] (cw x cw each), ready for wreduce. Uses the
+// whole shared work area as staging. Returns false if a completion wait timed
+// out (device status set).
+static __device__ __noinline__ bool w_grams_tc(WCtx& x, const double* A, const double* B, int cw) {
+    ProfScope ps_(x.prof, PF_ROWS_STREAM);
+    const umma::GramShape g = umma::gram_shape(4 * cw, cw);
+    unsigned char* stage = reinterpret_cast<unsigned char*>(x.sm->work);
+    double* dst = wpart(x, x.b);
+    const int kk = cw * cw;
+    const DevProblem& P = x.P;
+    bool ok = true;
+    for (int side = 0; side < 2; ++side) {
+        const int r0 = side == 0 ? x.c0 : x.m0;
+        const int rows = (side == 0 ? x.c1 : x.m1) - r0;
+        double* out = dst + side * 4 * kk;
+        if (rows <= 0) {
+            for (int e = threadIdx.x; e < 4 * kk; e += NT) out[e] = 0.0;
+            __syncthreads();
+            continue;
+        }
+        bool run;
+        if (side == 0) {
+            const double hx = 0.5 / P.dx, hy = 0.5 / P.dy, ix = 1.0 / P.dx, iy = 1.0 / P.dy;
+            run = umma::gram_run<NT, 4>(x.tc, g, stage, rows, true, [&](int r, int j, double* v) {
+                const int c = r0 + r;
+                const double* p = A + (size_t)c * KA + j;
+                v[0] = ldcg(p);
+                double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
+                if (!is_bnd_w(P, c)) {
+                    const double a0 = v[0] * __ldg(P.rinv + c);
+                    const double axm = ldcg(p - (size_t)P.ny * KA) * __ldg(P.rinv + c - P.ny);
+                    const double axp = ldcg(p + (size_t)P.ny * KA) * __ldg(P.rinv + c + P.ny);
+                    const double aym = ldcg(p - KA) * __ldg(P.rinv + c - 1);
+                    const double ayp = ldcg(p + KA) * __ldg(P.rinv + c + 1);
+                    l2x = (axp - axm) * hx;
+                    l2y = (ayp - aym) * hy;
+                    l1x = a0 * ix - hx * axm - hx * axp;
+                    l1y = a0 * iy - hy * aym - hy * ayp;
+                }
+                v[1] = l2x;
+                v[2] = l2y;
+                v[3] = l1x;
+                v[4] = l1y;
+            });
+        } else {
+            run = umma::gram_run<NT, 4>(x.tc, g, stage, rows, true, [&](int r, int j, double* v) {
+                const int m = r0 + r;
+                v[0] = ldcg(B + (size_t)m * KA + j);
+#pragma unroll
+                for (int d = 0; d < 4; ++d) {
+                    const Csr& Op = P.op[d];
+                    double s = 0.0;
+                    const int p1 = __ldg(Op.rowptr + m + 1);
+                    for (int q = __ldg(Op.rowptr + m); q < p1; ++q)
+                        s = fma(__ldg(Op.val + q), ldcg(B + (size_t)__ldg(Op.col + q) * KA + j), s);
+                    v[1 + d] = s;
+                }
+            });
+        }
+        const bool fin = umma::gram_finish(x.tc);
+        if (!(run && fin)) {
+            ok = false;
+            break;
+        }
+        umma::gram_read<NT>(x.tc, g, [&](int m, int n, double val) {
+            const int d = m / cw, i = m - d * cw;
+            out[d * kk + n * cw + i] = val;
+        });
+    }
+    return ok;
+}
+
+// MIXED mode setup and teardown around a launch's work: warp 0 allocates the
+// TMEM accumulators, thread 0 initialises the two completion barriers; at the
+// end every outstanding MMA is waited for (bounded) before the TMEM is freed.
+__device__ inline void tc_setup(WCtx& x) {
+    x.mixed = x.P.precision == 1;
+    if (!x.mixed) return;
+    if (threadIdx.x < 32) umma::tmem_alloc(&x.sm->tmem_slot, umma::TMEM_COLS);
+    if (threadIdx.x == 0) {
+        umma::mbar_init(&x.sm->mbar[0], 1);
+        umma::mbar_init(&x.sm->mbar[1], 1);
+        umma::fence_mbar_init();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    x.tc.mbar = x.sm->mbar;
+    x.tc.tmem = x.sm->tmem_slot;
+    x.tc.phase[0] = x.tc.phase[1] = 0u;
+    x.tc.pending[0] = x.tc.pending[1] = 0;
+    x.tc.status = x.st.status;
+    x.tc.limit = umma::kWaitCycles;
+}
+__device__ inline void tc_teardown(WCtx& x) {
+    if (!x.mixed) return;
+    umma::gram_finish(x.tc);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (threadIdx.x < 32) umma::tmem_dealloc(x.tc.tmem, umma::TMEM_COLS);
+}
+
 __device__ inline void w_acc_zero(double* acc, int cnt) {
     for (int e = threadIdx.x; e < cnt; e += NT) acc[e] = 0.0;
     __syncthreads();
@@ -256,11 +366,15 @@ __device__ inline void w_acc_zero(double* acc, int cnt) {
 static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
     ProfScope ps_(x.prof, PF_ROWS_STREAM);
     const int k = x.r;
-    double* acc = x.sm->work;
-    double* F = x.sm->work + 8 * k * k;
-    w_acc_zero(acc, 8 * k * k);
-    w_grams_pass(x, x.st.X, x.st.W, k, 0, 4, 0, acc, F, 5 * k, rows_fit(WORKD - 8 * k * k, 5 * k));
-    wpublish_chunk(x, acc, 0, 8 * k * k);
+    if (x.mixed && k >= kTcMinWidth) {
+        if (!w_grams_tc(x, x.st.X, x.st.W, k)) return false;
+    } else {
+        double* acc = x.sm->work;
+        double* F = x.sm->work + 8 * k * k;
+        w_acc_zero(acc, 8 * k * k);
+        w_grams_pass(x, x.st.X, x.st.W, k, 0, 4, 0, acc, F, 5 * k, rows_fit(WORKD - 8 * k * k, 5 * k));
+        wpublish_chunk(x, acc, 0, 8 * k * k);
+    }
     return wreduce(x, 8 * k * k, [&] {
         for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT)
             if (is_bnd_w(x.P, c))
@@ -1304,13 +1418,17 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 // operators per chunk: as many as fit with at least 16 feature rows
                 const int opc = (8 * mm + 16 * 5 * m <= WORKD) ? 4 : ((4 * mm + 16 * 5 * m <= WORKD) ? 2 : 1);
                 double* F = sm->work + 2 * opc * mm;
-                for (int d = 0; d < 4; d += opc) {
-                    w_acc_zero(acc, 2 * opc * mm);
-                    w_grams_pass(x, x.st.X, x.st.W, m, d, d + opc, 0, acc, F, 5 * m,
-                                 rows_fit(WORKD - 2 * opc * mm, 5 * m));
-                    wpublish_chunk(x, acc, d * mm, opc * mm);                   // X side G_d
-                    wpublish_chunk(x, acc + opc * mm, (4 + d) * mm, opc * mm);  // W side C_d
-                    __syncthreads();
+                if (x.mixed && m >= kTcMinWidth) {
+                    if (!w_grams_tc(x, x.st.X, x.st.W, m)) { aborted = true; break; }
+                } else {
+                    for (int d = 0; d < 4; d += opc) {
+                        w_acc_zero(acc, 2 * opc * mm);
+                        w_grams_pass(x, x.st.X, x.st.W, m, d, d + opc, 0, acc, F, 5 * m,
+                                     rows_fit(WORKD - 2 * opc * mm, 5 * m));
+                        wpublish_chunk(x, acc, d * mm, opc * mm);                   // X side G_d
+                        wpublish_chunk(x, acc + opc * mm, (4 + d) * mm, opc * mm);  // W side C_d
+                        __syncthreads();
+                    }
                 }
                 if (!wreduce(x, 8 * mm)) { aborted = true; break; }
                 // Sup = S2 - dE sum_d G_d S2 C_d ; eta from the [k:, k:] block
@@ -1564,7 +1682,9 @@ adaptive_kernel(DevProblem P, WideState* states, int G, int n_begin, int n_end, 
     ls.eta_count = ldcg(x.st.info + 4);
     ls.n = n_begin;
     ls.aborted = false;
+    tc_setup(x);
     energy_loop<METHOD>(x, n_begin, n_end, max_iters, ls);
+    tc_teardown(x);
     if (x.b == 0) {
         for (int e = threadIdx.x; e < KA * KA; e += NT) x.st.S[e] = sm->S[e];
         if (threadIdx.x == 0) {
@@ -1649,6 +1769,7 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
     x.m0 = (int)((long long)x.b * P0.N / G);
     x.m1 = (int)((long long)(x.b + 1) * P0.N / G);
     __shared__ int s_next;
+    tc_setup(x);
     while (true) {
         if (x.b == 0 && threadIdx.x == 0) {
             const int q = atomicAdd(queue, 1);
@@ -1657,7 +1778,7 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
         }
         __syncthreads();
         if (G > 1) {
-            if (!wsync(x)) return;
+            if (!wsync(x)) break;
             if (x.b != 0 && threadIdx.x == 0) s_next = ldcg(x.st.info + 6);
             __syncthreads();
         }
@@ -1675,7 +1796,7 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
         x.st.dose = sp.dose;
         init_spot(x, r0);
         x.r = r0;
-        if (!wsync(x)) return;
+        if (!wsync(x)) break;
         LoopState ls;
         ls.psi_idx = 0;
         ls.t = 0.0;
@@ -1687,13 +1808,14 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
         const int n_end = (METHOD == TITUS_PARALLEL_ADAPTIVE && max_steps_par > 0) ? min(sp.nE, 1 + max_steps_par)
                                                                                      : sp.n_end;
         energy_loop<METHOD>(x, 2, n_end, max_iters, ls);
-        if (ls.aborted) return;
+        if (ls.aborted) break;
         if (x.b == 0 && threadIdx.x == 0) {
             sp.result[0] = x.r;
             sp.result[1] = ls.iters;
             sp.result[2] = ls.rank_sum;
         }
     }
+    tc_teardown(x);
 }
 
 }  // namespace wide

@@ -55,6 +55,7 @@ struct DevProblem {
     int zero_smem;            // 1: clear the dynamic shared memory at kernel start
     long long spin_limit;     // polls before a team barrier gives up (0 = default, about a second)
     int fault_barrier;        // test hook: CTA 1 does not arrive at this barrier generation (<= 0: off)
+    int precision;            // 0: FP64; 1: MIXED (tensor-core operator Grams, adaptive integrators)
 };
 
 // Phase-timer categories (titus_profile reports them in this order).
@@ -123,6 +124,8 @@ struct TeamState {
     double* eta_hist;
     double* bound_hist;
     double* time_hist;
+    double* Y;      // 3 x n x KM: RK4 integrator stage buffers of the K-step (KUP, two stage inputs)
+    double* Z;      // 3 x N x KM: the same for the L-step
 };
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }

@@ -2,6 +2,7 @@
 // as phases of one persistent kernel. See dlr_kernel.cuh for the phase map.
 #pragma once
 #include "dlr_kernel.cuh"
+#include "limiter.cuh"
 
 namespace titus {
 
@@ -37,7 +38,20 @@ __device__ inline bool publish_sync(Ctx& x, int count) {
 
 // ---- phase A: (pending) second dose half-step, boundary inflow, first dose
 // half-step, X[bnd,:] = 0.  Own cells only; no reduction.
-__device__ inline void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc) {
+// Inflow cell of the RK4 integrator's two-layer boundary condition
+// (SolverCSD.jl:679-695): the second layer takes the PsiBeam value of the
+// first layer's coordinates, and the x-sides (written last) win at corners.
+// Returns the cell whose spatial factor applies, or -1 off the two rings.
+__device__ __forceinline__ int bc2_source(const DevProblem& P, int c) {
+    const int i = c / P.ny, j = c - (c / P.ny) * P.ny;
+    if (i <= 1) return j;                              // (0, j)
+    if (i >= P.nx - 2) return (P.nx - 1) * P.ny + j;   // (nx-1, j)
+    if (j <= 1) return i * P.ny;                       // (i, 0)
+    if (j >= P.ny - 2) return i * P.ny + P.ny - 1;     // (i, ny-1)
+    return -1;
+}
+
+__device__ inline void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_bc, bool two_layer = false) {
     const DevProblem& P = x.P;
     SmemLayout* sm = x.sm;
     const int k = x.k;
@@ -69,8 +83,9 @@ __device__ inline void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_
         }
         bool bnd = is_bnd(P, c);
         if (do_bc) {
-            if (bnd) {
-                double bs = bce * P.bc_space[c];
+            const int src = two_layer ? bc2_source(P, c) : (bnd ? c : -1);
+            if (src >= 0) {
+                double bs = bce * P.bc_space[src];
                 for (int kq = 0; kq < P.q; ++kq) pr[kq] = bs * P.bc_angle[kq];
             }
             double u = 0.0;
@@ -83,8 +98,27 @@ __device__ inline void phase_bc_dose(Ctx& x, int n, bool dose2_pending, bool do_
     }
 }
 
-// ---- uncollided sweep for own cells (psi_in -> psi_out)
-__device__ inline void sweep_cells(Ctx& x, double sigma0) {
+// Second-order limited flux of psi/rho at interior cell c (2 <= i < nx-2,
+// 2 <= j < ny-2), ordinate kq: solveFlux! (SolverCSD.jl:295-386).
+__device__ __forceinline__ double limited_flux_cell(const Ctx& x, int c, int kq) {
+    const DevProblem& P = x.P;
+    const double* p = x.psi_in + kq;
+    auto phi = [&](int cc) { return ldcg(p + (size_t)cc * QM) * P.rinv[cc]; };
+    const double ox = P.omega[kq * 3 + 0], oz = P.omega[kq * 3 + 2];
+    const int sx = P.ny;
+    const double f0 = phi(c);
+    const bool px = ox >= 0.0, pz = oz >= 0.0;
+    const double ew = titus_lim::axis_diff(px ? phi(c - 2 * sx) : 0.0, phi(c - sx), f0, phi(c + sx),
+                                           px ? 0.0 : phi(c + 2 * sx), px);
+    const double ns = titus_lim::axis_diff(pz ? phi(c - 2) : 0.0, phi(c - 1), f0, phi(c + 1), pz ? 0.0 : phi(c + 2), pz);
+    return __dadd_rn(__dmul_rn(__ddiv_rn(ox, P.dx), ew), __dmul_rn(__ddiv_rn(oz, P.dy), ns));
+}
+
+// ---- uncollided sweep for own cells (psi_in -> psi_out). `limited`: the RK4
+// integrator's second-order flux on the interior of the two outer rings (the
+// reference's flux buffer stays zero on the rings, :648, :707); otherwise the
+// first-order upwind flux on every non-boundary cell.
+__device__ inline void sweep_cells(Ctx& x, double sigma0, bool limited = false) {
     const DevProblem& P = x.P;
     const double dE = P.dE;
     const double den = 1.0 + dE * sigma0;
@@ -93,7 +127,10 @@ __device__ inline void sweep_cells(Ctx& x, double sigma0) {
         int c = x.c0 + e / q, kq = e - (e / q) * q;
         double pc = ldcg(x.psi_in + (size_t)c * QM + kq);
         double flux = 0.0;
-        if (!is_bnd(P, c)) {
+        if (limited) {
+            const int i = c / P.ny, j = c - (c / P.ny) * P.ny;
+            if (i >= 2 && i < P.nx - 2 && j >= 2 && j < P.ny - 2) flux = limited_flux_cell(x, c, kq);
+        } else if (!is_bnd(P, c)) {
             double ox = P.omega[kq * 3 + 0], oz = P.omega[kq * 3 + 2];
             double f0 = pc * P.rinv[c];
             double ew, ns;
@@ -110,24 +147,26 @@ __device__ inline void sweep_cells(Ctx& x, double sigma0) {
 }
 
 // ---- streaming Grams X^T L_d X (own cells) and W^T A_d W (own moments):
-// partial layout [G_0..G_3 | C_0..C_3], each k x k.
-__device__ inline void stream_grams_partial(Ctx& x) {
+// partial layout [G_0..G_{nops-1} | C_0..C_{nops-1}], each k x k. nops = 4:
+// L2x/Ax, L2y/Az, L1x/|Ax|, L1y/|Az|; nops = 2: the central pair only.
+__device__ inline void stream_grams_partial(Ctx& x, int nops = 4) {
     SmemLayout* sm = x.sm;
     const int k = x.k;
     for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
         int nr = min(TR, x.c1 - r0);
         load_rows(sm->tA, x.st.X, r0, nr, k);
-        stencil_tile(x, x.st.X, r0, nr, k, sm->tL);
+        if (nops == 2) stencil2_tile(x, x.st.X, r0, nr, k, sm->tL);
+        else stencil_tile(x, x.st.X, r0, nr, k, sm->tL);
         __syncthreads();
-        for (int d = 0; d < 4; ++d) gram_acc(sm->acc, d * k * k, sm->tA, KM, k, sm->tL[d], KM, k, nr);
+        for (int d = 0; d < nops; ++d) gram_acc(sm->acc, d * k * k, sm->tA, KM, k, sm->tL[d], KM, k, nr);
         __syncthreads();
     }
     for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
         int nr = min(TR, x.m1 - r0);
         load_rows(sm->tA, x.st.W, r0, nr, k);
-        spmm_tile(x, x.st.W, r0, nr, k, sm->tL);
+        spmm_tile(x, x.st.W, r0, nr, k, sm->tL, nops);
         __syncthreads();
-        for (int d = 0; d < 4; ++d) gram_acc(sm->acc, (4 + d) * k * k, sm->tA, KM, k, sm->tL[d], KM, k, nr);
+        for (int d = 0; d < nops; ++d) gram_acc(sm->acc, (nops + d) * k * k, sm->tA, KM, k, sm->tL[d], KM, k, nr);
         __syncthreads();
     }
 }
@@ -274,6 +313,176 @@ __device__ inline void sm_asbt(double* D, const double* A, const double* S, cons
     sm_mmt(D, tmp, B, k, k, k);
 }
 
+// ---- RK4 streaming of K and L (SolverCSD.jl:724-758), the RK4 ("HighOrder")
+// integrator's replacement of phase C. Four stages with one team barrier after
+// each of the first three: the stencils and the sparse P_N products read
+// other CTAs' rows of the stage input. Stage 1 works from X and W directly,
+// since L2_d (X S) C_d = (L2_d X)(S C_d) and A_d (W S^T) G_d^T = (A_d W)(S^T G_d^T).
+// Slots on entry (d = 0: x, 1: y): C0+d = C_d = W^T A_d W, C0+2+d = S C_d,
+// G0+d = G_d^T with G_d = X^T L2_d X, G0+2+d = S^T G_d^T.
+// K side: f(Y) = -L2x Y C_0 - L2y Y C_1; KUP accumulates as the reference does
+// (K + dE k1/6, then += 2 dE k2/6, += 2 dE k3/6, K = KUP + dE k4/6).
+// L side: f(Y) = -Ax Y G_0^T - Az Y G_1^T; L + dE (l1 + 2 l2 + 2 l3 + l4)/6.
+// On return K and L hold the new K, L and their Grams are published
+// (offsets 0 and k*k) for the range finder. Returns false if the team aborted.
+static __device__ __noinline__ bool rk4_stream(Ctx& x) {
+    SmemLayout* sm = x.sm;
+    const int k = x.k;
+    const double dE = x.P.dE;
+    const double* Sm = sm->slot[SL_S];
+    const size_t nK = (size_t)x.P.n * KM, NK = (size_t)x.P.N * KM;
+    double* KUP = x.st.Y;
+    double* Ya = x.st.Y + nK;
+    double* Yb = x.st.Y + 2 * nK;
+    double* LUP = x.st.Z;
+    double* La = x.st.Z + NK;
+    double* Lb = x.st.Z + 2 * NK;
+    for (int s = 1; s <= 4; ++s) {
+        // stage inputs: Y2 = K + dE/2 k1 (Ya), Y3 = K + dE/2 k2 (Yb), Y4 = K + dE k3 (Ya)
+        const double* Yin = (s == 3) ? Yb : Ya;
+        double* Yout = (s == 2) ? Yb : Ya;
+        const double* Lin = (s == 3) ? Lb : La;
+        double* Lout = (s == 2) ? Lb : La;
+        const double cnext = (s == 3) ? dE : 0.5 * dE;
+        const double wup = (s == 1 || s == 4) ? 1.0 : 2.0;
+        const double* C0 = sm->slot[SL_C0 + (s == 1 ? 2 : 0)];
+        const double* C1 = sm->slot[SL_C0 + (s == 1 ? 3 : 1)];
+        const double* H0 = sm->slot[SL_G0 + (s == 1 ? 2 : 0)];
+        const double* H1 = sm->slot[SL_G0 + (s == 1 ? 3 : 1)];
+        if (s == 4) acc_zero(x, 2 * k * k);
+        {
+            ProfScope ps(x.prof, PF_ROWS_STREAM);
+            for (int r0 = x.c0; r0 < x.c1; r0 += TR) {
+                const int nr = min(TR, x.c1 - r0);
+                if (s == 1) {
+                    load_rows(sm->tA, x.st.X, r0, nr, k);
+                    stencil2_tile(x, x.st.X, r0, nr, k, sm->tL);
+                } else {
+                    stencil2_tile(x, Yin, r0, nr, k, sm->tL);
+                }
+                __syncthreads();
+                for (int e = threadIdx.x; e < nr * k; e += NT) {
+                    const int r = e / k, j = e - (e / k) * k;
+                    const size_t g = (size_t)(r0 + r) * KM + j;
+                    double t = 0.0;
+                    for (int l = 0; l < k; ++l) t = fma(sm->tL[0][r * KM + l], C0[l * KM + j], t);
+                    for (int l = 0; l < k; ++l) t = fma(sm->tL[1][r * KM + l], C1[l * KM + j], t);
+                    const double kd = -t;
+                    double Kv;
+                    if (s == 1) {
+                        Kv = 0.0;
+                        for (int l = 0; l < k; ++l) Kv = fma(sm->tA[r * KM + l], Sm[l * KM + j], Kv);
+                        x.st.K[g] = Kv;
+                        KUP[g] = Kv + dE * kd / 6;
+                    } else {
+                        Kv = ldcg(x.st.K + g);
+                        if (s < 4) KUP[g] = ldcg(KUP + g) + wup * dE * kd / 6;
+                    }
+                    if (s < 4) {
+                        Yout[g] = Kv + cnext * kd;
+                    } else {
+                        const double Kn = ldcg(KUP + g) + dE * kd / 6;
+                        sm->tO[r * KM + j] = Kn;
+                    }
+                }
+                __syncthreads();
+                if (s == 4) {
+                    store_rows(x.st.K, sm->tO, r0, nr, k);
+                    gram_acc(sm->acc, 0, sm->tO, KM, k, sm->tO, KM, k, nr);
+                    __syncthreads();
+                }
+            }
+            for (int r0 = x.m0; r0 < x.m1; r0 += TR) {
+                const int nr = min(TR, x.m1 - r0);
+                if (s == 1) {
+                    load_rows(sm->tA, x.st.W, r0, nr, k);
+                    spmm_tile(x, x.st.W, r0, nr, k, sm->tL, 2);
+                } else {
+                    spmm_tile(x, Lin, r0, nr, k, sm->tL, 2);
+                }
+                __syncthreads();
+                for (int e = threadIdx.x; e < nr * k; e += NT) {
+                    const int r = e / k, j = e - (e / k) * k;
+                    const size_t g = (size_t)(r0 + r) * KM + j;
+                    double t = 0.0;
+                    for (int l = 0; l < k; ++l) t = fma(sm->tL[0][r * KM + l], H0[l * KM + j], t);
+                    for (int l = 0; l < k; ++l) t = fma(sm->tL[1][r * KM + l], H1[l * KM + j], t);
+                    const double ld = -t;
+                    double Lv;
+                    if (s == 1) {
+                        Lv = 0.0;  // (W S^T)[r][j]
+                        for (int l = 0; l < k; ++l) Lv = fma(sm->tA[r * KM + l], Sm[j * KM + l], Lv);
+                        x.st.L[g] = Lv;
+                        LUP[g] = ld;
+                    } else {
+                        Lv = ldcg(x.st.L + g);
+                        if (s < 4) LUP[g] = ldcg(LUP + g) + wup * ld;
+                    }
+                    if (s < 4) {
+                        Lout[g] = Lv + cnext * ld;
+                    } else {
+                        sm->tO[r * KM + j] = Lv + dE * (ldcg(LUP + g) + ld) / 6;
+                    }
+                }
+                __syncthreads();
+                if (s == 4) {
+                    store_rows(x.st.L, sm->tO, r0, nr, k);
+                    gram_acc(sm->acc, k * k, sm->tO, KM, k, sm->tO, KM, k, nr);
+                    __syncthreads();
+                }
+            }
+        }
+        if (s < 4) {
+            if (!tsync(x)) return false;
+        } else if (!publish_sync(x, 2 * k * k)) {
+            return false;
+        }
+    }
+    return true;
+}
+
+// S-step of the RK4 integrator in the small space (SolverCSD.jl:776-791):
+// f(Y) = -G_0 Y C_0 - G_1 Y C_1 with the new bases' Grams in slots G0+d, C0+d;
+// S <- S + dE (s1 + 2 s2 + 2 s3 + s4) / 6. Every CTA computes it redundantly.
+__device__ inline void rk4_small_s(Ctx& x) {
+    SmemLayout* sm = x.sm;
+    const int k = x.k;
+    const double dE = x.P.dE;
+    double* Sm = sm->slot[SL_S];
+    double* Y = sm->slot[SL_P0];
+    double* T1 = sm->slot[SL_P0 + 1];
+    double* kv = sm->slot[SL_P0 + 2];
+    double* sum = sm->slot[SL_P0 + 3];
+    double* T2 = sm->slot[SL_VK];
+    for (int s = 1; s <= 4; ++s) {
+        const double* in = (s == 1) ? Sm : Y;
+        sm_mm(T1, sm->slot[SL_G0], in, k, k, k);
+        sm_mm(kv, T1, sm->slot[SL_C0], k, k, k);
+        sm_mm(T1, sm->slot[SL_G0 + 1], in, k, k, k);
+        sm_mm(T2, T1, sm->slot[SL_C0 + 1], k, k, k);
+        const double w = (s == 1 || s == 4) ? 1.0 : 2.0;
+        const double cn = (s == 3) ? dE : 0.5 * dE;
+        for (int e = threadIdx.x; e < k * k; e += NT) {
+            const int o = (e / k) * KM + e % k;
+            const double d = -kv[o] - T2[o];
+            sum[o] = (s == 1) ? d : sum[o] + w * d;
+            if (s < 4) Y[o] = Sm[o] + cn * d;
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < k * k; e += NT) {
+        const int o = (e / k) * KM + e % k;
+        Sm[o] = Sm[o] + dE * sum[o] / 6;
+    }
+    __syncthreads();
+}
+
+// METHOD: 0 = fixed-rank DLR (SolveFirstCollisionSourceDLR), kHighOrder = the
+// RK4 variant (SolveFirstCollisionSourceDLRHighOrder, SolverCSD.jl:588-889):
+// two-layer inflow, limited second-order sweep, RK4 streaming with the
+// central operators; the scattering steps are shared.
+constexpr int kHighOrder = 3;
+
 template <int METHOD>
 __global__ void __launch_bounds__(NT, 1)
 dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int dose2_pending_in) {
@@ -311,6 +520,8 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
     __syncthreads();
     bool pending = dose2_pending_in != 0;
     int steps = 0;
+    constexpr bool HO = (METHOD == kHighOrder);   // RK4 integrator (SolveFirstCollisionSourceDLRHighOrder)
+    constexpr int nops = HO ? 2 : 4;               // streaming operators: central pair, or with Roe terms
     double* Sm = sm->slot[SL_S];
     for (int n = n_begin; n <= n_end; ++n) {
         x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
@@ -319,22 +530,40 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
         x.cur_n = n;
         const double dE = P.dE;
         // ---------------- phase A
-        phase_bc_dose(x, n, pending, true);
+        phase_bc_dose(x, n, pending, true, HO);
         pending = false;
         if (!tsync(x)) return;
         // ---------------- phase B: sweep + streaming Grams
-        sweep_cells(x, sig[0]);
+        sweep_cells(x, sig[0], HO);
         const bool stream = (n > 2);
         if (stream) {
-            acc_zero(x, 8 * k * k);
-            stream_grams_partial(x);
-            if (!publish_sync(x, 8 * k * k)) return;
+            acc_zero(x, 2 * nops * k * k);
+            stream_grams_partial(x, nops);
+            if (!publish_sync(x, 2 * nops * k * k)) return;
         } else if (!tsync(x)) {
             return;
         }
         psi_idx ^= 1;
         x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;  // swept psi
-        if (stream) {
+        if (stream && HO) {
+            // C0+d = C_d, C0+2+d = S C_d, G0+d = G_d^T, G0+2+d = S^T G_d^T (d = 0, 1)
+            for (int d = 0; d < 2; ++d) {
+                reduce_into(x, d * k * k, k, k, sm->slot[SL_P0]);
+                reduce_into(x, (2 + d) * k * k, k, k, sm->slot[SL_C0 + d]);
+                sm_mm(sm->slot[SL_C0 + 2 + d], Sm, sm->slot[SL_C0 + d], k, k, k);
+                for (int e = threadIdx.x; e < k * k; e += NT) {
+                    int i = e / k, j = e % k;
+                    sm->slot[SL_G0 + d][i * KM + j] = sm->slot[SL_P0][j * KM + i];
+                    double s2 = 0.0;
+                    for (int l = 0; l < k; ++l) s2 = fma(Sm[l * KM + i], sm->slot[SL_P0][j * KM + l], s2);
+                    sm->slot[SL_G0 + 2 + d][i * KM + j] = s2;
+                }
+                __syncthreads();
+            }
+            // ---------------- phase C (RK4): K and L streaming updates
+            if (!rk4_stream(x)) return;
+        }
+        if (stream && !HO) {
             for (int d = 0; d < 4; ++d) {
                 reduce_into(x, d * k * k, k, k, sm->slot[SL_G0 + d]);
                 reduce_into(x, (4 + d) * k * k, k, k, sm->slot[SL_C0 + d]);
@@ -394,6 +623,8 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
                 __syncthreads();
             }
             if (!publish_sync(x, 2 * k * k)) return;
+        }
+        if (stream) {
             // ---------------- phases D, E: range finders of K and L
             if (!range_finder(x, x.st.K, x.st.L, true, true, k)) return;
             // ---------------- phase F: new bases, MUp = XNew^T X, NUp = WNew^T W
@@ -425,9 +656,18 @@ dlr_kernel(DevProblem P, TeamState* states, int G, int n_begin, int n_end, int d
             sm_asbt(sm->slot[SL_P0 + 1], sm->slot[SL_M], Sm, sm->slot[SL_N], sm->slot[SL_P0], k);
             sm_copy(Sm, sm->slot[SL_P0 + 1], k, k);
             // ---------------- phase G: S-step Grams with the new X, W
-            acc_zero(x, 8 * k * k);
-            stream_grams_partial(x);
-            if (!publish_sync(x, 8 * k * k)) return;
+            acc_zero(x, 2 * nops * k * k);
+            stream_grams_partial(x, nops);
+            if (!publish_sync(x, 2 * nops * k * k)) return;
+        }
+        if (stream && HO) {
+            for (int d = 0; d < 2; ++d) {
+                reduce_into(x, d * k * k, k, k, sm->slot[SL_G0 + d]);
+                reduce_into(x, (2 + d) * k * k, k, k, sm->slot[SL_C0 + d]);
+            }
+            rk4_small_s(x);
+        }
+        if (stream && !HO) {
             for (int d = 0; d < 4; ++d) {
                 reduce_into(x, d * k * k, k, k, sm->slot[SL_G0 + d]);
                 reduce_into(x, (4 + d) * k * k, k, k, sm->slot[SL_C0 + d]);

@@ -161,9 +161,33 @@ __device__ inline void stencil_tile(const Ctx& x, const double* A, int r0, int n
     }
 }
 
-// Sparse P_N operators applied to rows [r0, r0+nr) of B (N x KM): t[d] = A_d B.
-__device__ inline void spmm_tile(const Ctx& x, const double* B, int r0, int nr, int k, double (*t)[TR * KM]) {
-    for (int e = threadIdx.x; e < NOPS * nr * k; e += NT) {
+// Central stencils only (the RK4 integrator's streaming): t[0] = L2x A,
+// t[1] = L2y A on rows [r0, r0+nr); zero on boundary rows.
+__device__ inline void stencil2_tile(const Ctx& x, const double* A, int r0, int nr, int k, double (*t)[TR * KM]) {
+    const DevProblem& P = x.P;
+    const double hx = 0.5 / P.dx, hy = 0.5 / P.dy;
+    for (int e = threadIdx.x; e < nr * k; e += NT) {
+        int r = e / k, j = e - (e / k) * k;
+        int c = r0 + r;
+        double l2x = 0.0, l2y = 0.0;
+        if (!is_bnd(P, c)) {
+            double axm = ldcg(A + (size_t)(c - P.ny) * KM + j) * P.rinv[c - P.ny];
+            double axp = ldcg(A + (size_t)(c + P.ny) * KM + j) * P.rinv[c + P.ny];
+            double aym = ldcg(A + (size_t)(c - 1) * KM + j) * P.rinv[c - 1];
+            double ayp = ldcg(A + (size_t)(c + 1) * KM + j) * P.rinv[c + 1];
+            l2x = (axp - axm) * hx;
+            l2y = (ayp - aym) * hy;
+        }
+        t[0][r * KM + j] = l2x;
+        t[1][r * KM + j] = l2y;
+    }
+}
+
+// Sparse P_N operators applied to rows [r0, r0+nr) of B (N x KM): t[d] = A_d B
+// for the first `nops` operators (Ax, Az, |Ax|, |Az|).
+__device__ inline void spmm_tile(const Ctx& x, const double* B, int r0, int nr, int k, double (*t)[TR * KM],
+                                 int nops = NOPS) {
+    for (int e = threadIdx.x; e < nops * nr * k; e += NT) {
         int d = e / (nr * k);
         int rem = e - d * nr * k;
         int r = rem / k, j = rem - (rem / k) * k;

@@ -114,6 +114,7 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
     P.prof = nullptr;
     P.zero_smem = 0;
+    P.precision = opt ? opt->precision : TITUS_PRECISION_FP64;
     s->take_debug_hooks(P);
     if (opt && opt->profile) {
         CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));
@@ -458,6 +459,7 @@ int titus_host::batch_launch(titus_batch* b, int method, const titus_options_t* 
     if (opt && opt->rank_tol > 0) P.rank_tol = opt->rank_tol;
     P.prof = nullptr;
     P.zero_smem = 0;
+    P.precision = opt ? opt->precision : TITUS_PRECISION_FP64;
     s->take_debug_hooks(P);
     if (opt && opt->profile) {
         CK(cudaMemsetAsync(s->prof, 0, PF_SLOTS * sizeof(unsigned long long), stream));

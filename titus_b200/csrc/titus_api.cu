@@ -228,6 +228,24 @@ static int create_impl(const titus_problem_t* pb, titus_solver* s) {
     CK(cudaMemcpy(s->d_st, &st, sizeof(TeamState), cudaMemcpyHostToDevice));
     CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sizeof(SmemLayout)));
+    CK(cudaFuncSetAttribute(dlr_kernel<TITUS_DLR_HIGH_ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(SmemLayout)));
+    return TITUS_OK;
+}
+
+static_assert(TITUS_DLR_HIGH_ORDER == titus::kHighOrder, "method id of the RK4 kernel");
+static bool is_fixed_family(int method) { return method == TITUS_DLR_FIXED || method == TITUS_DLR_HIGH_ORDER; }
+
+// The RK4 integrator's stage buffers (3 x n x KM and 3 x N x KM), allocated on
+// its first use.
+static int ensure_rk4_buffers(titus_solver* s) {
+    if (s->st.Y) return TITUS_OK;
+    int rc;
+    if ((rc = s->alloc(&s->st.Y, (size_t)3 * s->n * KM)) || (rc = s->alloc(&s->st.Z, (size_t)3 * s->N * KM))) {
+        s->st.Y = s->st.Z = nullptr;   // both stay tracked in allocs and are freed with the handle
+        return rc;
+    }
+    CK(cudaMemcpy(s->d_st, &s->st, sizeof(TeamState), cudaMemcpyHostToDevice));
     return TITUS_OK;
 }
 
@@ -283,14 +301,22 @@ static int init_state(titus_solver* s, int r, cudaStream_t stream) {
 
 static int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin, int n_end, int dose2_pending,
                   cudaStream_t stream) {
-    if (method != TITUS_DLR_FIXED) return fail(TITUS_ERR_ARG, "unknown method %d", method);
+    if (!is_fixed_family(method)) return fail(TITUS_ERR_ARG, "unknown method %d", method);
     if (s->r > KM)
         return fail(TITUS_ERR_LIMIT, "fixed-rank integrator: rank %d > %d supported by this build", s->r, KM);
+    const bool ho = method == TITUS_DLR_HIGH_ORDER;
+    if (ho && (s->P.nx < 5 || s->P.ny < 5))
+        return fail(TITUS_ERR_ARG, "RK4 integrator: the limited flux needs nx, ny >= 5 (got %d x %d)", s->P.nx, s->P.ny);
+    if (ho) {
+        int rc = ensure_rk4_buffers(s);
+        if (rc) return rc;
+    }
+    void* kfn = ho ? (void*)dlr_kernel<TITUS_DLR_HIGH_ORDER> : (void*)dlr_kernel<TITUS_DLR_FIXED>;
     int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : s->team_ctas;
     G = std::min(G, s->num_sms);
     G = std::max(G, 1);
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dlr_kernel<TITUS_DLR_FIXED>, NT, sizeof(SmemLayout)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, NT, sizeof(SmemLayout)));
     if (per_sm < 1) return fail(TITUS_ERR_CUDA, "kernel does not fit on an SM (smem %zu)", sizeof(SmemLayout));
     if (G > per_sm * s->num_sms) G = per_sm * s->num_sms;
     DevProblem P = s->P;
@@ -307,8 +333,7 @@ static int launch(titus_solver* s, int method, const titus_options_t* opt, int n
     CK(cudaMemsetAsync(s->st.diag, 0, 16 * sizeof(double), stream));
     TeamState* dst = s->d_st;
     void* args[] = {&P, &dst, &G, &n_begin, &n_end, &dose2_pending};
-    CK(cudaLaunchCooperativeKernel((void*)dlr_kernel<TITUS_DLR_FIXED>, dim3(G), dim3(NT), args, sizeof(SmemLayout),
-                                   stream));
+    CK(cudaLaunchCooperativeKernel(kfn, dim3(G), dim3(NT), args, sizeof(SmemLayout), stream));
     s->last_method = method;
     s->last_G = G;
     return TITUS_OK;
@@ -348,14 +373,24 @@ static int end_index(const titus_solver* s, const titus_options_t* opt, int n_be
     return n_end;
 }
 
+// precision must be a titus_precision_t; MIXED exists for the adaptive integrators only
+static int check_precision(int method, const titus_options_t* opt) {
+    const int p = opt ? opt->precision : TITUS_PRECISION_FP64;
+    if (p != TITUS_PRECISION_FP64 && p != TITUS_PRECISION_MIXED) return fail(TITUS_ERR_ARG, "unknown precision %d", p);
+    if (p == TITUS_PRECISION_MIXED && method != TITUS_PARALLEL_ADAPTIVE && method != TITUS_BUG_ADAPTIVE)
+        return fail(TITUS_ERR_ARG, "MIXED precision applies to the adaptive integrators (method 1 or 2), got %d", method);
+    return TITUS_OK;
+}
+
 extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus_options_t* opt, void* stream_) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (int rc = check_precision(method, opt)) return rc;
     cudaStream_t stream = (cudaStream_t)stream_;
     if (method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE) {
         s->last_method = method;
         return titus_host::wide_solve_device(s, method, opt, stream);
     }
-    if (method != TITUS_DLR_FIXED) return fail(TITUS_ERR_ARG, "unknown method %d", method);
+    if (!is_fixed_family(method)) return fail(TITUS_ERR_ARG, "unknown method %d", method);
     int rc = init_state(s, s->r, stream);
     if (rc) return rc;
     return launch(s, method, opt, 2, end_index(s, opt, 2), 0, stream);
@@ -444,6 +479,7 @@ extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X,
 extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t n_stop,
                                 titus_result_t* res) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (int rc = check_precision(method, opt)) return rc;
     if (method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE) {
         s->last_method = method;
         int rc = titus_host::wide_solve_from(s, method, opt, n_stop);
@@ -467,6 +503,7 @@ extern "C" int titus_solve_batched(titus_solver_t* s, int32_t method, const titu
     if (!s || !spots || !dose_out) return fail(TITUS_ERR_ARG, "NULL argument");
     if (method != TITUS_PARALLEL_ADAPTIVE && method != TITUS_BUG_ADAPTIVE)
         return fail(TITUS_ERR_ARG, "batched solves run the adaptive integrators (method 1 or 2), got %d", method);
+    if (int rc = check_precision(method, opt)) return rc;
     if (nspots < 1) return fail(TITUS_ERR_ARG, "nspots < 1");
     s->last_method = method;
     return titus_host::wide_solve_batched(s, method, opt, nspots, spots, dose_out, rank_out, iters_out);
@@ -484,6 +521,7 @@ extern "C" int titus_batch_solve_device(titus_batch_t* b, int32_t method, const 
     if (!b) return fail(TITUS_ERR_ARG, "batch is NULL");
     if (method != TITUS_PARALLEL_ADAPTIVE && method != TITUS_BUG_ADAPTIVE)
         return fail(TITUS_ERR_ARG, "batched solves run the adaptive integrators (method 1 or 2), got %d", method);
+    if (int rc = check_precision(method, opt)) return rc;
     return titus_host::batch_launch(b, method, opt, (cudaStream_t)stream);
 }
 

@@ -11,15 +11,16 @@
 // offsets -2..+1 where the ordinate's component is >= 0, -1..+2 where it is
 // negative. A thread owns one (j, l) pair and walks 32 rows along x: a warp
 // reads 256 contiguous bytes per operand, rows shared by neighbouring blocks
-// stay in L2, and DRAM sees phi once and flux once. The arithmetic uses the _rn
-// intrinsics in the reference's evaluation order (no FMA contraction), so the
-// result is the same IEEE double as the FP64 restatement of the loop body.
+// stay in L2, and DRAM sees phi once and flux once. The limiter arithmetic
+// (limiter.cuh) keeps the reference's evaluation order, so the result is the
+// same IEEE double as the FP64 restatement of the loop body.
 #include <cuda_runtime.h>
 
 #include <climits>
 #include <cstdint>
 
 #include "../../include/titus.h"
+#include "limiter.cuh"
 
 namespace titus_host {
 int fail(int code, const char* fmt, ...);
@@ -29,39 +30,13 @@ namespace {
 
 constexpr int kFluxThreads = 256;
 
-// minmod(x, y) = x < 0 ? clamp(y, x, 0) : clamp(y, 0, x), where Julia's
-// clamp(v, lo, hi) is v > hi ? hi : (v < lo ? lo : v)  (SolverCSD.jl:288).
-// (An fmin/fmax form gives the same values but costs more instructions.)
-__device__ __forceinline__ double minmod(double x, double y) {
-    const double lo = x < 0.0 ? x : 0.0;
-    const double hi = x < 0.0 ? 0.0 : x;
-    return y > hi ? hi : (y < lo ? lo : y);
-}
+using titus_lim::face_neg;
+using titus_lim::face_pos;
 
-// slopefit(l, c, r) = minmod(2 (r - c), minmod((r - l) / 2, 2 (c - l)))  (:290-293)
-__device__ __forceinline__ double slopefit(double l, double c, double r) {
-    const double tmp = minmod(__dmul_rn(0.5, __dsub_rn(r, l)), __dmul_rn(2.0, __dsub_rn(c, l)));
-    return minmod(__dmul_rn(2.0, __dsub_rn(r, c)), tmp);
-}
-
-// Face values. F+(a) = phi_a + slopefit(phi_{a-1}, phi_a, phi_{a+1})/2 is the
-// face between cells a and a+1 for a component >= 0; F-(a) = phi_a -
-// slopefit(phi_{a-1}, phi_a, phi_{a+1})/2 the face between a-1 and a for a
-// negative one. The reference's difference for cell i is F+(i) - F+(i-1)
-// (s1..s4 = offsets -2..+1, :309-331) or F-(i+1) - F-(i) (offsets -1..+2,
-// :333-355): with H(a) = the face between a and a+1 (F+(a), or F-(a+1)) both
-// read H(i) - H(i-1), and H(i) of one cell is H(i-1) of the next.
-__device__ __forceinline__ double face_pos(double m1, double c, double p1) {
-    return __dadd_rn(c, __dmul_rn(0.5, slopefit(m1, c, p1)));
-}
-__device__ __forceinline__ double face_neg(double m1, double c, double p1) {
-    return __dsub_rn(c, __dmul_rn(0.5, slopefit(m1, c, p1)));
-}
 // y difference of one cell from its four neighbours (the face is not shared:
 // adjacent j belong to other threads)
 __device__ __forceinline__ double diff_y(double m2, double m1, double c, double p1, double p2, bool pos) {
-    return pos ? __dsub_rn(face_pos(m1, c, p1), face_pos(m2, m1, c))
-               : __dsub_rn(face_neg(c, p1, p2), face_neg(m1, c, p1));
+    return titus_lim::axis_diff(m2, m1, c, p1, p2, pos);
 }
 
 constexpr int kRowsPerThread = 32;

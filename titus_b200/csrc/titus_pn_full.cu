@@ -290,6 +290,8 @@ void titus_host::pn_free(titus_solver* s) {
 
 extern "C" int titus_pn_full_solve_device(titus_solver_t* s, const titus_options_t* opt, void* stream_) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (opt && opt->precision != TITUS_PRECISION_FP64)
+        return fail(TITUS_ERR_ARG, "the full-rank P_N solver runs in FP64 only (precision %d)", opt->precision);
     int rc = pn_ensure(s);
     if (rc) return rc;
     titus_pn_state* st = s->pn;

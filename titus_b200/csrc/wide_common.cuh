@@ -11,6 +11,7 @@
 // take the same control decisions (ranks, rejections) without a broadcast.
 #pragma once
 #include "dlr_device.cuh"
+#include "umma.cuh"
 
 namespace titus {
 namespace wide {
@@ -98,6 +99,8 @@ struct WSmem {
     double wnrm[RA];
     int perm[KA];
     double sig[KA];
+    unsigned long long mbar[2];   // MIXED mode: completion barriers of the two tensor-core chunk buffers
+    unsigned tmem_slot;           // MIXED mode: TMEM base address written by tcgen05.alloc
 };
 
 // Per-side bookkeeping of one augmentation (identical in every CTA).
@@ -127,7 +130,12 @@ struct WCtx {
     int cur_n;
     unsigned long long* prof;
     SideInfo side[2];
+    int mixed;           // 1: MIXED precision (tensor-core operator Grams where the width >= 32)
+    umma::TcCtx tc;      // tensor-core state (MIXED only)
 };
+
+// Widths from which the MIXED mode forms the operator Grams on the tensor cores.
+constexpr int kTcMinWidth = 32;
 
 // Rows per tile that fit `avail` doubles of shared memory at `per_row` doubles a row.
 __device__ __forceinline__ int rows_fit(int avail, int per_row) {

@@ -27,10 +27,13 @@ from . import physics as ph
 
 
 class SolverCSD:
-    def __init__(self, settings, team_ctas: int = 0):
+    def __init__(self, settings, team_ctas: int = 0, precision: int = _lib.TITUS_PRECISION_FP64):
         s = settings
         self.settings = s
         self.team_ctas = team_ctas
+        # TITUS_PRECISION_FP64 or TITUS_PRECISION_MIXED (tensor-core operator
+        # Grams of the adaptive integrators; see include/titus.h)
+        self.precision = precision
         nx, ny = s.NCellsX, s.NCellsY
         self.n = nx * ny
         npn = s.nPN
@@ -207,6 +210,7 @@ class SolverCSD:
         o.max_steps = max_steps
         o.rank_tol = rank_tol
         o.profile = 1 if profile else 0
+        o.precision = self.precision
         return o
 
     def profile(self):
@@ -370,6 +374,17 @@ def SolveFirstCollisionSource(solver: SolverCSD, max_steps: int = 0):
 def SolveFirstCollisionSourceDLR(solver: SolverCSD, max_steps: int = 0):
     """Fixed-rank DLR (``SolverCSD.jl:891-1120``) on the GPU."""
     out = solver.run(_lib.TITUS_DLR_FIXED, max_steps=max_steps)
+    res = solver.outputs(out)
+    solver.dose = res[4]
+    return res
+
+
+def SolveFirstCollisionSourceDLRHighOrder(solver: SolverCSD, max_steps: int = 0):
+    """Fixed-rank DLR with RK4 streaming (``SolverCSD.jl:588-889``) on the GPU:
+    inflow on the two outer layers, the second-order limited sweep
+    (``solveFlux!``) and RK4 K/L/S streaming with the central operators. Same
+    return tuple as ``SolveFirstCollisionSourceDLR``."""
+    out = solver.run(_lib.TITUS_DLR_HIGH_ORDER, max_steps=max_steps)
     res = solver.outputs(out)
     solver.dose = res[4]
     return res
