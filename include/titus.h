@@ -39,6 +39,9 @@ extern "C" {
 #define TITUS_PARALLEL_ADAPTIVE 1
 #define TITUS_BUG_ADAPTIVE 2
 #define TITUS_DLR_HIGH_ORDER 3
+/* The full-rank P_N first-collision sweep (SolveFirstCollisionSource,
+ * SolverCSD.jl:465-586); the method of titus_dose_adjoint. */
+#define TITUS_PN_FULL 4
 
 /* Assembled problem. Replaces the fields of `SolverCSD{T}` that the energy
  * loop reads (SolverCSD.jl:20-146) plus the per-step tables the loop derives
@@ -275,6 +278,25 @@ int titus_pn_full_solve_device(titus_solver_t* solver, const titus_options_t* op
 int titus_pn_full_fetch(titus_solver_t* solver, double* u_out, double* dose_out, double* psi_out);
 int titus_pn_full_solve(titus_solver_t* solver, const titus_options_t* options, double* u_out, double* dose_out,
                         double* psi_out);
+
+/* Dose objective and its gradients (no counterpart in the reference, which
+ * has no adjoint): J = sum_c weight[c] (dose[c] - target[c])^2 of the sweep's
+ * dose, or any J whose dJ/d(dose) the caller passes in dj_ddose (then weight
+ * and target are ignored and *objective_out is NaN). Returns the dose (n), J,
+ * dJ/drho per cell (n) and dJ/dprofile (n): the sensitivity to PsiBeam's
+ * spatial factor problem->bc_space, nonzero on boundary cells only -- for a
+ * plan whose profile is sum_s w_s p_s, dJ/dw_s = p_s . dJ/dprofile. The
+ * energy grid and PsiBeam's rho_min are held fixed (they follow min(rho) when
+ * the problem is built). method: TITUS_PN_FULL, the exact discrete adjoint of
+ * titus_pn_full_solve's sweep, transposed stencils and P_N products run from
+ * the last energy step back to the first; checkpoint_every = k keeps (u, psi)
+ * entering every k-th step from one forward pass and recomputes each segment
+ * (0 = about sqrt(steps)); device memory about (steps/k + k + 12) n N words.
+ * weight, target, dj_ddose and the outputs are host arrays (NULL weight = 1,
+ * NULL target = 0, NULL outputs are skipped). Synchronous. FP64 only. */
+int titus_dose_adjoint(titus_solver_t* solver, int32_t method, const titus_options_t* options, const double* weight,
+                       const double* target, const double* dj_ddose, int32_t checkpoint_every, double* objective_out,
+                       double* dose_out, double* grad_density, double* grad_profile);
 
 /* Test hooks (no counterpart in the reference), for failure-detection tests
  * that fault nothing.

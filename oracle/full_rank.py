@@ -97,27 +97,78 @@ def _pn_step_pieces(solver: SolverCSD, n: int):
     return dE, D, Dvec, c
 
 
-def pn_full_dose_adjoint(solver: SolverCSD, g, max_steps: int | None = None):
-    """Discrete adjoint of ``solve_pn_full``'s dose, density gradient.
+def inflow_factor(solver: SolverCSD, E: float, n: int):
+    """PsiBeam without its spatial factor: the inflow of every reduced ordinate
+    at energy E with csd.S[n-1] (``SolverCSD.jl:275``), so that the boundary
+    value of cell c is ``bc_profile[c] * inflow_factor``."""
+    s = solver.settings
+    Om = solver.qReduced
+    ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - Om[:, 0]) ** 2) * np.exp(-s.sigmaO3Inv * (s.Omega3 - Om[:, 2]) ** 2)
+    return solver.psi_scale * ang * math.exp(-s.sigmaEInv * (s.eMax - E) ** 2) * solver.csd.S[n - 1] * s.densityMin
 
-    For a dose objective J with dJ/d(dose) = g (n cells) this returns
-    (dose, dJ/drho) with rho the cell densities, at a fixed energy grid (the
-    tau step follows min(rho) when Settings is built and stays fixed here) and
-    a fixed PsiBeam scale (densityMin is a setting). It is the exact transpose
-    of the forward recursion, run from the last energy step back to the first:
 
-    * forward step n: V_d = u A_d, uT = u - dE sum_d L_d V_d with the stencils
-      L_d = Ltilde_d diag(1/rho) (stencils.jl: every entry carries 1/rho of its
-      column cell), boundary rows zero, u' = P_int (uT + src) / (1 + dE D),
-      dose += c_n (u'[:,0] + uOUnc) / rho; psi does not depend on rho or u;
+def beam_profile(settings, x0: float | None = None, y0: float | None = None):
+    """Spatial factor of PsiBeam at every cell (row i*ny + j) for a beam centred at (x0, y0)."""
+    s = settings
+    x0 = s.x0 if x0 is None else x0
+    y0 = s.y0 if y0 is None else y0
+    xm = s.xMid[np.arange(s.NCellsX * s.NCellsY) // s.NCellsY]
+    ym = s.yMid[np.arange(s.NCellsX * s.NCellsY) % s.NCellsY]
+    return np.exp(-s.sigmaXInv * (xm - x0) ** 2) * np.exp(-s.sigmaYInv * (ym - y0) ** 2)
+
+
+def flux_upwind_T(solver: SolverCSD, w):
+    """Transpose of ``solver.flux_upwind`` (the interior-cell upwind differences
+    of ``solveFluxUpwind!``, ``SolverCSD.jl:388-463``) applied to w (nx, ny, q)."""
+    s = solver.settings
+    ax = solver.qReduced[:, 0] / s.dx
+    az = solver.qReduced[:, 2] / s.dy
+    px = solver.qReduced[:, 0] >= 0.0
+    pz = solver.qReduced[:, 2] >= 0.0
+    W = w[1:-1, 1:-1, :]
+    out = np.zeros_like(w)
+    # ew = c - xm (Omega_x >= 0) or xp - c: coefficient +ax on c and -ax on xm, or +ax on xp and -ax on c
+    out[1:-1, 1:-1, :] += np.where(px, ax * W, -ax * W)
+    out[:-2, 1:-1, :] += np.where(px, -ax * W, 0.0)
+    out[2:, 1:-1, :] += np.where(px, 0.0, ax * W)
+    out[1:-1, 1:-1, :] += np.where(pz, az * W, -az * W)
+    out[1:-1, :-2, :] += np.where(pz, -az * W, 0.0)
+    out[1:-1, 2:, :] += np.where(pz, 0.0, az * W)
+    return out
+
+
+def pn_full_dose_adjoint(solver: SolverCSD, g, max_steps: int | None = None, bc_profile=None):
+    """Discrete adjoint of ``solve_pn_full``'s dose: gradients of a dose
+    objective J with respect to the cell densities and to the inflow profile.
+
+    ``g`` is dJ/d(dose) (n cells), or a callable taking the dose and returning
+    it. ``bc_profile`` (n) replaces PsiBeam's spatial factor on the boundary
+    cells (a weighted sum of spot profiles for a treatment plan; None keeps the
+    settings' beam). Returns (dose, dJ/drho, dJ/dprofile): the last is nonzero
+    on boundary cells only, and for a plan with profile sum_s w_s p_s the
+    spot-weight gradient is p_s . dJ/dprofile. The energy grid (the tau step
+    follows min(rho) when Settings is built) and PsiBeam's rho_min stay fixed.
+
+    It is the exact transpose of the forward recursion, run from the last
+    energy step back to the first:
+
+    * forward step n: psi_bc = inflow on boundary cells, psi' = (psi_bc - dE F
+      psi_bc) / (1 + dE sigma_0); V_d = u A_d, uT = u - dE sum_d L_d V_d with
+      the stencils L_d = Ltilde_d diag(1/rho) (stencils.jl: every entry carries
+      1/rho of its column cell), boundary rows zero, u' = P_int (uT + dE Dvec .
+      (MReduced psi')) / (1 + dE D), dose += c_n (u'[:,0] + uOUnc) / rho;
     * backward: lambda (adjoint of u') gets g c_n / rho in its moment 0;
       mu = P_int lambda / (1 + dE D); Y_d = L_d^T mu;
       dJ/drho += (dE / rho) sum_d rowsum(Y_d * V_d);
       lambda <- mu - dE sum_d Y_d A_d^T (the adjoint of the previous u);
+      psibar' += P_int (dE (mu Dvec) MReduced + g c_n / rho MReduced[0, :]);
+      psibar_bc = (psibar' - dE F^T psibar') / (1 + dE sigma_0); its boundary
+      cells are the inflow's sensitivity (dJ/dprofile += psibar_bc . inflow
+      factor), its interior cells carry to the previous step;
     * the explicit 1/rho of the dose adds -g dose / rho.
 
-    The oracle keeps every step's V_d in memory, so it is for small cases
-    (the GPU path checkpoints u and recomputes). TEST INFRASTRUCTURE ONLY.
+    The oracle keeps every step's u in memory, so it is for small cases (the
+    GPU path checkpoints u and psi and recomputes). TEST INFRASTRUCTURE ONLY.
     """
     s = solver.settings
     eTrafo = solver.csd.eTrafo
@@ -136,18 +187,23 @@ def pn_full_dose_adjoint(solver: SolverCSD, g, max_steps: int | None = None):
     inner = np.zeros((nx, ny), dtype=bool)
     inner[1:-1, 1:-1] = True
     inner = inner.ravel()
+    bmask = ~inner.reshape(nx, ny)
     rho = solver.densityVec
     dose = np.zeros(n_cells)
     last = nE if max_steps is None else min(nE, 1 + max_steps)
-    V_hist = {}
+    prof = None if bc_profile is None else np.asarray(bc_profile, dtype=np.float64).reshape(nx, ny)
+    u_hist = {}
     for n in range(2, last + 1):
         sig, Dvec, D = sigma_vectors(solver, n)
         dE = eTrafo[n - 1] - eTrafo[n - 2]
-        solver.apply_bc(psi, energy[n - 1], n - 1)
+        if prof is None:
+            solver.apply_bc(psi, energy[n - 1], n - 1)
+        else:
+            psi[bmask, :] = prof[bmask][:, None] * inflow_factor(solver, energy[n - 1], n - 1)[None, :]
         psi = psi - dE * solver.flux_upwind(psi)
         psi_new = psi / (1.0 + dE * sig[0])
         V = [np.asarray((A.T @ u.T).T) for A in ops]
-        V_hist[n] = V
+        u_hist[n] = u
         uT = u - dE * sum(L @ Vd for L, Vd in zip(Ls, V))
         uT[bnd, :] = 0.0
         pv = psi_new.reshape(n_cells, -1)
@@ -159,16 +215,28 @@ def pn_full_dose_adjoint(solver: SolverCSD, g, max_steps: int | None = None):
         dose += c * (u_new[:, 0] + u_unc) / rho
         u = u_new
         psi = psi_new
-    g = np.asarray(g, dtype=np.float64)
+    g = np.asarray(g(dose) if callable(g) else g, dtype=np.float64)
     lam = np.zeros((n_cells, N))
+    psibar = np.zeros((nx, ny, Mr.shape[1]))
     grad = np.zeros(n_cells)
+    gprof = np.zeros((nx, ny))
     for n in range(last, 1, -1):
-        dE, D, _, c = _pn_step_pieces(solver, n)
+        dE, D, Dvec, c = _pn_step_pieces(solver, n)
+        sig, _, _ = sigma_vectors(solver, n)
         lam[:, 0] += g * c / rho
         mu = lam / (1.0 + dE * D)[None, :]
         mu[~inner, :] = 0.0
         Y = [np.asarray(L.T @ mu) for L in Ls]
-        grad += (dE / rho) * sum(np.sum(Yd * Vd, axis=1) for Yd, Vd in zip(Y, V_hist[n]))
+        V = [np.asarray((A.T @ u_hist[n].T).T) for A in ops]
+        grad += (dE / rho) * sum(np.sum(Yd * Vd, axis=1) for Yd, Vd in zip(Y, V))
         lam = mu - dE * sum(np.asarray((A @ Yd.T).T) for A, Yd in zip(ops, Y))
+        # psi' feeds the in-scattering source and uOUnc of interior cells
+        pb = psibar.reshape(n_cells, -1)
+        pb[inner] += dE * (mu[inner] * Dvec[None, :]) @ Mr + np.outer(g[inner] * c / rho[inner], Mr[0, :])
+        w = psibar / (1.0 + dE * sig[0])
+        pbc = w - dE * flux_upwind_T(solver, w)
+        gprof[bmask] += pbc[bmask] @ inflow_factor(solver, energy[n - 1], n - 1)
+        pbc[bmask, :] = 0.0
+        psibar = pbc
     grad += -g * dose / rho
-    return dose, grad
+    return dose, grad, gprof.ravel()

@@ -1,6 +1,6 @@
 """titus_b200: B200-native (sm_100a) CSD energy step of TITUS behind its Settings/SolverCSD/Solve* API."""
 from .settings import Settings  # noqa: F401
-from .solver import (PencilBeamBatch, SolveBatchedPencilBeams, SolverCSD, SolveFirstCollisionSource,  # noqa: F401
+from .solver import (DoseAdjoint, PencilBeamBatch, SolveBatchedPencilBeams, SolverCSD, SolveFirstCollisionSource,  # noqa: F401
                      SolveFirstCollisionSourceDLR, SolveFirstCollisionSourceDLRHighOrder,
                      SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel, scalar_flux)
 from .spots import partition, plan_dose, plan_objective  # noqa: F401

@@ -18,6 +18,7 @@ TITUS_DLR_FIXED = 0
 TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
 TITUS_DLR_HIGH_ORDER = 3
+TITUS_PN_FULL = 4
 TITUS_PRECISION_FP64 = 0
 TITUS_PRECISION_MIXED = 1
 # exclusive device timers (titus_profile order); "other" is time outside every named phase
@@ -92,6 +93,8 @@ SIGNATURES = [
     ("titus_pn_full_solve_device", C.c_int, [C.c_void_p, C.POINTER(Options), C.c_void_p]),
     ("titus_pn_full_fetch", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     ("titus_pn_full_solve", C.c_int, [C.c_void_p, C.POINTER(Options), _dp, _dp, _dp]),
+    ("titus_dose_adjoint", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), _dp, _dp, _dp, C.c_int32, _dp, _dp,
+                                     _dp, _dp]),
     ("titus_debug_barrier_fault", C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
     ("titus_debug_fail_alloc", C.c_int, [C.c_int32]),
     ("titus_debug_tc_gram", C.c_int, [_dp, C.c_int32, C.c_int32, C.c_int32, _dp]),

@@ -204,6 +204,26 @@ class SolverCSD:
         except Exception:
             pass
 
+    def set_beam_profile(self, profile):
+        """Replace PsiBeam's spatial factor (read on the boundary cells) by
+        ``profile`` (n cells, row i*ny + j), e.g. a weighted sum of spot
+        profiles; the device handle is rebuilt on next use."""
+        profile = np.ascontiguousarray(profile, dtype=np.float64).reshape(self.n)
+        if not np.all(np.isfinite(profile)):
+            raise ValueError("beam profile must be finite")
+        self.bc_space = profile
+        self.close()
+
+    def beam_profile(self, x0=None, y0=None):
+        """PsiBeam's spatial factor at every cell for a beam centred at (x0, y0)
+        (defaults: the settings' beam)."""
+        s = self.settings
+        x0 = s.x0 if x0 is None else x0
+        y0 = s.y0 if y0 is None else y0
+        xm = s.xMid[np.arange(self.n) // s.NCellsY]
+        ym = s.yMid[np.arange(self.n) % s.NCellsY]
+        return np.exp(-s.sigmaXInv * (xm - x0) ** 2) * np.exp(-s.sigmaYInv * (ym - y0) ** 2)
+
     def options(self, max_steps=0, rank_tol=0.0, profile=False):
         o = _lib.Options()
         o.team_ctas = self.team_ctas
@@ -369,6 +389,42 @@ def SolveFirstCollisionSource(solver: SolverCSD, max_steps: int = 0):
     solver.dose = dose
     s = solver.settings
     return 0.5 * math.sqrt(solver.gamma[0]) * u, dose, psi.reshape(s.NCellsX, s.NCellsY, solver.q)
+
+
+def DoseAdjoint(solver: SolverCSD, weight=None, target=None, dj_ddose=None, checkpoint_every: int = 0,
+                max_steps: int = 0):
+    """Dose objective of the full-rank sweep and its gradients, by the
+    discrete adjoint on the GPU (``titus_dose_adjoint``, method TITUS_PN_FULL).
+
+    J = sum_c weight[c] (dose[c] - target[c])^2 (weight None = 1, target None =
+    0), or any J given through ``dj_ddose``. Returns ``(J, dose, dJ/drho,
+    dJ/dprofile)``; for a plan set with ``solver.set_beam_profile(sum_s w_s
+    p_s)`` the spot-weight gradient is ``p_s @ dJ/dprofile``. The (u, psi)
+    state is checkpointed every ``checkpoint_every`` energy steps (0 = about
+    sqrt(steps)) and recomputed between checkpoints.
+    """
+    lib = _lib.load()
+    h = solver.handle()
+    n = solver.n
+
+    def arr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(n)
+        return a
+
+    w, t, g = arr(weight), arr(target), arr(dj_ddose)
+    dose = np.zeros(n)
+    gr = np.zeros(n)
+    gp = np.zeros(n)
+    J = C.c_double(0.0)
+    opt = solver.options(max_steps)
+    nul = C.POINTER(C.c_double)()
+    _lib.check(lib.titus_dose_adjoint(h, _lib.TITUS_PN_FULL, C.byref(opt), nul if w is None else _lib.as_dp(w),
+                                      nul if t is None else _lib.as_dp(t), nul if g is None else _lib.as_dp(g),
+                                      int(checkpoint_every), C.byref(J), _lib.as_dp(dose), _lib.as_dp(gr),
+                                      _lib.as_dp(gp)), "titus_dose_adjoint")
+    return J.value, dose, gr, gp
 
 
 def SolveFirstCollisionSourceDLR(solver: SolverCSD, max_steps: int = 0):
