@@ -42,6 +42,13 @@ extern "C" {
 /* The full-rank P_N first-collision sweep (SolveFirstCollisionSource,
  * SolverCSD.jl:465-586); the method of titus_dose_adjoint. */
 #define TITUS_PN_FULL 4
+/* SolveFirstCollisionSourceDLRParallelRejection (SolverCSD.jl:2376-2742): the
+ * parallel integrator's augmented step with the BUG loop's rejections. Where
+ * the reference's next step raises a DimensionMismatch (a scattering
+ * rejection after a streaming step that changed the rank, :2553, :2662-2665)
+ * the solve stops with TITUS_ERR_DEVICE. Plain solves and titus_solve_from
+ * only (not batched). */
+#define TITUS_PARALLEL_REJECTION 5
 
 /* Assembled problem. Replaces the fields of `SolverCSD{T}` that the energy
  * loop reads (SolverCSD.jl:20-146) plus the per-step tables the loop derives

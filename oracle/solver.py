@@ -719,3 +719,182 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict |
     bound_hist = np.array([etaVecTime, etaBoundVec], dtype=float).T
     return (X @ U, 0.5 * math.sqrt(solver.gamma[0]) * Sig, solver.O @ (W @ V), W @ V, solver.dose,
             rank_hist, eta_hist, bound_hist, psi)
+
+
+class ReferenceFailure(RuntimeError):
+    """The reference loop raises an error at this point of the sweep."""
+
+
+def solve_dlr_parallel_rejection(solver: SolverCSD, max_steps: int | None = None, state: dict | None = None,
+                                 n_begin: int = 2, return_state: bool = False, on_iter=None):
+    """``SolveFirstCollisionSourceDLRParallelRejection`` (``SolverCSD.jl:2376-2742``).
+
+    The parallel integrator's augmented step (``:2520-2558`` streaming,
+    ``:2600-2642`` scattering: ``S_new = [[Sbar, L^T W~], [X~^T K, 0]]``, then
+    ``truncate!``) inside the BUG loop's rejection logic (``:2561-2594``,
+    ``:2645-2668``). Readings of the reference, kept here:
+
+    * ``rmax`` (undefined, ``:2561, :2586, :2645, :2660``) is ``settings.r``,
+      as for the BUG loop;
+    * ``Sup`` (undefined in this function) appears only in the printed message
+      of the two rejections (``:2587, :2661``); the tests use ``norm(SUP)``,
+      and the message is read as printing that same bound;
+    * the loop runs ``while t < (nEnergies-1)*dE`` (``:2467``), not
+      ``nEnergies*dE`` as the BUG loop does;
+    * ``X0 = X; W0 = W; S0 = S`` (``:2518``) are aliases: the streaming K-step
+      (``:2532``; at n = 2 the in-scattering K-step, ``:2618``) zeroes X0's
+      boundary rows in place, and at n = 2 the out-scattering
+      ``S .= S2*Diagonal(S1)`` (``:2611``) rewrites S0. numpy's in-place
+      updates below keep the same aliasing;
+    * the first-branch rejections (``size(SUP,1) == 2r``, ``:2561, :2645``) do
+      not ``continue``: the truncated factors are kept and only ``n = n-1``
+      survives (the dose then uses ``S[n]`` of the decremented n);
+    * after a scattering rejection the basis is ``[X0 X~]`` with r0 + r'
+      columns (r0 entering the energy, r' after the streaming step) and the
+      reference sets ``r = 2r'`` (``:2662-2665``). When the streaming step
+      changed the rank (r0 != r') the repeated step's
+      ``SNew[1:r,1:r] .= SBar`` (``:2553``) raises a DimensionMismatch, so the
+      reference solve fails there; this restatement raises
+      :class:`ReferenceFailure` at the rejection instead.
+
+    Same arguments and returns as :func:`solve_dlr_bug`.
+    """
+    s = solver.settings
+    mode = solver.basis_mode
+    rmax = s.r
+    r = int(math.floor(s.r / 2))
+    eTrafo = solver.csd.eTrafo
+    energy = solver.csd.eGrid
+    psi = solver.setup_directions()
+    nx, ny = s.NCellsX, s.NCellsY
+    X, S, W = init_factors(solver, r)
+    bnd = solver.boundaryIdx
+    nE = eTrafo.size
+    dE = eTrafo[1] - eTrafo[0]
+    s.dE = dE
+    Mr = solver.MReduced
+    t = 0.0
+    n = 1
+    if state is not None:
+        X, S, W = state["X"].copy(), state["S"].copy(), state["W"].copy()
+        psi = state["psi"].reshape(psi.shape).copy()
+        solver.dose = state["dose"].copy()
+        r = S.shape[0]
+        t = state.get("t", (n_begin - 2) * dE)
+        n = n_begin - 1
+    timeVec, rankInTime, etaVec, etaVecTime, etaBoundVec = [], [], [], [], []
+    iters = 0
+    n_next = None
+    while t < (nE - 1) * dE:
+        n += 1
+        if n == nE:
+            n_next = n
+            break
+        if max_steps is not None and iters >= max_steps:
+            n_next = n
+            break
+        iters += 1
+        if on_iter is not None:
+            on_iter(r)
+        timeVec.append(energy[n - 1])
+        rankInTime.append(r)
+        sigma, Dvec, D = _step_prologue(solver, psi, X, S, W, n, dE)
+        X0, W0, S0 = X, W, S
+        if n > 2:
+            G = solver._x_grams(X, X)
+            C = solver._w_grams(W, W)
+            X[bnd, :] = 0.0
+            K = X @ S
+            K = solver._k_stream(K, *C, dE)
+            _, X1T = _augment_tilde(solver, X, K, "x")
+            L = W @ S.T
+            L = solver._l_stream(L, *G, dE)
+            _, W1T = _augment_tilde(solver, W, L, "w")
+            SBar = solver._s_stream(S, G, C, dE)
+            SNew = np.zeros((2 * r, 2 * r))
+            SNew[:r, :r] = SBar
+            SNew[r:, :r] = X1T.T @ K
+            SNew[:r, r:] = L.T @ W1T
+            Xa, Wa = np.column_stack([X, X1T]), np.column_stack([W, W1T])
+            XUP, SUP, WUP = solver.truncate(Xa, SNew, Wa)
+            if SUP.shape[0] == 2 * r and 2 * r < rmax:
+                r = 2 * r
+                n = n - 1
+            else:
+                Gt = solver._x_grams(X1T, X)
+                Ct = solver._w_grams(W, W1T)
+                eta = np.linalg.norm(Gt[0] @ S @ Ct[0] + Gt[1] @ S @ Ct[1] + Gt[2] @ S @ Ct[2] + Gt[3] @ S @ Ct[3])
+                etaVec.append(eta)
+                etaVecTime.append(energy[n - 1])
+                bound = s.c_eta * s.theta * max(1e-7, np.linalg.norm(SUP) ** s.thetaIndex) / dE
+                etaBoundVec.append(bound)
+                if eta > bound and 2 * r < rmax:
+                    S = (Xa.T @ X) @ S @ (W.T @ Wa)
+                    X, W = Xa, Wa
+                    r = 2 * r
+                    n = n - 1
+                    continue
+            S = SUP
+            X = XUP
+            W = WUP
+            r = S.shape[0]
+        # out scattering (S .= S2*Diagonal(S1): in place, so S0 follows at n = 2)
+        L = W @ S.T
+        L = L / (1.0 + dE * D)[:, None]
+        W, Snew = out_scatter_factor(L, mode, solver.w_completion)
+        S[...] = Snew
+        # in scattering
+        MtDW = Mr.T @ (Dvec[:, None] * W)
+        psiv = psi.reshape(nx * ny, -1)
+        Xtpsi = X.T @ psiv
+        X[bnd, :] = 0.0
+        K = X @ S
+        K = K + dE * psiv @ MtDW
+        K[bnd, :] = 0.0
+        _, X1T = _augment_tilde(solver, X, K, "x")
+        L = W @ S.T
+        L = L + dE * Dvec[:, None] * (Mr @ Xtpsi.T)
+        _, W1T = _augment_tilde(solver, W, L, "w")
+        SBar = S + dE * Xtpsi @ MtDW
+        SNew = np.zeros((2 * r, 2 * r))
+        SNew[:r, :r] = SBar
+        SNew[r:, :r] = X1T.T @ K
+        SNew[:r, r:] = L.T @ W1T
+        XUP, SUP, WUP = solver.truncate(np.column_stack([X, X1T]), SNew, np.column_stack([W, W1T]))
+        if SUP.shape[0] == 2 * r and 2 * r < rmax:
+            r = 2 * r
+            n = n - 1
+        else:
+            MtDWt = Mr.T @ (Dvec[:, None] * W1T)
+            Xtpsit = X1T.T @ psiv
+            eta = np.linalg.norm(Xtpsit @ MtDWt)
+            bound = s.c_eta * s.theta * max(1e-7, np.linalg.norm(SUP) ** s.thetaIndex) / dE
+            if eta > bound and 2 * r < rmax:
+                if X0.shape[1] != r:
+                    raise ReferenceFailure(f"scattering rejection at energy index {n} after the streaming step changed "
+                                           f"the rank ({X0.shape[1]} -> {r}): the reference's next step raises "
+                                           f"DimensionMismatch (SolverCSD.jl:2553)")
+                Xa, Wa = np.column_stack([X0, X1T]), np.column_stack([W0, W1T])
+                S = (Xa.T @ X0) @ S0 @ (W0.T @ Wa)
+                X, W = Xa, Wa
+                r = S.shape[0]
+                n = n - 1
+                continue
+        S = SUP
+        X = XUP
+        W = WUP
+        r = S.shape[0]
+        solver.dose_half(X, S, W, psi, dE, solver.csd.S[n - 1])
+        t += dE
+    if on_iter is not None:
+        on_iter(None)
+    if return_state:
+        return dict(X=X.copy(), S=S.copy(), W=W.copy(), psi=psi.copy(), dose=solver.dose.copy(), t=t,
+                    n_next=n_next if n_next is not None else n + 1, rank=rankInTime, eta=etaVec,
+                    bound=etaBoundVec, iters=iters)
+    U, Sig, V = la.svd_full(S)
+    rank_hist = np.array([timeVec, rankInTime], dtype=float)
+    eta_hist = np.array([etaVecTime, etaVec], dtype=float).T
+    bound_hist = np.array([etaVecTime, etaBoundVec], dtype=float).T
+    return (X @ U, 0.5 * math.sqrt(solver.gamma[0]) * Sig, solver.O @ (W @ V), W @ V, solver.dose,
+            rank_hist, eta_hist, bound_hist, psi)

@@ -210,3 +210,20 @@ def test_rank_beyond_capacity_fails_cleanly():
         g.run(_lib.TITUS_BUG_ADAPTIVE, max_steps=120)
     out = gsolver(23, 8, 3).run(_lib.TITUS_BUG_ADAPTIVE, max_steps=5)
     assert np.isfinite(out["dose"]).all()
+
+
+def test_truncation_completes_with_canonical_vectors():
+    """21x21 water beam, P7, cap 16, theta 1e-3: at n = 3 the augmented basis
+    [X X~] has a zero column (X's second column was a boundary cell, zeroed by
+    the K-step) and truncate! keeps all four directions of a rank-3 S_new. No
+    row of the basis completes the fourth left direction, so the canonical
+    vectors of R^4 must be tried, from the first one."""
+    nx, npn, r, steps = 21, 7, 16, 3
+    os_ = OSettings(nx, nx, r, "csdWaterBeam", nPN=npn)
+    os_.theta = 1e-3
+    gs = Settings(nx, nx, r, "csdWaterBeam", nPN=npn)
+    gs.theta = 1e-3
+    o = solve_dlr_parallel(OSolver(os_), max_steps=steps)
+    g = SolveFirstCollisionSourceDLRParallel(SolverCSD(gs), max_steps=steps)
+    np.testing.assert_array_equal(g[5][1], o[5][1])
+    assert dose_ok(g[4], o[4], nx)

@@ -2,6 +2,7 @@
 from .settings import Settings  # noqa: F401
 from .solver import (DoseAdjoint, PencilBeamBatch, SolveBatchedPencilBeams, SolverCSD, SolveFirstCollisionSource,  # noqa: F401
                      SolveFirstCollisionSourceDLR, SolveFirstCollisionSourceDLRHighOrder,
-                     SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel, scalar_flux)
+                     SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel,
+                     SolveFirstCollisionSourceDLRParallelRejection, scalar_flux)
 from .spots import partition, plan_dose, plan_objective  # noqa: F401
 from .output import write_dlm, write_dose_vtk, write_vtr  # noqa: F401

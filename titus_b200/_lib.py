@@ -19,6 +19,7 @@ TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
 TITUS_DLR_HIGH_ORDER = 3
 TITUS_PN_FULL = 4
+TITUS_PARALLEL_REJECTION = 5
 TITUS_PRECISION_FP64 = 0
 TITUS_PRECISION_MIXED = 1
 # exclusive device timers (titus_profile order); "other" is time outside every named phase

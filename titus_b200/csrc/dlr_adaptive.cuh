@@ -843,7 +843,12 @@ static __device__ __noinline__ void w_complete_side(WCtx& x, int nq1, int rho2, 
                 __syncthreads();
                 continue;
             }
-            if (threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+            if (threadIdx.x == 0 && atomicCAS(x.st.status, 0, ST_COMPLETION) == 0) {
+                x.st.diag[0] = 32;   // W side: candidate moments exhausted
+                x.st.diag[2] = need;
+                x.st.diag[3] = acc;
+                x.st.diag[7] = x.cur_n;
+            }
             __syncthreads();
             break;
         }
@@ -978,7 +983,12 @@ static __device__ __noinline__ bool augment(WCtx& x, bool with_q1, bool par_bloc
     SideInfo& sx = x.side[0];
     sx.need2 = k - sx.rho2;
     sx.cand0 = k - sx.rho1;
-    if (sx.cand0 + sx.need2 > x.P.nxcomp && threadIdx.x == 0) set_status(x.st.status, ST_COMPLETION);
+    if (sx.cand0 + sx.need2 > x.P.nxcomp && threadIdx.x == 0 && atomicCAS(x.st.status, 0, ST_COMPLETION) == 0) {
+        x.st.diag[0] = 31;   // X side: more completion vectors than candidate cells
+        x.st.diag[2] = sx.cand0 + sx.need2;
+        x.st.diag[3] = x.P.nxcomp;
+        x.st.diag[7] = x.cur_n;
+    }
     SideInfo& sw = x.side[1];
     sw.need2 = k - sw.rho2;
     sw.cand0 = 0;
@@ -1041,6 +1051,12 @@ static __device__ __noinline__ int w_truncate_svd(WCtx& x, int m) {
     kk = min(kk, m);
     const int rho = w_svd_complete(At, Vt, LDS, m, sm->sig, sm->perm, kk, kNullSvd, x.st.status, x.st.X, x.P.n,
                                    x.st.W, x.P.N, KA);
+    if (threadIdx.x == 0 && *(volatile int*)x.st.status == ST_COMPLETION && x.st.diag[0] == 0.0) {
+        x.st.diag[0] = 33;   // truncation: null directions of S not completed
+        x.st.diag[2] = m;
+        x.st.diag[3] = rho;
+        x.st.diag[7] = x.cur_n;
+    }
     // the completion read rows of X and W owned by other CTAs, which the
     // truncation then rewrites in place
     if (rho < kk && !wsync(x)) return -1;
@@ -1214,9 +1230,11 @@ static __device__ __noinline__ bool w_outscatter(WCtx& x, const double* sig) {
 
 // In-scattering K and L (:1905-1918): K = X S + dE psi MtDW (K[bnd] = 0),
 // L = W S^T + dE Dvec (MRed Xtpsi^T); Grams of [X K] and [W L]. With sbar:
-// Sbar = S + dE Xtpsi MtDW in scratch and the second dose half-step with
-// (X, Sbar, W) before truncation (parallel integrator, :1943).
-static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, bool sbar_dose, int dose_sidx) {
+// Sbar = S + dE Xtpsi MtDW in scratch; with dose also the second dose
+// half-step with (X, Sbar, W) before truncation (parallel integrator, :1943;
+// the parallel-rejection loop takes its dose after the truncation, :2683).
+static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, bool sbar, bool dose, int dose_sidx) {
+    const bool sbar_dose = sbar && dose;
     ProfScope ps_(x.prof, PF_ROWS_SCATTER);
     const int k = x.r;
     const DevProblem& P = x.P;
@@ -1231,7 +1249,7 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
     g_copy(Mt, KA, x.scr + SO_MTDW, KA, P.q, k);
     g_copy(Xp, QW, x.scr + SO_XTPSI, QW, k, P.q);
     double* Sb = x.scr + SO_SBAR;
-    if (sbar_dose) {
+    if (sbar) {
         // Sbar = S + dE Xtpsi MtDW
         for (int e = threadIdx.x; e < k * k; e += NT) {
             const int i = e / k, j = e - (e / k) * k;
@@ -1240,6 +1258,8 @@ static __device__ __noinline__ bool w_inscatter_KL(WCtx& x, const double* sig, b
             Sb[i * RA + j] = sm->S[i * KA + j] + dE * a;
         }
         __syncthreads();
+    }
+    if (sbar_dose) {
         // v = Sbar W[0,:]^T
         double* w0 = sm->vec + KA;
         for (int j = threadIdx.x; j < k; j += NT) w0[j] = ldcg(x.st.W + j);
@@ -1305,8 +1325,9 @@ __device__ inline void w_zero_bnd(WCtx& x) {
 }
 
 // Build the parallel integrator's augmented S (:1881-1885) in transposed
-// storage at work[0]: S_new = [[Sbar, L^T W~], [X~^T K, 0]].
-static __device__ __noinline__ void w_parallel_snew(WCtx& x) {
+// storage at work[0]: S_new = [[Sbar, L^T W~], [X~^T K, 0]]; `par` holds
+// [X~^T K | L^T W~] (k x k each) as augment() reduced them.
+static __device__ __noinline__ void w_parallel_snew(WCtx& x, const double* par) {
     const int k = x.r, m = 2 * k;
     double* At = x.sm->work;
     const double* Sb = x.scr + SO_SBAR;
@@ -1314,12 +1335,250 @@ static __device__ __noinline__ void w_parallel_snew(WCtx& x) {
         const int i = e / m, j = e - (e / m) * m;   // S_new[i][j] -> At[j][i]
         double v;
         if (i < k && j < k) v = Sb[i * RA + j];
-        else if (i < k) v = ldcg(x.redp + k * k + i * k + (j - k));        // (L^T W~)[i][j-k]
-        else if (j < k) v = ldcg(x.redp + (i - k) * k + j);                // (X~^T K)[i-k][j]
+        else if (i < k) v = ldcg(par + k * k + i * k + (j - k));        // (L^T W~)[i][j-k]
+        else if (j < k) v = ldcg(par + (i - k) * k + j);                // (X~^T K)[i-k][j]
         else v = 0.0;
         At[j * LDS + i] = v;
     }
     __syncthreads();
+}
+
+// ------------------------------------------------ parallel-rejection loop ---
+// SolveFirstCollisionSourceDLRParallelRejection (SolverCSD.jl:2376-2742): the
+// parallel integrator's augmented step inside the BUG loop's rejections.
+
+// S0 = S entering the energy, kept by every CTA (at n = 2 the out-scattering
+// rewrites the aliased S0 in place, :2518, :2611, so it is taken again there).
+__device__ inline void w_prej_save_s(WCtx& x) {
+    const int k = x.r;
+    double* S0 = x.scr + SO_S0;
+    for (int e = threadIdx.x; e < k * k; e += NT) S0[(e / k) * RA + e % k] = x.sm->S[(e / k) * KA + e % k];
+    __syncthreads();
+}
+// X0 = X entering the energy with its boundary rows zeroed (the streaming
+// K-step, or at n = 2 the in-scattering K-step, zeroes the aliased X0 in
+// place, :2532, :2618) and W0 = W, own rows; then S0.
+static __device__ __noinline__ void w_prej_save(WCtx& x) {
+    const int k = x.r;
+    for (int e = threadIdx.x; e < (x.c1 - x.c0) * k; e += NT) {
+        const int c = x.c0 + e / k, j = e - (e / k) * k;
+        x.st.X0[(size_t)c * RA + j] = is_bnd_w(x.P, c) ? 0.0 : ldcg(x.st.X + (size_t)c * KA + j);
+    }
+    for (int e = threadIdx.x; e < (x.m1 - x.m0) * k; e += NT) {
+        const int mo = x.m0 + e / k, j = e - (e / k) * k;
+        x.st.W0[(size_t)mo * RA + j] = ldcg(x.st.W + (size_t)mo * KA + j);
+    }
+    w_prej_save_s(x);
+}
+
+// Streaming rejection test (:2567-2586). With X (boundary rows zeroed) in
+// X[:, :k], X~ in X[:, k:2k], W in W[:, :k] and W~ in W[:, k:2k], one pass over
+// the team's rows reduces [X~^T L_d X (4 k^2) | W^T A_d W~ (4 k^2) |
+// [X X~]^T X (2k x k) | W^T [W W~] (k x 2k)]. Returns
+// eta^2 = ||sum_d (X~^T L_d X) S (W^T A_d W~)||_F^2 with the entering S (the
+// same value in every CTA), or -1 if the team aborted.
+static __device__ __noinline__ double w_prej_stream_eta(WCtx& x) {
+    const int k = x.r, m = 2 * k, kk = k * k;
+    WSmem* sm = x.sm;
+    {
+        ProfScope ps_(x.prof, PF_ROWS_STREAM);
+        double* acc = sm->work;   // 6 k^2 per side
+        double* F = sm->work + 6 * kk;
+        const int ldf = m + 4 * k;
+        const int tr = rows_fit(WORKD - 6 * kk, ldf);
+        GBlock bl[5];
+        w_acc_zero(acc, 6 * kk);
+        for (int d = 0; d < 4; ++d) bl[d] = GBlock{k, k, m + d * k, k, d * kk};   // X~^T (L_d X)
+        bl[4] = GBlock{0, m, 0, k, 4 * kk};                                        // [X X~]^T X
+        for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+            const int nr = min(tr, x.c1 - r0);
+            wload(F, ldf, 0, x.st.X, KA, 0, r0, nr, m);
+            w_stencil(x, x.st.X, KA, r0, nr, k, F, ldf, m);
+            __syncthreads();
+            gram_blocks(acc, F, ldf, nr, bl, 5);
+            __syncthreads();
+        }
+        wpublish_chunk(x, acc, 0, 4 * kk);
+        wpublish_chunk(x, acc + 4 * kk, 8 * kk, 2 * kk);
+        __syncthreads();
+        w_acc_zero(acc, 6 * kk);
+        for (int d = 0; d < 4; ++d) bl[d] = GBlock{0, k, m + d * k, k, d * kk};   // W^T (A_d W~)
+        bl[4] = GBlock{0, k, 0, m, 4 * kk};                                        // W^T [W W~]
+        for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+            const int nr = min(tr, x.m1 - r0);
+            wload(F, ldf, 0, x.st.W, KA, 0, r0, nr, m);
+            w_spmm(x, x.st.W + k, KA, r0, nr, k, F, ldf, m);
+            __syncthreads();
+            gram_blocks(acc, F, ldf, nr, bl, 5);
+            __syncthreads();
+        }
+        wpublish_chunk(x, acc, 4 * kk, 4 * kk);
+        wpublish_chunk(x, acc + 4 * kk, 10 * kk, 2 * kk);
+    }
+    if (!wreduce(x, 12 * kk)) return -1.0;
+    ProfScope ps_(x.prof, PF_SMALL);
+    double* Gt = sm->work;
+    double* Ct = sm->work + 4 * kk;
+    double* T = sm->work + 8 * kk;
+    double* U = sm->work + 9 * kk;
+    double* E = sm->work + 10 * kk;
+    load_red(x, 0, 4 * k, k, Gt, k);
+    load_red(x, 4 * kk, 4 * k, k, Ct, k);
+    g_zero(E, k, k, k);
+    for (int d = 0; d < 4; ++d) {
+        g_mm(T, k, Gt + d * kk, k, false, sm->S, KA, false, k, k, k);   // Gt_d S
+        g_mm(U, k, T, k, false, Ct + d * kk, k, false, k, k, k);        // (Gt_d S) Ct_d
+        for (int e = threadIdx.x; e < kk; e += NT) E[e] += U[e];
+        __syncthreads();
+    }
+    double e2 = 0.0;
+    for (int e = threadIdx.x; e < kk; e += NT) e2 = fma(E[e], E[e], e2);
+    return cta_sum(e2);
+}
+
+// Streaming rejection (:2588-2592): S = ([X X~]^T X) S (W^T [W W~]) from the
+// blocks w_prej_stream_eta reduced (still in x.redp); X and W already hold
+// [X X~] and [W W~].
+static __device__ __noinline__ void w_prej_expand_stream(WCtx& x) {
+    ProfScope ps_(x.prof, PF_SMALL);
+    const int k = x.r, m = 2 * k, kk = k * k;
+    WSmem* sm = x.sm;
+    double* Mu = sm->work;      // m x k
+    double* Nu = Mu + m * k;    // k x m
+    double* T = Nu + m * k;     // m x k: Mu S
+    double* U = T + m * k;      // m x m
+    load_red(x, 8 * kk, m, k, Mu, k);
+    load_red(x, 10 * kk, k, m, Nu, m);
+    g_mm(T, k, Mu, k, false, sm->S, KA, false, m, k, k);
+    g_mm(U, m, T, k, false, Nu, m, false, m, k, m);
+    for (int e = threadIdx.x; e < KA * KA; e += NT) {
+        const int i = e / KA, j = e - (e / KA) * KA;
+        sm->S[e] = (i < m && j < m) ? U[i * m + j] : 0.0;
+    }
+    __syncthreads();
+}
+
+// Scattering rejection test (:2652-2660): reduces X~^T psi (k x q),
+// (MRed^T diag(Dvec) W~)^T (q x k) and row 0 of [W W~] (2k entries, written to
+// w0 for the dose after the truncation). Returns eta^2 = ||X~^T psi MRed^T D W~||_F^2,
+// or -1 if the team aborted.
+static __device__ __noinline__ double w_prej_scatter_eta(WCtx& x, const double* sig, double* w0) {
+    const int k = x.r, m = 2 * k;
+    const DevProblem& P = x.P;
+    WSmem* sm = x.sm;
+    const int q = P.q;
+    {
+        ProfScope ps_(x.prof, PF_ROWS_SCATTER);
+        double* acc = sm->work;   // 2 k q + m
+        const int ldt = k + q + ((k + q) & 1);
+        const int tstart = 2 * KA * QW + KA;
+        const int tr = rows_fit(WORKD - tstart, ldt);
+        double* tt = sm->work + tstart;
+        w_acc_zero(acc, 2 * k * q + m);
+        const GBlock bx{0, k, k, q, 0};
+        for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+            const int nr = min(tr, x.c1 - r0);
+            wload(tt, ldt, 0, x.st.X, KA, k, r0, nr, k);
+            wload(tt, ldt, k, x.psi_in, QW, 0, r0, nr, q);
+            __syncthreads();
+            gram_blocks(acc, tt, ldt, nr, &bx, 1);
+            __syncthreads();
+        }
+        const GBlock bw{k, q, 0, k, k * q};
+        for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+            const int nr = min(tr, x.m1 - r0);
+            wload(tt, ldt, 0, x.st.W, KA, k, r0, nr, k);
+            for (int e = threadIdx.x; e < nr * q; e += NT) {
+                const int r = e / q, kq = e - (e / q) * q;
+                const int mo = r0 + r;
+                tt[r * ldt + k + kq] = P.mred[(size_t)mo * q + kq] * sig[P.lof[mo]];
+            }
+            __syncthreads();
+            gram_blocks(acc, tt, ldt, nr, &bw, 1);
+            __syncthreads();
+        }
+        // row 0 of [W W~] travels through the reduction (only its owner adds it)
+        if (x.m0 == 0 && x.m1 > 0)
+            for (int j = threadIdx.x; j < m; j += NT) acc[2 * k * q + j] = ldcg(x.st.W + j);
+        __syncthreads();
+        wpublish_chunk(x, acc, 0, 2 * k * q + m);
+    }
+    if (!wreduce(x, 2 * k * q + m)) return -1.0;
+    ProfScope ps_(x.prof, PF_SMALL);
+    double* Xp = sm->work;         // k x q
+    double* Mt = Xp + k * q;       // q x k
+    load_red(x, 0, k, q, Xp, q);
+    load_red(x, k * q, q, k, Mt, k);
+    load_red(x, 2 * k * q, 1, m, w0, m);
+    double e2 = 0.0;
+    for (int e = threadIdx.x; e < k * k; e += NT) {
+        const int i = e / k, j = e - (e / k) * k;
+        double a = 0.0;
+        for (int l = 0; l < q; ++l) a = fma(Xp[i * q + l], Mt[l * k + j], a);
+        e2 = fma(a, a, e2);
+    }
+    return cta_sum(e2);
+}
+
+// Scattering rejection with an unchanged rank (:2662-2665): S = ([X0 X~]^T X0)
+// S0 (W0^T [W0 W~]), X = [X0 X~], W = [W0 W~]. X~ and W~ sit in columns
+// [k, 2k) of X and W already, so only the first k columns are replaced (own
+// rows), followed by a team barrier (the next step's stencils read them).
+static __device__ __noinline__ bool w_prej_expand_scatter(WCtx& x) {
+    const int k = x.r, m = 2 * k;
+    WSmem* sm = x.sm;
+    {
+        ProfScope ps_(x.prof, PF_ROWS_SCATTER);
+        double* acc = sm->work;   // 2 m k
+        double* t = sm->work + 2 * m * k;
+        const int tr = rows_fit(WORKD - 2 * m * k, m);
+        w_acc_zero(acc, 2 * m * k);
+        const GBlock bx{0, m, 0, k, 0};   // [X0 X~]^T X0
+        for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
+            const int nr = min(tr, x.c1 - r0);
+            wload(t, m, 0, x.st.X0, RA, 0, r0, nr, k);
+            wload(t, m, k, x.st.X, KA, k, r0, nr, k);
+            __syncthreads();
+            gram_blocks(acc, t, m, nr, &bx, 1);
+            __syncthreads();
+        }
+        const GBlock bw{0, k, 0, m, m * k};   // W0^T [W0 W~]
+        for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
+            const int nr = min(tr, x.m1 - r0);
+            wload(t, m, 0, x.st.W0, RA, 0, r0, nr, k);
+            wload(t, m, k, x.st.W, KA, k, r0, nr, k);
+            __syncthreads();
+            gram_blocks(acc, t, m, nr, &bw, 1);
+            __syncthreads();
+        }
+        wpublish_chunk(x, acc, 0, 2 * m * k);
+    }
+    if (!wreduce(x, 2 * m * k)) return false;
+    {
+        ProfScope ps_(x.prof, PF_SMALL);
+        double* Mu = sm->work;      // m x k
+        double* Nu = Mu + m * k;    // k x m
+        double* T = Nu + m * k;     // m x k: Mu S0
+        double* U = T + m * k;      // m x m
+        load_red(x, 0, m, k, Mu, k);
+        load_red(x, m * k, k, m, Nu, m);
+        g_mm(T, k, Mu, k, false, x.scr + SO_S0, RA, false, m, k, k);
+        g_mm(U, m, T, k, false, Nu, m, false, m, k, m);
+        for (int e = threadIdx.x; e < KA * KA; e += NT) {
+            const int i = e / KA, j = e - (e / KA) * KA;
+            sm->S[e] = (i < m && j < m) ? U[i * m + j] : 0.0;
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < (x.c1 - x.c0) * k; e += NT) {
+        const int c = x.c0 + e / k, j = e - (e / k) * k;
+        x.st.X[(size_t)c * KA + j] = x.st.X0[(size_t)c * RA + j];
+    }
+    for (int e = threadIdx.x; e < (x.m1 - x.m0) * k; e += NT) {
+        const int mo = x.m0 + e / k, j = e - (e / k) * k;
+        x.st.W[(size_t)mo * KA + j] = x.st.W0[(size_t)mo * RA + j];
+    }
+    return wsync(x);
 }
 
 // ---------------------------------------------------------------- kernel ---
@@ -1335,7 +1594,8 @@ struct LoopState {
 };
 
 // The energy loop of one solve on this team (METHOD 1: n = n_begin..n_end;
-// METHOD 2: the BUG while-loop with rejections), from the state in x / ls.
+// METHOD 2: the BUG while-loop with rejections; METHOD 5: the
+// parallel-rejection while-loop), from the state in x / ls.
 template <int METHOD>
 static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end, int max_iters, LoopState& ls) {
     WSmem* sm = x.sm;
@@ -1355,7 +1615,8 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
         if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
             if (n > n_end) break;
         } else {
-            if (!(t < nE * dE)) break;
+            // BUG: while t < nEnergies dE (:2102); parallel rejection: (nEnergies-1) dE (:2467)
+            if (!(t < (METHOD == TITUS_BUG_ADAPTIVE ? nE : nE - 1) * dE)) break;
             if (n == nE || n > n_end) break;
         }
         if (iters >= max_iters) break;
@@ -1363,13 +1624,15 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
         x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
         x.psi_out = psi_idx ? x.st.psi0 : x.st.psi1;
         const double* sig = P.sigma + (size_t)(n - 1) * (P.npn + 1);
-        if (METHOD == TITUS_BUG_ADAPTIVE && x.b == 0 && threadIdx.x == 0 && iters < x.st.hist_cap) {
+        if (METHOD != TITUS_PARALLEL_ADAPTIVE && x.b == 0 && threadIdx.x == 0 && iters < x.st.hist_cap) {
             x.st.rank_hist[iters] = x.r;
             x.st.time_hist[iters] = (double)n;   // energy index (eGrid[n-1] on the host)
         }
         ++iters;
         rank_sum += x.r;
         // ---- A, B
+        const int k0 = x.r;   // rank entering the energy (parallel rejection: X0, W0, S0)
+        if (METHOD == TITUS_PARALLEL_REJECTION) w_prej_save(x);
         w_phase_A(x, n);
         if (!wsync(x)) { aborted = true; break; }
         w_sweep(x, sig[0]);
@@ -1384,11 +1647,55 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
         x.psi_in = psi_idx ? x.st.psi1 : x.st.psi0;
         if (stream) {
             const int k = x.r;
-            w_stream_small(x, METHOD == TITUS_PARALLEL_ADAPTIVE);
+            w_stream_small(x, METHOD != TITUS_BUG_ADAPTIVE);
             if (!w_phase_C(x)) { aborted = true; break; }
-            if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
+            if (METHOD == TITUS_PARALLEL_REJECTION) {
+                // [X X~], [W W~] (:2535, :2544); S_new from Sbar (:2549-2555); truncate! (:2558)
                 if (!augment(x, false, true)) { aborted = true; break; }
-                w_parallel_snew(x);
+                double* par = x.scr + SO_TMP;
+                for (int e = threadIdx.x; e < 2 * k * k; e += NT) par[e] = ldcg(x.redp + e);
+                __syncthreads();
+                const double eta2 = w_prej_stream_eta(x);
+                if (eta2 < 0.0) { aborted = true; break; }
+                w_parallel_snew(x, par);
+                const int kk = w_truncate_svd(x, 2 * k);
+                if (kk < 0) { aborted = true; break; }
+                bool repeat = false;
+                if (kk == 2 * k && 2 * k < P.r) {
+                    repeat = true;   // keep the truncation, redo this energy (n = n-1 without continue, :2561-2566)
+                } else {
+                    double s2 = 0.0;
+                    for (int j = 0; j < kk; ++j) s2 += sm->sig[j] * sm->sig[j];
+                    const double eta = sqrt(eta2);
+                    const double bound = P.c_eta * P.theta * fmax(1e-7, pow(sqrt(s2), P.theta_index)) / dE;
+                    if (x.b == 0 && threadIdx.x == 0 && eta_count < x.st.hist_cap) {
+                        x.st.eta_hist[eta_count] = eta;
+                        x.st.bound_hist[eta_count] = bound;
+                    }
+                    ++eta_count;
+                    if (eta > bound && 2 * k < P.r) {
+                        // reject: S = ([X X~]^T X) S (W^T [W W~]), rank 2k, repeat energy n (:2586-2593)
+                        w_prej_expand_stream(x);
+                        x.r = 2 * k;
+                        n -= 1;
+                        if (x.r > RA) {
+                            if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                            aborted = true;
+                            break;
+                        }
+                        continue;
+                    }
+                }
+                w_truncate_apply(x, 2 * k, kk, -1, nullptr);
+                if (repeat) n -= 1;
+                if (x.r > RA) {
+                    if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                    aborted = true;
+                    break;
+                }
+            } else if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
+                if (!augment(x, false, true)) { aborted = true; break; }
+                w_parallel_snew(x, x.redp);
                 const int kk = w_truncate_svd(x, 2 * k);
                 if (kk < 0) { aborted = true; break; }
                 w_truncate_apply(x, 2 * k, kk, -1, nullptr);
@@ -1507,14 +1814,18 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
         }
         // ---- out-scattering
         if (!w_outscatter(x, sig)) { aborted = true; break; }
+        if (METHOD == TITUS_PARALLEL_REJECTION && !stream) w_prej_save_s(x);   // S0 aliases S at n = 2
         // ---- in-scattering
         w_zero_bnd(x);
         {
             const int k = x.r;
-            if (!w_inscatter_KL(x, sig, METHOD == TITUS_PARALLEL_ADAPTIVE, n - 1)) { aborted = true; break; }
+            if (!w_inscatter_KL(x, sig, METHOD != TITUS_BUG_ADAPTIVE, METHOD == TITUS_PARALLEL_ADAPTIVE, n - 1)) {
+                aborted = true;
+                break;
+            }
             if (METHOD == TITUS_PARALLEL_ADAPTIVE) {
                 if (!augment(x, false, true)) { aborted = true; break; }
-                w_parallel_snew(x);
+                w_parallel_snew(x, x.redp);
                 const int kk = w_truncate_svd(x, 2 * k);
                 if (kk < 0) { aborted = true; break; }
                 w_truncate_apply(x, 2 * k, kk, -1, nullptr);
@@ -1528,6 +1839,58 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                         x.st.rank_hist[n - 1] = x.r;
                         x.st.time_hist[n - 1] = t;
                     }
+                }
+                t += dE;
+            } else if (METHOD == TITUS_PARALLEL_REJECTION) {
+                // [X X~], [W W~] (:2627, :2632); S_new (:2634-2639); truncate! (:2642)
+                if (!augment(x, false, true)) { aborted = true; break; }
+                double* par = x.scr + SO_TMP;
+                double* w0 = x.scr + SO_TMP + 2 * KA * KA;   // row 0 of [W W~] for the dose
+                for (int e = threadIdx.x; e < 2 * k * k; e += NT) par[e] = ldcg(x.redp + e);
+                __syncthreads();
+                const double eta2 = w_prej_scatter_eta(x, sig, w0);
+                if (eta2 < 0.0) { aborted = true; break; }
+                w_parallel_snew(x, par);
+                const int kk = w_truncate_svd(x, 2 * k);
+                if (kk < 0) { aborted = true; break; }
+                bool repeat = false;
+                if (kk == 2 * k && 2 * k < P.r) {
+                    repeat = true;   // :2645-2650, no continue
+                } else {
+                    double s2 = 0.0;
+                    for (int j = 0; j < kk; ++j) s2 += sm->sig[j] * sm->sig[j];
+                    const double eta = sqrt(eta2);
+                    const double bound = P.c_eta * P.theta * fmax(1e-7, pow(sqrt(s2), P.theta_index)) / dE;
+                    if (eta > bound && 2 * k < P.r) {
+                        if (k0 != k) {
+                            // [X0 X~] has k0 + k columns but the reference sets r = 2k; its
+                            // repeated step's SNew[1:r,1:r] .= SBar (:2553) raises DimensionMismatch
+                            if (threadIdx.x == 0 && atomicCAS(x.st.status, 0, ST_REF_SHAPE) == 0) {
+                                x.st.diag[0] = k0;
+                                x.st.diag[2] = k;
+                                x.st.diag[7] = n;
+                            }
+                            aborted = true;
+                            break;
+                        }
+                        if (!w_prej_expand_scatter(x)) { aborted = true; break; }
+                        x.r = 2 * k;
+                        n -= 1;
+                        if (x.r > RA) {
+                            if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                            aborted = true;
+                            break;
+                        }
+                        continue;
+                    }
+                }
+                // the dose takes S[n] of the decremented n after a first-branch rejection (:2683)
+                w_truncate_apply(x, 2 * k, kk, repeat ? n - 2 : n - 1, w0);
+                if (repeat) n -= 1;
+                if (x.r > RA) {
+                    if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);
+                    aborted = true;
+                    break;
                 }
                 t += dE;
             } else {
@@ -1622,7 +1985,8 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                         continue;
                     }
                 }
-                w_truncate_apply(x, m, kk, n - 1, x.scr + SO_TMP);
+                // the dose takes S[n] of the decremented n after a first-branch rejection (:2315)
+                w_truncate_apply(x, m, kk, repeat ? n - 2 : n - 1, x.scr + SO_TMP);
                 if (repeat) n -= 1;
                 if (x.r > RA) {
                     if (threadIdx.x == 0) set_status(x.st.status, ST_LIMIT);

@@ -1,5 +1,6 @@
 // Host side of the rank-adaptive integrators (TITUS_PARALLEL_ADAPTIVE,
-// TITUS_BUG_ADAPTIVE): device state, initial factors, launch and result copy.
+// TITUS_BUG_ADAPTIVE, TITUS_PARALLEL_REJECTION): device state, initial factors,
+// launch and result copy.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,13 +36,16 @@ int ensure_state(titus_solver* s) {
         (rc = s->walloc(&w.status, 1)) || (rc = s->walloc(&w.info, 8)) || (rc = s->walloc(&w.diag, 16)) ||
         (rc = s->walloc(&w.tvar, 1)) || (rc = s->walloc(&w.rank_hist, (size_t)w.hist_cap)) ||
         (rc = s->walloc(&w.time_hist, (size_t)w.hist_cap)) || (rc = s->walloc(&w.eta_hist, (size_t)w.hist_cap)) ||
-        (rc = s->walloc(&w.bound_hist, (size_t)w.hist_cap)))
+        (rc = s->walloc(&w.bound_hist, (size_t)w.hist_cap)) || (rc = s->walloc(&w.X0, (size_t)n * RA)) ||
+        (rc = s->walloc(&w.W0, (size_t)N * RA)))
         return rc;
     if ((rc = s->walloc(&s->d_wst, 1))) return rc;
     CK(cudaMemcpy(s->d_wst, &w, sizeof(WideState), cudaMemcpyHostToDevice));
     CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sizeof(WSmem)));
     CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_BUG_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(WSmem)));
+    CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_REJECTION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sizeof(WSmem)));
     return TITUS_OK;
 }
@@ -102,12 +106,12 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : std::min(s->num_sms, 64);
     G = std::max(1, std::min(G, s->num_sms));
     int per_sm = 0;
-    auto kern = method == TITUS_PARALLEL_ADAPTIVE ? (void*)adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>
-                                                  : (void*)adaptive_kernel<TITUS_BUG_ADAPTIVE>;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm,
-        method == TITUS_PARALLEL_ADAPTIVE ? adaptive_kernel<TITUS_PARALLEL_ADAPTIVE> : adaptive_kernel<TITUS_BUG_ADAPTIVE>,
-        wide::NT, sizeof(WSmem)));
+    void (*kfun)(DevProblem, WideState*, int, int, int, int) =
+        method == TITUS_PARALLEL_ADAPTIVE    ? adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>
+        : method == TITUS_PARALLEL_REJECTION ? adaptive_kernel<TITUS_PARALLEL_REJECTION>
+                                             : adaptive_kernel<TITUS_BUG_ADAPTIVE>;
+    auto kern = (void*)kfun;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, wide::NT, sizeof(WSmem)));
     if (per_sm < 1) return fail(TITUS_ERR_CUDA, "adaptive kernel does not fit on an SM (smem %zu)", sizeof(WSmem));
     G = std::min(G, per_sm * s->num_sms);
     DevProblem P = s->P;
@@ -148,7 +152,10 @@ int check_status(titus_solver* s) {
                        : status == ST_LIMIT          ? "rank exceeds the adaptive kernel's capacity"
                        : status == ST_UNSUPPORTED    ? "angular basis not orthonormal (cannot complete)"
                        : status == ST_SVD            ? "Jacobi SVD did not converge"
-                                                     : "device error";
+                       : status == ST_REF_SHAPE
+                           ? "scattering rejection after the streaming step changed the rank: the reference's next "
+                             "step raises DimensionMismatch (SolverCSD.jl:2553)"
+                           : "device error";
     const int code = status == ST_LIMIT ? TITUS_ERR_LIMIT : TITUS_ERR_DEVICE;
     if (status == ST_BARRIER_TIMEOUT) {
         unsigned counter = 0;
@@ -156,7 +163,7 @@ int check_status(titus_solver* s) {
         return fail(code, "device status %d: %s (CTA %g at barrier %g saw %g arrivals, wanted %g; counter now %u)",
                     status, what, d[8], d[14], d[9], d[10], counter);
     }
-    if (status == ST_SVD) {
+    if (status == ST_SVD || (status == ST_COMPLETION && d[0] == 33)) {
         // statistics of the matrix handed to the SVD (CTA 0's copy)
         std::vector<double> a((size_t)KA * KA);
         CK(cudaMemcpy(a.data(), s->wst.scr + SO_DBG, a.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -178,6 +185,9 @@ int check_status(titus_solver* s) {
         return fail(code, "device status %d: %s (m %d at step %g; input: %d non-finite, %d zeros, |a| in [%.3e, %.3e]; "
                     "column 0: %s)", status, what, m, d[7], nonfinite, zeros, amin, amax, row.c_str());
     }
+    if (status == ST_REF_SHAPE)
+        return fail(code, "device status %d: %s (rank %g entering energy index %g, %g after streaming)", status, what,
+                    d[0], d[7], d[2]);
     return fail(code, "device status %d: %s (rank cap %d, adaptive width %d; diag %g %g %g step %g)", status, what,
                 RA, KA, d[0], d[2], d[3], d[7]);
 }

@@ -235,6 +235,9 @@ static int create_impl(const titus_problem_t* pb, titus_solver* s) {
 
 static_assert(TITUS_DLR_HIGH_ORDER == titus::kHighOrder, "method id of the RK4 kernel");
 static bool is_fixed_family(int method) { return method == TITUS_DLR_FIXED || method == TITUS_DLR_HIGH_ORDER; }
+static bool is_wide_family(int method) {
+    return method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE || method == TITUS_PARALLEL_REJECTION;
+}
 
 // The RK4 integrator's stage buffers (3 x n x KM and 3 x N x KM), allocated on
 // its first use.
@@ -386,7 +389,7 @@ extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
     if (int rc = check_precision(method, opt)) return rc;
     cudaStream_t stream = (cudaStream_t)stream_;
-    if (method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE) {
+    if (is_wide_family(method)) {
         s->last_method = method;
         return titus_host::wide_solve_device(s, method, opt, stream);
     }
@@ -398,7 +401,7 @@ extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus
 
 extern "C" int titus_fetch(titus_solver_t* s, titus_result_t* res) {
     if (!s || !res) return fail(TITUS_ERR_ARG, "NULL argument");
-    if (s->last_method == TITUS_PARALLEL_ADAPTIVE || s->last_method == TITUS_BUG_ADAPTIVE)
+    if (is_wide_family(s->last_method))
         return titus_host::wide_fetch(s, res);
     int rc = check_status(s);
     if (rc) return rc;
@@ -480,7 +483,7 @@ extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_o
                                 titus_result_t* res) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
     if (int rc = check_precision(method, opt)) return rc;
-    if (method == TITUS_PARALLEL_ADAPTIVE || method == TITUS_BUG_ADAPTIVE) {
+    if (is_wide_family(method)) {
         s->last_method = method;
         int rc = titus_host::wide_solve_from(s, method, opt, n_stop);
         if (rc) return rc;
@@ -566,8 +569,7 @@ extern "C" int titus_profile(titus_solver_t* s, double* ns, int32_t n) {
 extern "C" int titus_resume_point(titus_solver_t* s, int32_t* n_next, double* t) {
     if (!s || !n_next) return fail(TITUS_ERR_ARG, "NULL argument");
     CK(cudaDeviceSynchronize());
-    if (s->last_method == TITUS_PARALLEL_ADAPTIVE || s->last_method == TITUS_BUG_ADAPTIVE ||
-        (s->last_method < 0 && s->wide_state_valid)) {
+    if (is_wide_family(s->last_method) || (s->last_method < 0 && s->wide_state_valid)) {
         if (!s->d_wst) return fail(TITUS_ERR_ARG, "no solver state yet");
         int info[8];
         CK(cudaMemcpy(info, s->wst.info, sizeof(info), cudaMemcpyDeviceToHost));

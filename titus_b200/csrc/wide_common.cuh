@@ -34,6 +34,7 @@ constexpr int WCS = 3 * RA;     // row stride of the W-side completion coefficie
 constexpr int ST_LIMIT = 5;        // rank would exceed RA
 constexpr int ST_UNSUPPORTED = 6;  // angular basis lost orthonormality (cannot complete)
 constexpr int ST_SVD = 7;          // Jacobi SVD did not converge
+constexpr int ST_REF_SHAPE = 8;    // the reference's next step raises DimensionMismatch (parallel-rejection loop)
 
 struct WideState {
     double* X;      // n x KA
@@ -60,6 +61,8 @@ struct WideState {
     double* time_hist;
     double* eta_hist;
     double* bound_hist;
+    double* X0;     // n x RA: X entering the energy, boundary rows zeroed (parallel-rejection loop)
+    double* W0;     // N x RA: W entering the energy (parallel-rejection loop)
     int hist_cap;
 };
 
@@ -86,7 +89,8 @@ constexpr int SO_XTPSI = SO_SIDE + 2 * SIDE_STRIDE;  // KA x QW   X^T psi
 constexpr int SO_MTDW = SO_XTPSI + KA * QW;          // QW x KA   MRed^T diag(Dvec) W
 constexpr int SO_TMP = SO_MTDW + QW * KA;            // 3 x KA x KA general temporaries
 constexpr int SO_DBG = SO_TMP + 3 * KA * KA;           // KA x KA: input of the last truncation SVD
-constexpr int SO_END = SO_DBG + KA * KA;
+constexpr int SO_S0 = SO_DBG + KA * KA;                 // RA x RA: S entering the energy (parallel-rejection loop)
+constexpr int SO_END = SO_S0 + RA * RA;
 static_assert(SO_END <= SCRW, "per-CTA scratch too small");
 
 struct WSmem {

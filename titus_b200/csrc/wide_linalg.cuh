@@ -428,7 +428,8 @@ static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld
                             found = cand + f;
                             cand = found + 1;
                         } else {
-                            cand += NT / 32;
+                            // stop at nrows: the canonical vectors come next, from the first
+                            cand = min(cand + NT / 32, nrows);
                         }
                     }
                     if (found < 0) continue;   // rows exhausted: canonical vectors next

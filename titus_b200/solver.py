@@ -474,7 +474,24 @@ def SolveFirstCollisionSourceDLRBUGRejection(solver: SolverCSD, recordGif: bool 
     (repeated energies included) and one (energy, eta) / (energy, bound) row per
     streaming rejection test. The device records at most nEnergies iterations.
     """
-    out = solver.run(_lib.TITUS_BUG_ADAPTIVE, max_steps=max_steps)
+    return _rejection_outputs(solver, _lib.TITUS_BUG_ADAPTIVE, max_steps)
+
+
+def SolveFirstCollisionSourceDLRParallelRejection(solver: SolverCSD, recordGif: bool = False, max_steps: int = 0):
+    """Parallel integrator with step rejection (``SolverCSD.jl:2376-2742``).
+
+    The parallel integrator's augmented step (``S_new = [[Sbar, L^T W~],
+    [X~^T K, 0]]``, then ``truncate!``) inside the BUG loop's rejection tests.
+    Same return tuple as :func:`SolveFirstCollisionSourceDLRBUGRejection`.
+    Where the reference's next step raises a DimensionMismatch (a scattering
+    rejection after a streaming step that changed the rank) the solve raises
+    ``TitusError`` (``TITUS_ERR_DEVICE``).
+    """
+    return _rejection_outputs(solver, _lib.TITUS_PARALLEL_REJECTION, max_steps)
+
+
+def _rejection_outputs(solver: SolverCSD, method: int, max_steps: int):
+    out = solver.run(method, max_steps=max_steps)
     res = solver.outputs(out)
     solver.dose = res[4]
     it = min(out["steps"], solver.nE)
