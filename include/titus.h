@@ -120,13 +120,17 @@ typedef struct titus_result {
     int32_t rank;          /* out: rank of the returned factors */
     int32_t steps_done;    /* out: loop iterations executed */
     int32_t* rank_history; /* optional (nE): fixed / parallel: rank after the step with energy
-                              index n at [n-1]; BUG: rank at the start of each loop iteration
-                              (repeated energies included, first nE iterations); -1 if unused */
-    double* eta_history;   /* optional (nE): BUG streaming eta of each rejection test, in order */
+                              index n at [n-1]; BUG and parallel rejection: rank at the start of
+                              each loop iteration (repeated energies included, first nE
+                              iterations); -1 if unused */
+    double* eta_history;   /* optional (nE): BUG / parallel rejection: streaming eta of each
+                              rejection test, in order */
     double* bound_history; /* optional (nE): the matching bound
-                              c_eta * theta * max(1e-7, ||S||^theta_index) / dE (SolverCSD.jl:2224) */
+                              c_eta * theta * max(1e-7, ||S||^theta_index) / dE with the S of the
+                              streaming S-step (BUG, SolverCSD.jl:2224) or the truncated S
+                              (parallel rejection, :2583) */
     double* time_history;  /* optional (nE): parallel: pseudo-time t at [n-1];
-                              BUG: energy index n (1-based) of each iteration */
+                              BUG and parallel rejection: energy index n (1-based) of each iteration */
 } titus_result_t;
 
 typedef struct titus_solver titus_solver_t;
