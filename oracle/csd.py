@@ -38,6 +38,8 @@ def analytic_stopping_power(kind: str, E):
         return 0.2 / E * np.log1p(10.0 * E)
     if kind == "proton_bethe":  # S(E) = (a/E) ln(b E), a = 250, b = 0.07
         return 250.0 / E * np.log(0.07 * E)
+    if kind == "proton_log1p":  # S(E) = (a/E) ln(1 + b E): the form above kept positive below 1/b
+        return 250.0 / E * np.log1p(0.07 * E)
     raise ValueError(f"unknown stopping power model {kind!r}")
 
 

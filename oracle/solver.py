@@ -44,6 +44,7 @@ class SolverCSD:
         self.N = pnmod.n_moments(s.nPN)
         self.density = s.density.astype(np.float64)
         nx, ny = s.NCellsX, s.NCellsY
+        self.n_cells = nx * ny
         self.densityVec = self.density.reshape(nx * ny)
         self.dose = np.zeros(nx * ny)
         # boundary cells, SolverCSD.jl:108-131 (0-based rows, order kept)
@@ -194,8 +195,7 @@ class SolverCSD:
 
     def dose_half(self, X, S, W, psi, dE, Sn):
         """``dose += 0.5 dE (X S W[1,:] + uOUnc) S[n] ./ rho`` (``:990-997``)."""
-        nx, ny = self.settings.NCellsX, self.settings.NCellsY
-        uOUnc = psi.reshape(nx * ny, -1) @ self.MReduced[0, :]
+        uOUnc = psi.reshape(self.n_cells, -1) @ self.MReduced[0, :]
         self.dose += 0.5 * dE * (X @ (S @ W[0, :]) + uOUnc) * Sn / self.densityVec
 
     # Grams used by the streaming substeps
@@ -216,6 +216,10 @@ class SolverCSD:
 
     def _s_stream(self, S, G, C, dE, sign=-1.0):
         return S + sign * dE * (G[0] @ S @ C[0] + G[1] @ S @ C[1] + G[2] @ S @ C[2] + G[3] @ S @ C[3])
+
+    def _op_sum(self, G, S, C):
+        """sum_d G_d S C_d over the streaming operators (the eta products, ``:2220``)."""
+        return G[0] @ S @ C[0] + G[1] @ S @ C[1] + G[2] @ S @ C[2] + G[3] @ S @ C[3]
 
     def truncate(self, X, S, W):
         """``truncate!`` (``SolverCSD.jl:3369-3399``): l1 tail test, clamp [2, r]."""
@@ -257,7 +261,7 @@ def init_factors(solver, r):
     """``svd!(zeros)`` factors (``SolverCSD.jl:931-938``): first r identity columns;
     X's boundary rows are then zeroed (``:955``)."""
     s = solver.settings
-    n = s.NCellsX * s.NCellsY
+    n = solver.n_cells
     X = np.eye(n, r)
     W = np.eye(solver.N, r)
     S = np.zeros((r, r))
@@ -280,7 +284,7 @@ def _fixed_scatter(solver, X, S, W, psi, Dvec, D, dE):
     # in scattering, K-step
     X[bnd, :] = 0.0
     K = X @ S
-    psiv = psi.reshape(s.NCellsX * s.NCellsY, -1)
+    psiv = psi.reshape(solver.n_cells, -1)
     K = K + dE * psiv @ (Mr.T @ (Dvec[:, None] * W))
     K[bnd, :] = 0.0
     XNew = la.orth(K, mode, order=solver.x_completion)
@@ -537,7 +541,7 @@ def solve_dlr_parallel(solver: SolverCSD, max_steps: int | None = None, state: d
         S[...] = Snew  # S .= S2 * Diagonal(S1)
         # in scattering
         MtDW = Mr.T @ (Dvec[:, None] * W)
-        psiv = psi.reshape(nx * ny, -1)
+        psiv = psi.reshape(solver.n_cells, -1)
         Xtpsi = X.T @ psiv  # before X[bnd] = 0 (:1904)
         X[bnd, :] = 0.0
         K = X @ S
@@ -650,7 +654,7 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict |
             else:
                 Gt = solver._x_grams(X1T, X)
                 Ct = solver._w_grams(W, W1T)
-                eta = np.linalg.norm(Gt[0] @ S @ Ct[0] + Gt[1] @ S @ Ct[1] + Gt[2] @ S @ Ct[2] + Gt[3] @ S @ Ct[3])
+                eta = np.linalg.norm(solver._op_sum(Gt, S, Ct))
                 etaVec.append(eta)
                 etaVecTime.append(energy[n - 1])
                 bound = s.c_eta * s.theta * max(1e-7, np.linalg.norm(Sup) ** s.thetaIndex) / dE
@@ -670,7 +674,7 @@ def solve_dlr_bug(solver: SolverCSD, max_steps: int | None = None, state: dict |
         S[...] = Snew
         # in scattering
         MtDW = Mr.T @ (Dvec[:, None] * W)
-        psiv = psi.reshape(nx * ny, -1)
+        psiv = psi.reshape(solver.n_cells, -1)
         Xtpsi = X.T @ psiv
         X[bnd, :] = 0.0
         K = X @ S
@@ -823,7 +827,7 @@ def solve_dlr_parallel_rejection(solver: SolverCSD, max_steps: int | None = None
             else:
                 Gt = solver._x_grams(X1T, X)
                 Ct = solver._w_grams(W, W1T)
-                eta = np.linalg.norm(Gt[0] @ S @ Ct[0] + Gt[1] @ S @ Ct[1] + Gt[2] @ S @ Ct[2] + Gt[3] @ S @ Ct[3])
+                eta = np.linalg.norm(solver._op_sum(Gt, S, Ct))
                 etaVec.append(eta)
                 etaVecTime.append(energy[n - 1])
                 bound = s.c_eta * s.theta * max(1e-7, np.linalg.norm(SUP) ** s.thetaIndex) / dE
@@ -845,7 +849,7 @@ def solve_dlr_parallel_rejection(solver: SolverCSD, max_steps: int | None = None
         S[...] = Snew
         # in scattering
         MtDW = Mr.T @ (Dvec[:, None] * W)
-        psiv = psi.reshape(nx * ny, -1)
+        psiv = psi.reshape(solver.n_cells, -1)
         Xtpsi = X.T @ psiv
         X[bnd, :] = 0.0
         K = X @ S

@@ -155,6 +155,10 @@ def stopping_power(kind: str, E):
         return 0.2 / E * np.log1p(10.0 * E)
     if kind == "proton_bethe":
         return 250.0 / E * np.log(0.07 * E)
+    if kind == "proton_log1p":
+        # (a / E) ln(1 + b E), a = 250 MeV^2 cm^2/g, b = 0.07 / MeV: the Bethe-like
+        # form (a / E) ln(b E) is negative below 1/b = 14.3 MeV
+        return 250.0 / E * np.log1p(0.07 * E)
     raise ValueError(f"unknown stopping power {kind!r}")
 
 

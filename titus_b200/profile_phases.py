@@ -2,6 +2,7 @@
 
     python -m titus_b200.profile_phases [--nx 101] [--npn 21] [--r 20] [--steps 200] [--team 0]
                                         [--method fixed|parallel|bug] [--problem csdWaterBeam]
+                                        [--precision fp64|mixed] [--theta 1e-2]
 
 Timers are exclusive (each cycle is charged to the innermost open phase) and
 recorded on the first CTA; "total" is their sum.
@@ -26,11 +27,16 @@ def main():
     ap.add_argument("--team", type=int, default=0)
     ap.add_argument("--problem", default="csdWaterBeam")
     ap.add_argument("--method", default="fixed", choices=["fixed", "parallel", "bug"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--theta", type=float, default=None, help="truncation tolerance (problem default if unset)")
     a = ap.parse_args()
     method = {"fixed": _lib.TITUS_DLR_FIXED, "parallel": _lib.TITUS_PARALLEL_ADAPTIVE,
               "bug": _lib.TITUS_BUG_ADAPTIVE}[a.method]
     s = Settings(a.nx, a.nx, a.r, a.problem, nPN=a.npn)
-    g = SolverCSD(s, team_ctas=a.team)
+    if a.theta is not None:
+        s.theta = a.theta
+    prec = {"fp64": _lib.TITUS_PRECISION_FP64, "mixed": _lib.TITUS_PRECISION_MIXED}[a.precision]
+    g = SolverCSD(s, team_ctas=a.team, precision=prec)
     g.run(method, max_steps=5)
     t0 = time.perf_counter()
     out = g.run(method, max_steps=a.steps, profile=True)
