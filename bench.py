@@ -2,14 +2,17 @@
 """Benchmark: dose solves/s of the CSD-DLR energy loop on the B200 (plain FP64).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl titus|reference]
-                    [--method bug|parallel|fixed|batched] [--no-batched] [--no-cpu-baseline]
+                    [--method bug|parallel|fixed|pn_full|pn3d|batched] [--no-batched] [--no-cpu-baseline]
 
 Workload (default ``bug``): the seeded water/lung/bone phantom on 200 x 200
 cells, P_29 (900 moments), rank cap 80, 5 MeV -> 1 keV electrons in 29 697
 energy steps (29 695 loop iterations), solved with the rank-adaptive BUG
 integrator. ``--method parallel`` runs the parallel integrator on it;
 ``--method fixed`` the fixed-rank integrator on the 100 x 100 water beam
-(P_21, r = 20); ``--method batched`` makes the batched pencil-beam plan below
+(P_21, r = 20); ``--method pn_full`` the full-rank P_N solver on that water
+beam; ``--method pn3d`` the full-rank P_N solver on the 3D proton problem (96^3
+cells at 1 mm, seeded water / lung / bone spheres, P_13, 90 -> 1 MeV in 1336
+energy steps); ``--method batched`` makes the batched pencil-beam plan below
 the timed step.
 
 A step is one complete dose solve (the whole energy sweep, one kernel
@@ -62,6 +65,9 @@ WORKLOADS = {
                   method="fixed"),
     "pn_full": dict(name="csd_water_beam_100x100_P21_full_rank", Nx=101, r=4, nPN=21, problem="csdWaterBeam",
                     method="pn_full"),
+    # the 3D proton problem (96^3 cells at 1 mm, seeded spheres, P13) with the full-rank solver
+    "pn3d": dict(name="csd_proton3d_96cube_P13_full_rank", Nx=97, r=40, nPN=13, problem="csdProton3D",
+                 method="pn3d"),
 }
 BATCHED = dict(name="pencil_beams256_phantom_128x128_P21_cap60_bug", Nx=129, r=60, nPN=21, problem="csdPhantom",
                spots=256, seed=3, emin=2.0, emax=8.0, ymin=0.1, ymax=0.9)
@@ -157,6 +163,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------ CPU baseline
 def _oracle_setup(w):
+    if w["method"] == "pn3d":
+        from oracle.three_d import Settings3D as OSettings3D
+        from oracle.three_d import SolverCSD3D as OSolver3D
+
+        return lambda: OSolver3D(OSettings3D(w["Nx"], w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"]))
     from oracle.settings import Settings as OSettings
     from oracle.solver import SolverCSD as OSolver
 
@@ -220,6 +231,17 @@ def cpu_cost_model(w, ranks, state200=None, head=40, tail=20):
         per = (time.perf_counter() - t0) / head
         steps = o.csd.eTrafo.size - 1
         return per * steps, (f"FP64 oracle, full-rank P_N: {head} energy steps timed, x {steps} steps "
+                             f"(constant cost per step)"), None
+    if w["method"] == "pn3d":
+        from oracle.three_d import solve_pn_full_3d
+
+        o = mk()
+        k = 2   # one 96^3 x 196 step of the oracle takes tens of seconds
+        t0 = time.perf_counter()
+        solve_pn_full_3d(o, max_steps=k)
+        per = (time.perf_counter() - t0) / k
+        steps = o.csd.eTrafo.size - 1
+        return per * steps, (f"FP64 oracle, 3D full-rank P_N: {k} energy steps timed, x {steps} steps "
                              f"(constant cost per step)"), None
     fn = {"bug": solve_dlr_bug, "parallel": solve_dlr_parallel, "fixed": solve_dlr_fixed}[w["method"]]
     if w["method"] == "fixed":
@@ -355,11 +377,14 @@ def run_gpu_pn_full(args, w, rank, world, local_rank, dist):
     import numpy as np
     import torch
 
-    from titus_b200 import Settings, SolverCSD, _lib
+    from titus_b200 import Settings, Settings3D, SolverCSD, SolverCSD3D, _lib
     from titus_b200.replicas import replica_throughput
 
-    s = Settings(w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"])
-    solver = SolverCSD(s)
+    three_d = w["method"] == "pn3d"
+    if three_d:
+        solver = SolverCSD3D(Settings3D(w["Nx"], w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"]))
+    else:
+        solver = SolverCSD(Settings(w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"]))
     lib = _lib.load()
     h = solver.handle()
     opt = solver.options()
@@ -392,6 +417,13 @@ def run_gpu_pn_full(args, w, rank, world, local_rank, dist):
     _lib.check(lib.titus_pn_full_fetch(h, None, _lib.as_dp(dose), None), "titus_pn_full_fetch")
     # end to end: upload, solve, u/dose/psi copy-out, free
     p, keep = solver.problem_struct()
+    ext = None
+    if three_d:
+        ext = _lib.Problem3D()
+        ext.nz, ext.dz = solver.settings.NCellsZ, solver.settings.dz
+        for d, (rp, ci, v) in enumerate(solver.ops3):
+            keep += [rp, ci, v]
+            ext.op_rowptr[d], ext.op_col[d], ext.op_val[d] = _lib.as_ip(rp), _lib.as_ip(ci), _lib.as_dp(v)
     h2d = sum(a.nbytes for a in keep)
     u = np.zeros((solver.n, solver.N))
     psi = np.zeros((solver.n, solver.q))
@@ -399,16 +431,25 @@ def run_gpu_pn_full(args, w, rank, world, local_rank, dist):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     h2 = C.c_void_p()
-    _lib.check(lib.titus_create(C.byref(p), C.byref(h2)), "titus_create")
+    if three_d:
+        _lib.check(lib.titus_create_3d(C.byref(p), C.byref(ext), C.byref(h2)), "titus_create_3d")
+    else:
+        _lib.check(lib.titus_create(C.byref(p), C.byref(h2)), "titus_create")
     rc = lib.titus_pn_full_solve(h2, C.byref(opt), _lib.as_dp(u), _lib.as_dp(dose), _lib.as_dp(psi))
     lib.titus_destroy(h2)
     _lib.check(rc, "titus_pn_full_solve")
     e2e_value, _ = replica_throughput(1, time.perf_counter() - t0, world, device="cuda")
     steps = solver.nE - 1
     nN = solver.n * solver.N
-    # per step: moments read u, write W (5 nN); stream reads u, W (4 nN), writes u' (6 nN);
-    # psi read + write (2 n q), dose read + write (2 n)
-    alg = steps * 8 * (11 * nN + 2 * solver.n * solver.q + 2 * solver.n)
+    if three_d:
+        # per step, the fused stencil + moment kernel reads u and writes u' (2 nN); psi is
+        # written by the sweep and read by the sweep and the stream kernel (3 n q); the
+        # dose is read and written and 1/rho read once (3 n)
+        alg = steps * 8 * (2 * nN + 3 * solver.n * solver.q + 3 * solver.n)
+    else:
+        # per step: moments read u, write W (5 nN); stream reads u, W (4 nN), writes u' (6 nN);
+        # psi read + write (2 n q), dose read + write (2 n)
+        alg = steps * 8 * (11 * nN + 2 * solver.n * solver.q + 2 * solver.n)
     peak, peak_kind = read_peaks()
     achieved = alg / (t_max / args.steps) / 1e9
     info = dict(value=value, ms_per_step=t_max / args.steps * 1e3, e2e_value=e2e_value, h2d=h2d, d2h=d2h,
@@ -622,7 +663,7 @@ def run_reference(args, w, rank):
                      "config": batched_config(cfg, world=args.gpus)})
     else:
         ranks = _ranks_for(w)
-        if ranks is None and w["method"] not in ("fixed", "pn_full"):
+        if ranks is None and w["method"] not in ("fixed", "pn_full", "pn3d"):
             print(json.dumps({"impl": "reference", "unavailable": "rank-history fixture missing: run "
                               "tests/golden/make_rank_history.py on a GPU"}), flush=True)
             return
@@ -645,10 +686,11 @@ def run_reference(args, w, rank):
 
 def solve_config(w, iterations=None, world=1, team=148):
     """The `config` dict both arms print for a single-solve workload."""
-    cells = (w["Nx"] - 1) ** 2
+    cells = (w["Nx"] - 1) ** (3 if w["method"] == "pn3d" else 2)
     cfg = {"workload": w["name"], "cells": cells, "moments": (w["nPN"] + 1) ** 2, "method": w["method"],
-           "rank_cap" if w["method"] != "fixed" else "rank": w["r"], "parallelism": f"replicas{world}",
-           "l2": "flushed between solves (256 MB write)"}
+           "parallelism": f"replicas{world}", "l2": "flushed between solves (256 MB write)"}
+    if w["method"] not in ("pn_full", "pn3d"):
+        cfg["rank_cap" if w["method"] != "fixed" else "rank"] = w["r"]
     if iterations is not None:
         cfg["loop_iterations"] = int(iterations)
     return cfg
@@ -690,7 +732,7 @@ def run_gpu(args, w, rank, world, local_rank):
                 t, sample = batched_reference_seconds(BATCHED)
                 line["cpu_baseline"] = {"value": BATCHED["spots"] / t, "unit": "solves/s",
                                         "cores": cores, "kind": "port", "sample": sample}
-    elif args.method == "pn_full":
+    elif args.method in ("pn_full", "pn3d"):
         info = run_gpu_pn_full(args, w, rank, world, local_rank, dist)
         if rank == 0:
             line = {"metric": "dose solves/s", "value": info["value"], "unit": "solves/s", "n_gpus": world,
@@ -703,8 +745,9 @@ def run_gpu(args, w, rank, world, local_rank):
                     "roofline": {"bound": "hbm", "achieved": info["achieved"], "peak": info["peak"], "unit": "GB/s",
                                  "frac": info["achieved"] / info["peak"], "traffic": None,
                                  "peak_kind": info["peak_kind"], "algorithmic_bytes_per_launch": info["alg"],
-                                 "note": "all three kernels of every energy step (one graph launch)"},
-                    "clocks": info["clocks"], "gpu_launches": 3 * info["steps_per_solve"] * args.steps,
+                                 "note": "all kernels of every energy step (one graph launch)"},
+                    "clocks": info["clocks"],
+                    "gpu_launches": (2 if args.method == "pn3d" else 3) * info["steps_per_solve"] * args.steps,
                     "dose_max": info["dose_max"], "cpu_baseline": None}
             if world == 1 and not args.no_cpu_baseline:
                 cores = host_threads()

@@ -290,6 +290,28 @@ int titus_pn_full_fetch(titus_solver_t* solver, double* u_out, double* dose_out,
 int titus_pn_full_solve(titus_solver_t* solver, const titus_options_t* options, double* u_out, double* dose_out,
                         double* psi_out);
 
+/* Three-dimensional problems (no counterpart in the reference, which is 2D:
+ * code/stencils.jl:7-11 builds x and y stencils only). The same scheme with a
+ * z direction: cell (i, j, k) has row (k*nx + i)*ny + j (z slowest, so every
+ * z layer is a 2D grid in the reference's row order); the boundary (ghost)
+ * cells are those on any of the six faces; z streams with the P_N matrix Ay
+ * (PNSystem.jl:142-194, unused in 2D) and its Roe |Ay|, through the
+ * density-weighted stencils of stencils.jl written with dz; the uncollided
+ * sweep adds (Omega_y / dz) times the upwind z difference.
+ * titus_create_3d takes the 2D problem struct with every cell array (density,
+ * bc_space, x_completion and sweep_restore indices) over nx ny nz cells, plus
+ * this extension. A 3D handle runs the full-rank P_N solver
+ * (titus_pn_full_solve*, u and psi over nx ny nz rows); the DLR entry points
+ * return TITUS_ERR_ARG for it. */
+typedef struct titus_problem_3d {
+    int32_t nz;                   /* z layers (>= 3) */
+    double dz;                    /* z spacing (> 0) */
+    const int32_t* op_rowptr[2];  /* CSR (N x N) of Ay, |Ay| */
+    const int32_t* op_col[2];
+    const double* op_val[2];
+} titus_problem_3d_t;
+int titus_create_3d(const titus_problem_t* problem, const titus_problem_3d_t* ext, titus_solver_t** out);
+
 /* Dose objective and its gradients (no counterpart in the reference, which
  * has no adjoint): J = sum_c weight[c] (dose[c] - target[c])^2 of the sweep's
  * dose, or any J whose dJ/d(dose) the caller passes in dj_ddose (then weight

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     txt = open(os.path.join(ROOT, "include", "titus.h")).read()
-    return sorted(set(re.findall(r"\b(titus_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(titus_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_header_matches_binding():
@@ -67,3 +67,19 @@ def test_non_finite_inputs_are_rejected_without_gpu(field, index, value):
     assert rc == 1
     err = _lib.last_error()
     assert ("not finite" in err or "density must be > 0" in err) and field.split("_")[0] in err, err
+
+
+def test_invalid_3d_extension_is_rejected_without_gpu():
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libtitus.so not built")
+    import ctypes as C
+    lib = _lib.load()
+    p = _lib.Problem()
+    e = _lib.Problem3D()
+    e.nz, e.dz = 2, 0.1   # too few z layers: rejected before any CUDA call
+    h = C.c_void_p()
+    assert lib.titus_create_3d(C.byref(p), C.byref(e), C.byref(h)) == _lib.TITUS_ERR_ARG
+    assert "nz" in _lib.last_error()
+    e.nz, e.dz = 5, float("nan")
+    assert lib.titus_create_3d(C.byref(p), C.byref(e), C.byref(h)) == _lib.TITUS_ERR_ARG
+    assert lib.titus_create_3d(C.byref(p), None, C.byref(h)) == _lib.TITUS_ERR_ARG

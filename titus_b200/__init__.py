@@ -1,6 +1,7 @@
 """titus_b200: B200-native (sm_100a) CSD energy step of TITUS behind its Settings/SolverCSD/Solve* API."""
-from .settings import Settings  # noqa: F401
-from .solver import (DoseAdjoint, PencilBeamBatch, SolveBatchedPencilBeams, SolverCSD, SolveFirstCollisionSource,  # noqa: F401
+from .settings import Settings, Settings3D  # noqa: F401
+from .solver import (DoseAdjoint, PencilBeamBatch, SolveBatchedPencilBeams, SolverCSD, SolverCSD3D,  # noqa: F401
+                     SolveFirstCollisionSource,
                      SolveFirstCollisionSourceDLR, SolveFirstCollisionSourceDLRHighOrder,
                      SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel,
                      SolveFirstCollisionSourceDLRParallelRejection, scalar_flux)

@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtitus.so")
 
+TITUS_OK, TITUS_ERR_ARG, TITUS_ERR_CUDA, TITUS_ERR_DEVICE, TITUS_ERR_LIMIT = 0, 1, 2, 3, 4
 TITUS_DLR_FIXED = 0
 TITUS_PARALLEL_ADAPTIVE = 1
 TITUS_BUG_ADAPTIVE = 2
@@ -49,6 +50,11 @@ class Problem(C.Structure):
     ]
 
 
+class Problem3D(C.Structure):
+    _fields_ = [("nz", C.c_int32), ("dz", C.c_double), ("op_rowptr", _ip * 2), ("op_col", _ip * 2),
+                ("op_val", _dp * 2)]
+
+
 class Options(C.Structure):
     _fields_ = [("team_ctas", C.c_int32), ("max_steps", C.c_int32), ("rank_tol", C.c_double),
                 ("profile", C.c_int32), ("precision", C.c_int32)]
@@ -70,6 +76,7 @@ class Spot(C.Structure):
 # (name, restype, argtypes) for every symbol include/titus.h declares
 SIGNATURES = [
     ("titus_create", C.c_int, [C.POINTER(Problem), C.POINTER(C.c_void_p)]),
+    ("titus_create_3d", C.c_int, [C.POINTER(Problem), C.POINTER(Problem3D), C.POINTER(C.c_void_p)]),
     ("titus_solve", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.POINTER(Result)]),
     ("titus_solve_device", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Options), C.c_void_p]),
     ("titus_fetch", C.c_int, [C.c_void_p, C.POINTER(Result)]),

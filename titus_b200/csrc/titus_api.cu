@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -41,13 +42,31 @@ int titus_host::fail(int code, const char* fmt, ...) {
 
 titus_solver::~titus_solver() {
     titus_host::pn_free(this);
+    titus_host::pn3_free(this);
     titus_host::wide_free(this);
     for (void* p : allocs) cudaFree(p);
 }
 
-static int validate(const titus_problem_t* pb) {
+// CSR of one P_N operator (N x N): rowptr monotone from 0, columns in range, values finite.
+static int validate_csr(const int32_t* rp, const int32_t* ci, const double* v, int N, int d) {
+    if (!rp || (!ci && rp[N] > 0) || (!v && rp[N] > 0)) return fail(TITUS_ERR_ARG, "operator %d CSR arrays missing", d);
+    if (rp[0] != 0) return fail(TITUS_ERR_ARG, "operator %d rowptr[0] != 0", d);
+    for (int m = 0; m < N; ++m)
+        if (rp[m + 1] < rp[m]) return fail(TITUS_ERR_ARG, "operator %d rowptr not monotone", d);
+    for (int p = 0; p < rp[N]; ++p) {
+        if (ci[p] < 0 || ci[p] >= N) return fail(TITUS_ERR_ARG, "operator %d column index out of range", d);
+        if (!std::isfinite(v[p])) return fail(TITUS_ERR_ARG, "operator %d value %d is not finite", d, p);
+    }
+    return TITUS_OK;
+}
+
+// `nz` = 0 for the reference's 2D problems; >= 3 z layers for a 3D problem
+// (titus_create_3d), whose cell arrays hold nx ny nz entries.
+static int validate(const titus_problem_t* pb, int nz = 0) {
     if (!pb) return fail(TITUS_ERR_ARG, "problem is NULL");
     if (pb->nx < 3 || pb->ny < 3) return fail(TITUS_ERR_ARG, "need nx, ny >= 3 (got %d, %d)", pb->nx, pb->ny);
+    if ((long long)pb->nx * pb->ny * (nz ? nz : 1) > INT_MAX / 64)
+        return fail(TITUS_ERR_LIMIT, "%d x %d x %d cells exceed this build's index range", pb->nx, pb->ny, nz);
     if (pb->npn < 0) return fail(TITUS_ERR_ARG, "npn < 0");
     if (pb->n_moments != (pb->npn + 1) * (pb->npn + 1))
         return fail(TITUS_ERR_ARG, "n_moments %d != (npn+1)^2", pb->n_moments);
@@ -69,7 +88,7 @@ static int validate(const titus_problem_t* pb) {
         if (!p) return fail(TITUS_ERR_ARG, "a required problem array is NULL");
     // non-finite inputs would propagate through the whole energy loop unnoticed
     {
-        const int n = pb->nx * pb->ny, nE = pb->n_energies, q = pb->n_ordinates, N = pb->n_moments;
+        const int n = pb->nx * pb->ny * (nz ? nz : 1), nE = pb->n_energies, q = pb->n_ordinates, N = pb->n_moments;
         struct Arr {
             const double* p;
             size_t count;
@@ -88,13 +107,9 @@ static int validate(const titus_problem_t* pb) {
             for (size_t i = 0; i < a.count; ++i)
                 if (!std::isfinite(a.p[i])) return fail(TITUS_ERR_ARG, "%s[%zu] is not finite", a.name, i);
     }
-    for (int d = 0; d < 4; ++d)
-        if (!pb->op_rowptr[d] || (!pb->op_col[d] && pb->op_rowptr[d][pb->n_moments] > 0) ||
-            (!pb->op_val[d] && pb->op_rowptr[d][pb->n_moments] > 0))
-            return fail(TITUS_ERR_ARG, "operator %d CSR arrays missing", d);
     if (pb->n_x_completion < 0 || pb->n_w_completion < 0 || pb->n_sweep_restore < 0)
         return fail(TITUS_ERR_ARG, "negative list length");
-    const int n = pb->nx * pb->ny;
+    const int n = pb->nx * pb->ny * (nz ? nz : 1);
     for (int i = 0; i < n; ++i)
         if (!(pb->density[i] > 0)) return fail(TITUS_ERR_ARG, "density must be > 0 (cell %d)", i);
     for (int i = 0; i < pb->n_x_completion; ++i)
@@ -104,30 +119,21 @@ static int validate(const titus_problem_t* pb) {
             return fail(TITUS_ERR_ARG, "w_completion out of range");
     for (int i = 0; i < pb->n_sweep_restore; ++i)
         if (pb->sweep_restore[i] < 0 || pb->sweep_restore[i] >= n) return fail(TITUS_ERR_ARG, "sweep_restore out of range");
-    for (int d = 0; d < 4; ++d) {
-        const int32_t* rp = pb->op_rowptr[d];
-        if (rp[0] != 0) return fail(TITUS_ERR_ARG, "operator %d rowptr[0] != 0", d);
-        for (int m = 0; m < pb->n_moments; ++m)
-            if (rp[m + 1] < rp[m]) return fail(TITUS_ERR_ARG, "operator %d rowptr not monotone", d);
-        for (int p = 0; p < rp[pb->n_moments]; ++p) {
-            if (pb->op_col[d][p] < 0 || pb->op_col[d][p] >= pb->n_moments)
-                return fail(TITUS_ERR_ARG, "operator %d column index out of range", d);
-            if (!std::isfinite(pb->op_val[d][p])) return fail(TITUS_ERR_ARG, "operator %d value %d is not finite", d, p);
-        }
-    }
+    for (int d = 0; d < 4; ++d)
+        if (int rc = validate_csr(pb->op_rowptr[d], pb->op_col[d], pb->op_val[d], pb->n_moments, d)) return rc;
     return TITUS_OK;
 }
 
 // Uploads the problem into `s`; on any failure the caller deletes `s`, which
 // releases every allocation made so far.
-static int create_impl(const titus_problem_t* pb, titus_solver* s) {
+static int create_impl(const titus_problem_t* pb, titus_solver* s, int nz = 0) {
     int rc;
     CK(cudaGetDevice(&s->device));
     CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
     int coop = 0;
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device));
     if (!coop) return fail(TITUS_ERR_CUDA, "device does not support cooperative launch");
-    const int n = pb->nx * pb->ny, N = pb->n_moments, q = pb->n_ordinates, nE = pb->n_energies;
+    const int n = pb->nx * pb->ny * (nz ? nz : 1), N = pb->n_moments, q = pb->n_ordinates, nE = pb->n_energies;
     s->n = n;
     s->N = N;
     s->q = q;
@@ -266,6 +272,43 @@ extern "C" int titus_create(const titus_problem_t* pb, titus_solver_t** out) {
     return TITUS_OK;
 }
 
+extern "C" int titus_create_3d(const titus_problem_t* pb, const titus_problem_3d_t* ext, titus_solver_t** out) {
+    if (!out) return fail(TITUS_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!ext) return fail(TITUS_ERR_ARG, "3D extension is NULL");
+    if (ext->nz < 3) return fail(TITUS_ERR_ARG, "need nz >= 3 (got %d)", ext->nz);
+    if (!(ext->dz > 0) || !std::isfinite(ext->dz)) return fail(TITUS_ERR_ARG, "dz must be finite and > 0");
+    int rc = validate(pb, ext->nz);
+    if (rc) return rc;
+    for (int d = 0; d < 2; ++d)
+        if ((rc = validate_csr(ext->op_rowptr[d], ext->op_col[d], ext->op_val[d], pb->n_moments, 4 + d))) return rc;
+    auto* s = new titus_solver();
+    rc = create_impl(pb, s, ext->nz);
+    for (int d = 0; d < 2 && !rc; ++d) {
+        const int nnz = ext->op_rowptr[d][pb->n_moments];
+        int32_t* rp = nullptr;
+        int32_t* ci = nullptr;
+        double* v = nullptr;
+        if (!(rc = s->alloc(&rp, (size_t)pb->n_moments + 1, ext->op_rowptr[d])) &&
+            !(rc = s->alloc(&ci, nnz, ext->op_col[d])) && !(rc = s->alloc(&v, nnz, ext->op_val[d])))
+            s->op3[d] = Csr{rp, ci, v};
+    }
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    s->nz = ext->nz;
+    s->dz = ext->dz;
+    *out = s;
+    return TITUS_OK;
+}
+
+// The DLR integrators, their batched and resumed forms run the reference's 2D
+// problems; a 3D handle (titus_create_3d) runs the full-rank P_N solver.
+static int reject_3d(const titus_solver* s, const char* what) {
+    return s->nz ? fail(TITUS_ERR_ARG, "%s: 3D problems run with titus_pn_full_solve", what) : TITUS_OK;
+}
+
 // Initial factors of SolverCSD.jl:931-955: X = first r identity columns with
 // boundary rows zeroed, W = first r identity columns, S = 0.
 __global__ void init_factors_kernel(TeamState* states, int n, int N, int nx, int ny, int r, int nE) {
@@ -387,6 +430,7 @@ static int check_precision(int method, const titus_options_t* opt) {
 
 extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus_options_t* opt, void* stream_) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (int rc = reject_3d(s, "titus_solve")) return rc;
     if (int rc = check_precision(method, opt)) return rc;
     cudaStream_t stream = (cudaStream_t)stream_;
     if (is_wide_family(method)) {
@@ -453,6 +497,7 @@ extern "C" int titus_solve_problem(const titus_problem_t* pb, int32_t method, co
 extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X, const double* S, const double* W,
                                const double* psi, const double* dose, int32_t n_next) {
     if (!s || !X || !S || !W || !psi || !dose) return fail(TITUS_ERR_ARG, "NULL argument");
+    if (int rc = reject_3d(s, "titus_set_state")) return rc;
     if (rank < 1 || rank > wide::RA) return fail(TITUS_ERR_LIMIT, "rank %d outside [1, %d]", rank, wide::RA);
     if (n_next < 2 || n_next > s->nE + 1) return fail(TITUS_ERR_ARG, "n_next %d outside [2, nE+1]", n_next);
     // the adaptive integrators' state always; the fixed-rank state when the rank fits
@@ -482,6 +527,7 @@ extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X,
 extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t n_stop,
                                 titus_result_t* res) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (int rc = reject_3d(s, "titus_solve_from")) return rc;
     if (int rc = check_precision(method, opt)) return rc;
     if (is_wide_family(method)) {
         s->last_method = method;
@@ -504,6 +550,7 @@ extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_o
 extern "C" int titus_solve_batched(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t nspots,
                                    const titus_spot_t* spots, double* dose_out, int32_t* rank_out, int32_t* iters_out) {
     if (!s || !spots || !dose_out) return fail(TITUS_ERR_ARG, "NULL argument");
+    if (int rc = reject_3d(s, "titus_solve_batched")) return rc;
     if (method != TITUS_PARALLEL_ADAPTIVE && method != TITUS_BUG_ADAPTIVE)
         return fail(TITUS_ERR_ARG, "batched solves run the adaptive integrators (method 1 or 2), got %d", method);
     if (int rc = check_precision(method, opt)) return rc;
@@ -516,6 +563,7 @@ extern "C" int titus_batch_upload(titus_solver_t* s, int32_t nspots, const titus
                                   titus_batch_t** out) {
     if (!s || !spots || !out) return fail(TITUS_ERR_ARG, "NULL argument");
     *out = nullptr;
+    if (int rc = reject_3d(s, "titus_batch_upload")) return rc;
     if (nspots < 1) return fail(TITUS_ERR_ARG, "nspots < 1");
     return titus_host::batch_upload(s, nspots, spots, out);
 }

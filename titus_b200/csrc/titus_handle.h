@@ -10,6 +10,7 @@
 struct titus_solver;
 struct titus_batch;
 struct titus_pn_state;
+struct titus_pn3_state;
 
 namespace titus_host {
 
@@ -50,8 +51,11 @@ int batch_launch(titus_batch* b, int method, const titus_options_t* opt, cudaStr
 int batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out, int32_t* iters_out);
 void batch_free(titus_batch* b);
 int batch_rank_sums(titus_batch* b, int32_t* out);
-// full-rank P_N solver state (titus_pn_full.cu)
+// full-rank P_N solver state (titus_pn_full.cu; 3D: titus_pn3d.cu)
 void pn_free(titus_solver* s);
+void pn3_free(titus_solver* s);
+int pn3_solve_device(titus_solver* s, const titus_options_t* opt, cudaStream_t stream);
+int pn3_fetch(titus_solver* s, double* u_out, double* dose_out, double* psi_out);
 int wide_solve_batched(titus_solver* s, int method, const titus_options_t* opt, int nspots, const titus_spot_t* spots,
                        double* dose_out, int32_t* rank_out, int32_t* iters_out);
 
@@ -84,6 +88,12 @@ struct titus_solver {
     int wide_state_valid = 0;   // 1 after an adaptive solve or titus_set_state
     // full-rank P_N solver (allocated on first use) and csd.SMid
     titus_pn_state* pn = nullptr;
+    // 3D problems (titus_create_3d): z layers, spacing, the z pair Ay / |Ay|
+    // (device CSR) and the 3D full-rank solver state
+    int nz = 0;
+    double dz = 0.0;
+    titus::Csr op3[2] = {};
+    titus_pn3_state* pn3 = nullptr;
     double* smid = nullptr;
     // test hook (titus_debug_barrier_fault), consumed by the next launch
     long long dbg_spin_limit = 0;

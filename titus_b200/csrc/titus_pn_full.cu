@@ -304,6 +304,7 @@ extern "C" int titus_pn_full_solve_device(titus_solver_t* s, const titus_options
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
     if (opt && opt->precision != TITUS_PRECISION_FP64)
         return fail(TITUS_ERR_ARG, "the full-rank P_N solver runs in FP64 only (precision %d)", opt->precision);
+    if (s->nz) return titus_host::pn3_solve_device(s, opt, (cudaStream_t)stream_);
     int rc = pn_ensure(s);
     if (rc) return rc;
     titus_pn_state* st = s->pn;
@@ -366,6 +367,7 @@ extern "C" int titus_pn_full_solve_device(titus_solver_t* s, const titus_options
 
 extern "C" int titus_pn_full_fetch(titus_solver_t* s, double* u_out, double* dose_out, double* psi_out) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (s->nz) return titus_host::pn3_fetch(s, u_out, dose_out, psi_out);
     if (!s->pn || !s->pn->have_result) return fail(TITUS_ERR_ARG, "no full-rank solve has run on this handle");
     titus_pn_state* st = s->pn;
     CK(cudaDeviceSynchronize());
@@ -612,6 +614,7 @@ extern "C" int titus_dose_adjoint(titus_solver_t* s, int32_t method, const titus
                                   double* objective_out, double* dose_out, double* grad_density,
                                   double* grad_profile) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
+    if (s->nz) return fail(TITUS_ERR_ARG, "titus_dose_adjoint: the adjoint runs the reference's 2D problems");
     if (method != TITUS_PN_FULL)
         return fail(TITUS_ERR_ARG, "titus_dose_adjoint: method %d has no adjoint (TITUS_PN_FULL = %d)", method,
                     TITUS_PN_FULL);

@@ -83,6 +83,58 @@ def flux_matrices(npn: int):
     return Ax, Az
 
 
+def flux_matrix_y(npn: int):
+    """Dense Ay of the real-SH P_N system (``PNSystem.jl:142-194``; unused by
+    the reference's 2D solvers, the z direction of the 3D problems). It is the
+    moment matrix of Omega_y: M diag(Omega_y) O."""
+    N = (npn + 1) ** 2
+    Ay = np.zeros((N, N))
+    r2 = math.sqrt(2.0)
+
+    def frac(a, b):
+        return math.sqrt(a / b)
+
+    def C_(l, k):
+        return frac((l + k + 1) * (l + k + 2), (2 * l + 3) * (2 * l + 1))
+
+    def D_(l, k):
+        return frac((l - k) * (l - k - 1), (2 * l + 1) * (2 * l - 1))
+
+    def E_(l, k):
+        return frac((l - k + 1) * (l - k + 2), (2 * l + 3) * (2 * l + 1))
+
+    def F_(l, k):
+        return frac((l + k) * (l + k - 1), (2 * l + 1) * (2 * l - 1))
+
+    def Ct(l, k):
+        return 0.0 if k < 0 else (r2 * C_(l, k) if k == 0 else C_(l, k))
+
+    def Dt(l, k):
+        return 0.0 if k < 0 else (r2 * D_(l, k) if k == 0 else D_(l, k))
+
+    def Et(l, k):
+        return r2 * E_(l, k) if k == 1 else E_(l, k)
+
+    def Ft(l, k):
+        return r2 * F_(l, k) if k == 1 else F_(l, k)
+
+    sgn = lambda k: 1 if k >= 0 else -1  # noqa: E731
+    for l in range(npn + 1):
+        for k in range(-l, l + 1):
+            i = moment_index(l, k)
+            kp, km, s = k + sgn(k), k - sgn(k), sgn(k)
+            ent = []
+            if k != 1:
+                ent.append((moment_index(l - 1, -km), -0.5 * s * Ct(l - 1, abs(k) - 1)))
+                ent.append((moment_index(l + 1, -km), 0.5 * s * Dt(l + 1, abs(k) - 1)))
+            ent.append((moment_index(l - 1, -kp), -0.5 * s * Et(l - 1, abs(k) + 1)))
+            ent.append((moment_index(l + 1, -kp), 0.5 * s * Ft(l + 1, abs(k) + 1)))
+            for j, v in ent:
+                if 0 <= j < N:
+                    Ay[i, j] = v
+    return Ay
+
+
 def roe(A: np.ndarray, drop: float = 1e-10) -> np.ndarray:
     """|A| = V |Lambda| V^-1 with |entries| <= drop removed (``SolverCSD.jl:83-97``)."""
     lam, V = np.linalg.eigh(0.5 * (A + A.T))

@@ -84,3 +84,72 @@ class Settings:
         y = np.concatenate([[y[0] - self.dy], y]) + self.dy / 2
         self.y, self.yMid = y, y[:-1] + 0.5 * self.dy
         self.dE = self.cfl * min(self.dx, self.dy) * self.density.min()
+
+
+def seeded_spheres(ncx, ncy, ncz, L, seed, n_lung=3, n_bone=1, rho_water=1.0, rho_lung=0.25, rho_bone=1.85,
+                   rmin=0.5, rmax=2.0):
+    """Water cube [0, L]^3 with random lung, then bone spheres from ``default_rng(seed)``
+    (centres uniform in the inner 80 %, radii U(rmin, rmax) cm); indexed [k, i, j] = (z, x, y)."""
+    rng = np.random.default_rng(seed)
+    Z, X, Y = np.meshgrid(np.linspace(0.0, L, ncz), np.linspace(0.0, L, ncx), np.linspace(0.0, L, ncy),
+                          indexing="ij")
+    rho = np.full((ncz, ncx, ncy), rho_water)
+    for val in [rho_lung] * n_lung + [rho_bone] * n_bone:
+        c = rng.uniform(0.1 * L, 0.9 * L, 3)
+        rad = rng.uniform(rmin, rmax)
+        rho[(X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= rad * rad] = val
+    return rho
+
+
+def _ghost_axis(a, b, ncells):
+    """Cell centres spanning [a, b] with the reference's ghost shift (settings.jl:315-325)."""
+    x = np.linspace(a, b, ncells)
+    dx = x[1] - x[0]
+    x = np.concatenate([[x[0] - dx], x]) + dx / 2
+    return x, x[:-1] + 0.5 * dx, dx
+
+
+class Settings3D:
+    """Settings of the 3D proton problem ``"csdProton3D"`` (no counterpart in
+    the reference, which is 2D): a 96^3 grid at 1 mm ([0, 9.5]^3 cm with the
+    ghost-cell grid), seeded water / lung / bone spheres, a pencil beam along +x
+    entering at x = 0 centred at (y0, z0) = (4.75, 4.75) cm (spatial sigma
+    0.3 cm, angular sigma 0.01 rad about +x), protons 90 -> 1 MeV with
+    S(E) = (250 / E) ln(1 + 0.07 E) MeV cm^2/g (the Bethe-like (a/E) ln(b E)
+    is negative below 1/b = 14.3 MeV), Henyey-Greenstein sigma_l =
+    100 * 0.95^l cm^-1, P_13 (196 moments), rank cap 40. The energy step is
+    the stability bound dtau = tau_cfl min(dx, dy, dz) min(rho) with
+    tau_cfl = 1/3 (1336 steps)."""
+
+    def __init__(self, Nx: int = 97, Ny: int = 97, Nz: int = 97, r: int = 40, problem: str = "csdProton3D",
+                 nPN: int = 13, seed: int = 20240605, nEnergies: int = 0, tau_cfl: float = 1.0 / 3.0,
+                 L: float = 9.5):
+        if problem != "csdProton3D":
+            raise ValueError(f"3D problem {problem!r} not available; choose 'csdProton3D'")
+        self.problem, self.particle = problem, "Protons"
+        self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
+        self.NCellsX, self.NCellsY, self.NCellsZ = Nx - 1, Ny - 1, Nz - 1
+        self.x, self.xMid, self.dx = _ghost_axis(0.0, L, self.NCellsX)
+        self.y, self.yMid, self.dy = _ghost_axis(0.0, L, self.NCellsY)
+        self.z, self.zMid, self.dz = _ghost_axis(0.0, L, self.NCellsZ)
+        self.eRest = 938.26
+        self.eMax, self.eMin = 90.0, 1.0
+        self.stopping = "proton_log1p"
+        self.hg_g, self.sigmaT_hg = 0.95, 100.0
+        self.x0, self.y0, self.z0 = 0.0, 0.5 * L, 0.5 * L
+        self.Omega1, self.Omega2, self.Omega3 = 1.0, 0.0, 0.0
+        self.densityMin = 1.0
+        self.sigmaXInv = self.sigmaYInv = self.sigmaZInv = 1.0 / (2 * 0.3**2)
+        self.sigmaO1Inv = self.sigmaO2Inv = self.sigmaO3Inv = 1.0 / (2 * 0.01**2)
+        self.sigmaEInv = 1.0
+        self.psi_scale = 1e5
+        self.beam_peak_normalized = True
+        self.seed = seed
+        self.density = seeded_spheres(self.NCellsX, self.NCellsY, self.NCellsZ, L, seed)
+        self.r = r
+        self.theta, self.thetaIndex, self.c_eta = 1e-2, 1.0, 5.0
+        self.nPN = nPN
+        self.nEnergies = nEnergies
+        self.tau_cfl = tau_cfl
+        self.cfl = tau_cfl
+        self.dE = tau_cfl * min(self.dx, self.dy, self.dz) * self.density.min()

@@ -85,6 +85,11 @@ class SolverCSD:
         self._handle = None
         self._keep = None
 
+    @property
+    def psi_shape(self):
+        s = self.settings
+        return (s.NCellsX, s.NCellsY, self.q)
+
     def beam_tables(self, energy: float, y0: float):
         """Energy grid and PsiBeam tables of a pencil beam entering at (x0, y0)
         with energy ``energy`` on this solver's phantom (``CSD.jl:47-89``,
@@ -372,6 +377,106 @@ class PencilBeamBatch:
             pass
 
 
+class SolverCSD3D(SolverCSD):
+    """Solver data of a 3D problem (``Settings3D``; no counterpart in the
+    reference, which is 2D), uploaded with ``titus_create_3d``.
+
+    Cell (i, j, k) has row ``(k*nx + i)*ny + j``; the boundary cells are those
+    on any face. The z direction streams with the P_N matrix Ay and |Ay| (the
+    x / y pairs are the reference's), the sweep's z term uses Omega_y, and
+    PsiBeam gains the factors exp(-sigmaO2Inv (Omega2 - Omega_y)^2) and
+    exp(-sigmaZInv (z - z0)^2), applied on every face cell. The sweep's
+    boundary-slab quirk (``SolverCSD.jl:1002,1005``) is applied in every z
+    layer. A 3D handle runs the full-rank P_N solver
+    (``SolveFirstCollisionSource``).
+    """
+
+    def __init__(self, settings, team_ctas: int = 0, precision: int = _lib.TITUS_PRECISION_FP64):
+        s = settings
+        self.settings = s
+        self.team_ctas = team_ctas
+        self.precision = precision
+        nz, nx, ny = s.NCellsZ, s.NCellsX, s.NCellsY
+        self.n = nz * nx * ny
+        npn = s.nPN
+        self.N = (npn + 1) ** 2
+        self.gamma = np.array([2.0 / (2 * l + 1) for l in range(npn + 1)])
+        Ax, Az = ph.flux_matrices(npn)
+        Ay = ph.flux_matrix_y(npn)
+        self.ops = [ph.to_csr(A) for A in (Ax, Az, ph.roe(Ax), ph.roe(Az))]
+        self.ops3 = [ph.to_csr(A) for A in (Ay, ph.roe(Ay))]
+        q = npn + 1
+        self.Q_points, self.Q_weights, self.O, self.M = ph.quadrature(q, npn)
+        self.eGrid, self.eTrafo, self.S, self.SMid = ph.energy_grid(s, with_mid=True)
+        self.nE = self.eTrafo.size
+        P = self.Q_points
+        ang = np.exp(-s.sigmaO1Inv * (s.Omega1 - P[:, 0]) ** 2) * np.exp(-s.sigmaO2Inv * (s.Omega2 - P[:, 1]) ** 2) * \
+            np.exp(-s.sigmaO3Inv * (s.Omega3 - P[:, 2]) ** 2)
+        scale = s.psi_scale / ang.max() if s.beam_peak_normalized else s.psi_scale
+        # direction reduction (SolverCSD.jl:912-925): PsiBeam at eMax on the beam axis
+        beam = scale * ang * self.S[0] * s.densityMin
+        self.idxBeam = np.nonzero(beam > 1e-17 * beam.max())[0]
+        self.qReduced = self.Q_points[self.idxBeam]
+        self.MReduced = np.ascontiguousarray(self.M[:, self.idxBeam])
+        self.OReduced = self.O[self.idxBeam]
+        self.q = self.idxBeam.size
+        self.bc_angle = np.ascontiguousarray(ang[self.idxBeam])
+        self.bc_energy = scale * np.exp(-s.sigmaEInv * (s.eMax - self.eGrid) ** 2) * self.S * s.densityMin
+        self.bc_space = self.beam_profile()
+        sig = np.array([s.sigmaT_hg * s.hg_g**l for l in range(npn + 1)])
+        self.sigma = np.ascontiguousarray(np.tile(sig, (self.nE, 1)))
+        self.density = np.ascontiguousarray(np.asarray(s.density, dtype=np.float64).reshape(self.n))
+        face = np.zeros((nz, nx, ny), dtype=bool)
+        face[0], face[-1], face[:, 0], face[:, -1], face[:, :, 0], face[:, :, -1] = (True,) * 6
+        self.boundaryIdx = np.nonzero(face.ravel())[0]
+        # the 2D restore positions (L % nx, L // nx) of the reference's boundary order, per z layer
+        bidx = []
+        for i in range(nx):
+            bidx += [i * ny, i * ny + ny - 1]
+        for j in range(ny):
+            bidx += [j, (nx - 1) * ny + j]
+        Lb = np.array(bidx, dtype=np.int64)
+        layer = np.unique((Lb % nx) * ny + Lb // nx)
+        self.sweep_restore = (np.arange(nz)[:, None] * (nx * ny) + layer[None, :]).ravel().astype(np.int32)
+        self.x_completion = self.boundaryIdx.astype(np.int32)
+        self.w_completion = np.arange(self.N, dtype=np.int32)
+        self.dose = np.zeros(self.n)
+        self._handle = None
+        self._keep = None
+
+    @property
+    def psi_shape(self):
+        s = self.settings
+        return (s.NCellsZ, s.NCellsX, s.NCellsY, self.q)
+
+    def beam_profile(self, x0=None, y0=None, z0=None):
+        """PsiBeam's spatial factor at every cell for a beam centred at (x0, y0, z0)."""
+        s = self.settings
+        x0 = s.x0 if x0 is None else x0
+        y0 = s.y0 if y0 is None else y0
+        z0 = s.z0 if z0 is None else z0
+        prof = np.exp(-s.sigmaXInv * (s.xMid[None, :, None] - x0) ** 2) * \
+            np.exp(-s.sigmaYInv * (s.yMid[None, None, :] - y0) ** 2) * \
+            np.exp(-s.sigmaZInv * (s.zMid[:, None, None] - z0) ** 2)
+        return np.ascontiguousarray(np.broadcast_to(prof, (s.NCellsZ, s.NCellsX, s.NCellsY)).reshape(self.n))
+
+    def handle(self):
+        if self._handle is None:
+            lib = _lib.load()
+            p, keep = self.problem_struct()
+            e = _lib.Problem3D()
+            e.nz, e.dz = self.settings.NCellsZ, self.settings.dz
+            for d, (rp, ci, v) in enumerate(self.ops3):
+                keep += [rp, ci, v]
+                e.op_rowptr[d] = _lib.as_ip(rp)
+                e.op_col[d] = _lib.as_ip(ci)
+                e.op_val[d] = _lib.as_dp(v)
+            h = C.c_void_p()
+            _lib.check(lib.titus_create_3d(C.byref(p), C.byref(e), C.byref(h)), "titus_create_3d")
+            self._handle = h
+        return self._handle
+
+
 def SolveFirstCollisionSource(solver: SolverCSD, max_steps: int = 0):
     """Full-rank P_N first-collision solver (``SolverCSD.jl:465-586``) on the GPU.
 
@@ -387,8 +492,7 @@ def SolveFirstCollisionSource(solver: SolverCSD, max_steps: int = 0):
     _lib.check(lib.titus_pn_full_solve(h, C.byref(opt), _lib.as_dp(u), _lib.as_dp(dose), _lib.as_dp(psi)),
                "titus_pn_full_solve")
     solver.dose = dose
-    s = solver.settings
-    return 0.5 * math.sqrt(solver.gamma[0]) * u, dose, psi.reshape(s.NCellsX, s.NCellsY, solver.q)
+    return 0.5 * math.sqrt(solver.gamma[0]) * u, dose, psi.reshape(solver.psi_shape)
 
 
 def DoseAdjoint(solver: SolverCSD, weight=None, target=None, dj_ddose=None, checkpoint_every: int = 0,
