@@ -68,7 +68,20 @@ WORKLOADS = {
     # the 3D proton problem (96^3 cells at 1 mm, seeded spheres, P13) with the full-rank solver
     "pn3d": dict(name="csd_proton3d_96cube_P13_full_rank", Nx=97, r=40, nPN=13, problem="csdProton3D",
                  method="pn3d"),
+    # the same 3D problem with the rank-adaptive BUG integrator (rank cap 40)
+    "bug3d": dict(name="csd_proton3d_96cube_P13_cap40_bug", Nx=97, r=40, nPN=13, problem="csdProton3D",
+                  method="bug3d"),
 }
+THREE_D = ("pn3d", "bug3d")
+
+
+def three_d_workload(w, size):
+    """`w` with `size` cells per axis (3D workloads; 0 keeps the workload's 96)."""
+    if not size or w["method"] not in THREE_D:
+        return w
+    w = dict(w, Nx=size + 1)
+    w["name"] = w["name"].replace("96cube", f"{size}cube")
+    return w
 BATCHED = dict(name="pencil_beams256_phantom_128x128_P21_cap60_bug", Nx=129, r=60, nPN=21, problem="csdPhantom",
                spots=256, seed=3, emin=2.0, emax=8.0, ymin=0.1, ymax=0.9)
 # the batched plan measured beside the default solve: every spot's first
@@ -163,7 +176,7 @@ class ClockSampler:
 
 # ------------------------------------------------------------ CPU baseline
 def _oracle_setup(w):
-    if w["method"] == "pn3d":
+    if w["method"] in THREE_D:
         from oracle.three_d import Settings3D as OSettings3D
         from oracle.three_d import SolverCSD3D as OSolver3D
 
@@ -233,17 +246,26 @@ def cpu_cost_model(w, ranks, state200=None, head=40, tail=20):
         return per * steps, (f"FP64 oracle, full-rank P_N: {head} energy steps timed, x {steps} steps "
                              f"(constant cost per step)"), None
     if w["method"] == "pn3d":
+        from oracle.csd import CSD
+        from oracle.three_d import Settings3D as OSettings3D
+        from oracle.three_d import SolverCSD3D as OSolver3D
         from oracle.three_d import solve_pn_full_3d
 
-        o = mk()
-        k = 2   # one 96^3 x 196 step of the oracle takes tens of seconds
+        # one oracle step on 96^3 cells takes minutes: time steps on the same problem
+        # at half the resolution and scale by the cell count (the step's cost is
+        # linear in the cells) and the full grid's step count
+        nfull = w["Nx"] - 1
+        nh = max(8, nfull // 2)
+        o = OSolver3D(OSettings3D(nh + 1, nh + 1, nh + 1, w["r"], w["problem"], nPN=w["nPN"]))
+        k = 2
         t0 = time.perf_counter()
         solve_pn_full_3d(o, max_steps=k)
-        per = (time.perf_counter() - t0) / k
-        steps = o.csd.eTrafo.size - 1
-        return per * steps, (f"FP64 oracle, 3D full-rank P_N: {k} energy steps timed, x {steps} steps "
-                             f"(constant cost per step)"), None
-    fn = {"bug": solve_dlr_bug, "parallel": solve_dlr_parallel, "fixed": solve_dlr_fixed}[w["method"]]
+        per = (time.perf_counter() - t0) / k * (nfull / nh) ** 3
+        steps = CSD(OSettings3D(w["Nx"], w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"])).eTrafo.size - 1
+        return per * steps, (f"FP64 oracle, 3D full-rank P_N: {k} energy steps timed on the {nh}^3 grid, "
+                             f"x ({nfull}/{nh})^3 cells, x {steps} steps (cost linear in cells, constant per step)"), None
+    fn = {"bug": solve_dlr_bug, "bug3d": solve_dlr_bug, "parallel": solve_dlr_parallel,
+          "fixed": solve_dlr_fixed}[w["method"]]
     if w["method"] == "fixed":
         o = mk()
         t0 = time.perf_counter()
@@ -253,6 +275,16 @@ def cpu_cost_model(w, ranks, state200=None, head=40, tail=20):
         return per * steps, (f"FP64 oracle, fixed rank: {head} energy steps timed, x {steps} steps "
                              f"(constant cost per step)"), None
     clock = _IterClock()
+    if w["method"] == "bug3d":
+        # one oracle iteration on 96^3 cells takes tens of seconds: the opening
+        # iterations only, their per-rank times carried over the GPU's rank history
+        fn(mk(), max_steps=3, on_iter=clock)
+        total, direct = _cost_of_history(clock.by_rank, ranks)
+        measured = {r: len(v) for r, v in sorted(clock.by_rank.items())}
+        return total, (f"FP64 oracle (BUG, 3D), per-iteration times of iterations 1-3 by rank ({measured}), "
+                       f"summed over the {len(ranks)} iterations of the GPU solve's rank history; "
+                       f"{100 * direct:.1f}% of those at a directly timed rank, the rest take the nearest "
+                       f"timed rank's cost"), None
     fn(mk(), max_steps=head, on_iter=clock)
     if state200 is None:
         state200 = fn(mk(), max_steps=200, return_state=True)
@@ -288,14 +320,19 @@ def run_gpu_solve(args, w, rank, world, local_rank, dist):
     import numpy as np
     import torch
 
-    from titus_b200 import Settings, SolverCSD
+    from titus_b200 import Settings, Settings3D, SolverCSD, SolverCSD3D
     from titus_b200 import _lib
     from titus_b200.replicas import replica_throughput
 
-    method = {"fixed": _lib.TITUS_DLR_FIXED, "bug": _lib.TITUS_BUG_ADAPTIVE,
+    method = {"fixed": _lib.TITUS_DLR_FIXED, "bug": _lib.TITUS_BUG_ADAPTIVE, "bug3d": _lib.TITUS_BUG_ADAPTIVE,
               "parallel": _lib.TITUS_PARALLEL_ADAPTIVE}[w["method"]]
-    s = Settings(w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"])
-    solver = SolverCSD(s, team_ctas=args.team)
+    three_d = w["method"] == "bug3d"
+    if three_d:
+        s = Settings3D(w["Nx"], w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"])
+        solver = SolverCSD3D(s, team_ctas=args.team)
+    else:
+        s = Settings(w["Nx"], w["Nx"], w["r"], w["problem"], nPN=w["nPN"])
+        solver = SolverCSD(s, team_ctas=args.team)
     lib = _lib.load()
     h = solver.handle()
     opt = solver.options()
@@ -338,6 +375,13 @@ def run_gpu_solve(args, w, rank, world, local_rank, dist):
 
     # end to end: one-shot C-ABI call with host buffers (upload, solve, copy-out, free)
     p, keep = solver.problem_struct()
+    ext = None
+    if three_d:
+        ext = _lib.Problem3D()
+        ext.nz, ext.dz = s.NCellsZ, s.dz
+        for d, (rp, ci, v) in enumerate(solver.ops3):
+            keep += [rp, ci, v]
+            ext.op_rowptr[d], ext.op_col[d], ext.op_val[d] = _lib.as_ip(rp), _lib.as_ip(ci), _lib.as_dp(v)
     h2d = sum(a.nbytes for a in keep)
     res2, bufs2 = solver._result(s.r)
     d2h = sum(b.nbytes for b in bufs2.values())
@@ -347,7 +391,16 @@ def run_gpu_solve(args, w, rank, world, local_rank, dist):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        _lib.check(lib.titus_solve_problem(C.byref(p), method, C.byref(opt), C.byref(res2)), "titus_solve_problem")
+        if three_d:
+            # one-shot: titus_create_3d, titus_solve, titus_destroy
+            h2 = C.c_void_p()
+            _lib.check(lib.titus_create_3d(C.byref(p), C.byref(ext), C.byref(h2)), "titus_create_3d")
+            rc = lib.titus_solve(h2, method, C.byref(opt), C.byref(res2))
+            lib.titus_destroy(h2)
+            _lib.check(rc, "titus_solve")
+        else:
+            _lib.check(lib.titus_solve_problem(C.byref(p), method, C.byref(opt), C.byref(res2)),
+                       "titus_solve_problem")
     t_e2e = time.perf_counter() - t0
     e2e_value, t_e2e = replica_throughput(e2e_steps, t_e2e, world, device="cuda")
 
@@ -851,6 +904,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--method", default="bug", choices=sorted(WORKLOADS) + ["batched"])
     ap.add_argument("--team", type=int, default=148, help="CTAs per solve (0 = library default)")
+    ap.add_argument("--size", type=int, default=0, help="cells per axis of the 3D workloads (default 96)")
     ap.add_argument("--team-batched", type=int, default=0, help="CTAs per spot of the batched plan (0 = tuned)")
     ap.add_argument("--impl", default="titus", choices=["titus", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

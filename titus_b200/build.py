@@ -10,7 +10,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("titus_api.cu", "titus_noalloc.cu", "titus_adaptive.cu", "titus_flux.cu", "titus_pn_full.cu", "titus_pn3d.cu", "titus_tc_probe.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("titus_api.cu", "titus_noalloc.cu", "titus_adaptive.cu", "titus_adaptive3d.cu", "titus_flux.cu", "titus_pn_full.cu", "titus_pn3d.cu", "titus_tc_probe.cu")]
 DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "titus.h")]
 TARGET = os.path.join(HERE, "libtitus.so")

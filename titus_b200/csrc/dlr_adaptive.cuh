@@ -21,7 +21,7 @@
 #include "wide_linalg.cuh"
 
 namespace titus {
-namespace wide {
+namespace TITUS_WIDE_NS {
 
 constexpr double kCertW = 1e5;   // ||R||_F ||R^-1||_F bound of the certified Cholesky paths
 constexpr double kNullSvd = 1e-12;
@@ -33,7 +33,8 @@ __device__ __forceinline__ double* sside(const WCtx& x, int s, int off) {
 }
 
 // ------------------------------------------------------------- row kernels ---
-// F[r][fc + d*k + j] = (L_d A)[r0 + r][j]; zero on boundary rows (stencils.jl:26-128).
+// F[r][fc + d*k + j] = (L_d A)[r0 + r][j]; zero on boundary rows (stencils.jl:26-128;
+// 3D problems append L2z, L1z, the same rows with dz and the z neighbours).
 __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0, int nr, int k, double* F, int ldf,
                                  int fc) {
     const DevProblem& P = x.P;
@@ -42,7 +43,7 @@ __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0
     for (int e = threadIdx.x; e < nr * k; e += NT) {
         const int r = e / k, j = e - (e / k) * k;
         const int c = r0 + r;
-        double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
+        double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0, l2z = 0.0, l1z = 0.0;
         if (!is_bnd_w(P, c)) {
             const double* p = A + (size_t)c * lda + j;
             const double a0 = ldcg(p) * __ldg(P.rinv + c);
@@ -54,15 +55,28 @@ __device__ inline void w_stencil(const WCtx& x, const double* A, int lda, int r0
             l2y = (ayp - aym) * hy;
             l1x = a0 * ix - hx * axm - hx * axp;
             l1y = a0 * iy - hy * aym - hy * ayp;
+            if constexpr (kThreeD) {
+                const int nxy = P.nx * P.ny;
+                const double hz = 0.5 / P.dz, iz = 1.0 / P.dz;
+                const double azm = ldcg(p - (size_t)nxy * lda) * __ldg(P.rinv + c - nxy);
+                const double azp = ldcg(p + (size_t)nxy * lda) * __ldg(P.rinv + c + nxy);
+                l2z = (azp - azm) * hz;
+                l1z = a0 * iz - hz * azm - hz * azp;
+            }
         }
         double* row = F + r * ldf + fc;
         row[0 * k + j] = l2x;
         row[1 * k + j] = l2y;
         row[2 * k + j] = l1x;
         row[3 * k + j] = l1y;
+        if constexpr (kThreeD) {
+            row[4 * k + j] = l2z;
+            row[5 * k + j] = l1z;
+        }
     }
 }
-// F[r][fc + d*k + j] = (A_d B)[r0 + r][j] (sparse P_N operators Ax, Az, |Ax|, |Az|).
+// F[r][fc + d*k + j] = (A_d B)[r0 + r][j] (sparse P_N operators Ax, Az, |Ax|, |Az|
+// and, for 3D problems, Ay, |Ay|).
 // A thread takes one (operator, row) and a group of up to SPJ consecutive
 // columns: per nonzero it loads the index and value once and SPJ contiguous
 // entries of B, so the loads of a row segment are independent. The sum over
@@ -71,7 +85,7 @@ __device__ inline void w_spmm(const WCtx& x, const double* B, int ldb, int r0, i
                               int fc) {
     constexpr int SPJ = 8;
     const int ng = (k + SPJ - 1) / SPJ;
-    for (int e = threadIdx.x; e < NOPS * nr * ng; e += NT) {
+    for (int e = threadIdx.x; e < NOPS_W * nr * ng; e += NT) {
         const int d = e / (nr * ng);
         const int rem = e - d * nr * ng;
         const int r = rem / ng, g = rem - (rem / ng) * ng;
@@ -161,28 +175,30 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
     const double dE = P.dE;
     const double den = 1.0 + dE * sigma0;
     const int q = P.q;
-    // the per-ordinate quotients Omega_x / dx, Omega_z / dy, formed once
-    __shared__ double s_cx[QW], s_cz[QW];
+    // the per-ordinate quotients Omega_x / dx, Omega_z / dy (3D: Omega_y / dz), formed once
+    __shared__ double s_cx[QW], s_cz[QW], s_cy[kThreeD ? QW : 1];
     __syncthreads();   // a previous call's readers are done
     for (int l = threadIdx.x; l < q; l += NT) {
         s_cx[l] = P.omega[l * 3 + 0] / P.dx;
         s_cz[l] = P.omega[l * 3 + 2] / P.dy;
+        if constexpr (kThreeD) s_cy[l] = P.omega[l * 3 + 1] / P.dz;
     }
     __syncthreads();
+    const int nxy = P.nx * P.ny;
     // four entries per thread: their upwind neighbours are loaded before any is used
     constexpr int SU = 4;
     const int cnt = (x.c1 - x.c0) * q;
     for (int b = threadIdx.x; b < cnt; b += SU * NT) {
-        double pcv[SU], nxv[SU], nyv[SU];
-        int cv[SU], kv[SU], ncx[SU], ncy[SU];
+        double pcv[SU], nxv[SU], nyv[SU], nzv[SU];
+        int cv[SU], kv[SU], ncx[SU], ncy[SU], ncz[SU];
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
             const int e = b + u * NT;
             const int c = x.c0 + e / q, kq = e - (e / q) * q;
             cv[u] = c;
             kv[u] = kq;
-            pcv[u] = nxv[u] = nyv[u] = 0.0;
-            ncx[u] = ncy[u] = c;
+            pcv[u] = nxv[u] = nyv[u] = nzv[u] = 0.0;
+            ncx[u] = ncy[u] = ncz[u] = c;
             if (e < cnt) {
                 pcv[u] = ldcg(x.psi_in + (size_t)c * QW + kq);
                 if (!is_bnd_w(P, c)) {
@@ -190,6 +206,10 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
                     ncy[u] = P.omega[kq * 3 + 2] >= 0.0 ? c - 1 : c + 1;
                     nxv[u] = ldcg(x.psi_in + (size_t)ncx[u] * QW + kq);
                     nyv[u] = ldcg(x.psi_in + (size_t)ncy[u] * QW + kq);
+                    if constexpr (kThreeD) {
+                        ncz[u] = P.omega[kq * 3 + 1] >= 0.0 ? c - nxy : c + nxy;
+                        nzv[u] = ldcg(x.psi_in + (size_t)ncz[u] * QW + kq);
+                    }
                 }
             }
         }
@@ -209,6 +229,12 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
                 if (oz >= 0.0) ns = f0 - nyv[u] * P.rinv[ncy[u]];
                 else ns = nyv[u] * P.rinv[ncy[u]] - f0;
                 flux = s_cx[kq] * ew + s_cz[kq] * ns;
+                if constexpr (kThreeD) {
+                    double tb;
+                    if (P.omega[kq * 3 + 1] >= 0.0) tb = f0 - nzv[u] * P.rinv[ncz[u]];
+                    else tb = nzv[u] * P.rinv[ncz[u]] - f0;
+                    flux = flux + s_cy[kq] * tb;
+                }
             }
             double out = (pc - dE * flux) / den;
             if (kq == 0 && P.restore[c]) out = pc;
@@ -218,12 +244,12 @@ static __device__ __noinline__ void w_sweep(WCtx& x, double sigma0) {
 }
 
 // ---- streaming Grams of width k over A (cells, stencils) and B (moments, P_N
-// operators): acc[d k^2 ..] = A^T L_d A, acc[(4+d) k^2 ..] = B^T A_d B.
+// operators): acc[d k^2 ..] = A^T L_d A, acc[(NOPS_W+d) k^2 ..] = B^T A_d B.
 // `cw` = width of A and B used; blocks for d in [d0, d1) only (chunking).
 static __device__ __noinline__ void w_grams_pass(WCtx& x, const double* A, const double* B, int cw, int d0, int d1, int off0,
                                     double* acc, double* F, int ldf, int tr) {
     ProfScope ps_(x.prof, PF_ROWS_STREAM);
-    GBlock bl[4];
+    GBlock bl[NOPS_W];
     int nb = 0;
     const int kk = cw * cw;
     for (int d = d0; d < d1; ++d) bl[nb++] = GBlock{0, cw, (d + 1) * cw, cw, (d - d0) * kk};
@@ -257,7 +283,7 @@ static __device__ __noinline__ void w_grams_pass(WCtx& x, const double* A, const
 // out (device status set).
 static __device__ __noinline__ bool w_grams_tc(WCtx& x, const double* A, const double* B, int cw) {
     ProfScope ps_(x.prof, PF_ROWS_STREAM);
-    const umma::GramShape g = umma::gram_shape(4 * cw, cw);
+    const umma::GramShape g = umma::gram_shape(NOPS_W * cw, cw);
     unsigned char* stage = reinterpret_cast<unsigned char*>(x.sm->work);
     double* dst = wpart(x, x.b);
     const int kk = cw * cw;
@@ -266,20 +292,20 @@ static __device__ __noinline__ bool w_grams_tc(WCtx& x, const double* A, const d
     for (int side = 0; side < 2; ++side) {
         const int r0 = side == 0 ? x.c0 : x.m0;
         const int rows = (side == 0 ? x.c1 : x.m1) - r0;
-        double* out = dst + side * 4 * kk;
+        double* out = dst + side * NOPS_W * kk;
         if (rows <= 0) {
-            for (int e = threadIdx.x; e < 4 * kk; e += NT) out[e] = 0.0;
+            for (int e = threadIdx.x; e < NOPS_W * kk; e += NT) out[e] = 0.0;
             __syncthreads();
             continue;
         }
         bool run;
         if (side == 0) {
             const double hx = 0.5 / P.dx, hy = 0.5 / P.dy, ix = 1.0 / P.dx, iy = 1.0 / P.dy;
-            run = umma::gram_run<NT, 4>(x.tc, g, stage, rows, true, [&](int r, int j, double* v) {
+            run = umma::gram_run<NT, NOPS_W>(x.tc, g, stage, rows, true, [&](int r, int j, double* v) {
                 const int c = r0 + r;
                 const double* p = A + (size_t)c * KA + j;
                 v[0] = ldcg(p);
-                double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0;
+                double l2x = 0.0, l2y = 0.0, l1x = 0.0, l1y = 0.0, l2z = 0.0, l1z = 0.0;
                 if (!is_bnd_w(P, c)) {
                     const double a0 = v[0] * __ldg(P.rinv + c);
                     const double axm = ldcg(p - (size_t)P.ny * KA) * __ldg(P.rinv + c - P.ny);
@@ -290,18 +316,30 @@ static __device__ __noinline__ bool w_grams_tc(WCtx& x, const double* A, const d
                     l2y = (ayp - aym) * hy;
                     l1x = a0 * ix - hx * axm - hx * axp;
                     l1y = a0 * iy - hy * aym - hy * ayp;
+                    if constexpr (kThreeD) {
+                        const int nxy = P.nx * P.ny;
+                        const double hz = 0.5 / P.dz, iz = 1.0 / P.dz;
+                        const double azm = ldcg(p - (size_t)nxy * KA) * __ldg(P.rinv + c - nxy);
+                        const double azp = ldcg(p + (size_t)nxy * KA) * __ldg(P.rinv + c + nxy);
+                        l2z = (azp - azm) * hz;
+                        l1z = a0 * iz - hz * azm - hz * azp;
+                    }
                 }
                 v[1] = l2x;
                 v[2] = l2y;
                 v[3] = l1x;
                 v[4] = l1y;
+                if constexpr (kThreeD) {
+                    v[5] = l2z;
+                    v[6] = l1z;
+                }
             });
         } else {
-            run = umma::gram_run<NT, 4>(x.tc, g, stage, rows, true, [&](int r, int j, double* v) {
+            run = umma::gram_run<NT, NOPS_W>(x.tc, g, stage, rows, true, [&](int r, int j, double* v) {
                 const int m = r0 + r;
                 v[0] = ldcg(B + (size_t)m * KA + j);
 #pragma unroll
-                for (int d = 0; d < 4; ++d) {
+                for (int d = 0; d < NOPS_W; ++d) {
                     const Csr& Op = P.op[d];
                     double s = 0.0;
                     const int p1 = __ldg(Op.rowptr + m + 1);
@@ -361,7 +399,7 @@ __device__ inline void w_acc_zero(double* acc, int cnt) {
 }
 
 // Streaming Grams with the rank-r factors (before X[bnd,:] = 0, :1856-1859),
-// published at [G_0..G_3 | C_0..C_3] (r x r each) and reduced; X's boundary
+// published at [G_0..G_{NOPS_W-1} | C_0..C_{NOPS_W-1}] (r x r each) and reduced; X's boundary
 // rows are zeroed between the barriers (:1859).
 static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
     ProfScope ps_(x.prof, PF_ROWS_STREAM);
@@ -370,12 +408,13 @@ static __device__ __noinline__ bool w_stream_grams(WCtx& x) {
         if (!w_grams_tc(x, x.st.X, x.st.W, k)) return false;
     } else {
         double* acc = x.sm->work;
-        double* F = x.sm->work + 8 * k * k;
-        w_acc_zero(acc, 8 * k * k);
-        w_grams_pass(x, x.st.X, x.st.W, k, 0, 4, 0, acc, F, 5 * k, rows_fit(WORKD - 8 * k * k, 5 * k));
-        wpublish_chunk(x, acc, 0, 8 * k * k);
+        double* F = x.sm->work + 2 * NOPS_W * k * k;
+        w_acc_zero(acc, 2 * NOPS_W * k * k);
+        w_grams_pass(x, x.st.X, x.st.W, k, 0, NOPS_W, 0, acc, F, (NOPS_W + 1) * k,
+                     rows_fit(WORKD - 2 * NOPS_W * k * k, (NOPS_W + 1) * k));
+        wpublish_chunk(x, acc, 0, 2 * NOPS_W * k * k);
     }
-    return wreduce(x, 8 * k * k, [&] {
+    return wreduce(x, 2 * NOPS_W * k * k, [&] {
         for (int c = x.c0 + threadIdx.x; c < x.c1; c += NT)
             if (is_bnd_w(x.P, c))
                 for (int j = 0; j < k; ++j) x.st.X[(size_t)c * KA + j] = 0.0;
@@ -388,16 +427,17 @@ static __device__ __noinline__ void w_stream_small(WCtx& x, bool want_sbar) {
     ProfScope ps_(x.prof, PF_SMALL);
     const int k = x.r;
     WSmem* sm = x.sm;
-    double* Gd = sm->work;                 // 4 k x k (ld k), from red
-    double* Cd = sm->work + 4 * RA * RA;   // 4 k x k
-    double* T = sm->work + 8 * RA * RA;    // k x k temp
-    double* U = sm->work + 9 * RA * RA;    // k x k temp
+    double* Gd = sm->work;                      // NOPS_W k x k (ld k), from red
+    double* Cd = sm->work + NOPS_W * RA * RA;   // NOPS_W k x k
+    // k x k temporaries: shared memory in 2D; the 3D Grams leave no room there
+    double* T = kThreeD ? x.scr + SO_TMP : sm->work + 2 * NOPS_W * RA * RA;
+    double* U = kThreeD ? x.scr + SO_TMP + RA * RA : sm->work + (2 * NOPS_W + 1) * RA * RA;
     double* SC = x.scr + SO_SC;
     double* SG = x.scr + SO_SG;
     double* Sb = x.scr + SO_SBAR;
-    load_red(x, 0, 4 * k, k, Gd, k);
-    load_red(x, 4 * k * k, 4 * k, k, Cd, k);
-    for (int d = 0; d < 4; ++d) {
+    load_red(x, 0, NOPS_W * k, k, Gd, k);
+    load_red(x, NOPS_W * k * k, NOPS_W * k, k, Cd, k);
+    for (int d = 0; d < NOPS_W; ++d) {
         const double* G = Gd + d * k * k;
         const double* C = Cd + d * k * k;
         g_mm(SC + d * k * k, k, sm->S, KA, false, C, k, false, k, k, k);         // S C_d
@@ -405,7 +445,7 @@ static __device__ __noinline__ void w_stream_small(WCtx& x, bool want_sbar) {
     }
     if (want_sbar) {
         g_copy(Sb, RA, sm->S, KA, k, k);
-        for (int d = 0; d < 4; ++d) {
+        for (int d = 0; d < NOPS_W; ++d) {
             g_mm(T, k, sm->S, KA, false, Cd + d * k * k, k, false, k, k, k);     // S C_d
             g_mm(U, k, Gd + d * k * k, k, false, T, k, false, k, k, k);          // G_d S C_d
             for (int e = threadIdx.x; e < k * k; e += NT) Sb[(e / k) * RA + e % k] -= x.P.dE * U[e];
@@ -423,15 +463,15 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
     const double dE = x.P.dE;
     WSmem* sm = x.sm;
     double* acc = sm->work;                      // 6 k^2
-    double* ST = sm->work + 6 * k * k;           // 4k x k stacked (SC or SG)
-    double* F = ST + 4 * k * k;                  // tr x 4k stencil / operator outputs
-    const int ldF = 4 * k, ldT = 2 * k;
-    const int tr = rows_fit(WORKD - 10 * k * k, ldF + ldT);
+    double* ST = sm->work + 6 * k * k;           // NOPS_W k x k stacked (SC or SG)
+    double* F = ST + NOPS_W * k * k;             // tr x NOPS_W k stencil / operator outputs
+    const int ldF = NOPS_W * k, ldT = 2 * k;
+    const int tr = rows_fit(WORKD - (6 + NOPS_W) * k * k, ldF + ldT);
     double* T = F + tr * ldF;                    // tr x 2k feature tile [A | B]
     w_acc_zero(acc, 6 * k * k);
     const GBlock bl[3] = {{0, k, 0, k, 0}, {0, k, k, k, k * k}, {k, k, k, k, 2 * k * k}};
     // X side
-    g_copy(ST, k, x.scr + SO_SC, k, 4 * k, k);
+    g_copy(ST, k, x.scr + SO_SC, k, NOPS_W * k, k);
     for (int r0 = x.c0; r0 < x.c1; r0 += tr) {
         const int nr = min(tr, x.c1 - r0);
         wload(T, ldT, 0, x.st.X, KA, 0, r0, nr, k);
@@ -442,7 +482,7 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
         const double* Sm = sm->S;
         row_mm<4>(nr, k, k, T, ldT, [&](int l, int j) { return Sm[l * KA + j]; },
                   [&](int r, int j, double v) { T[r * ldT + k + j] = v; });
-        row_mm<4>(nr, 4 * k, k, F, ldF, [&](int l, int j) { return ST[l * k + j]; },
+        row_mm<4>(nr, NOPS_W * k, k, F, ldF, [&](int l, int j) { return ST[l * k + j]; },
                   [&](int r, int j, double v) { T[r * ldT + k + j] = T[r * ldT + k + j] - dE * v; });
         __syncthreads();
         wstore(x.st.K, RA, 0, T, ldT, k, r0, nr, k);
@@ -450,7 +490,7 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
         __syncthreads();
     }
     // W side
-    g_copy(ST, k, x.scr + SO_SG, k, 4 * k, k);
+    g_copy(ST, k, x.scr + SO_SG, k, NOPS_W * k, k);
     const GBlock bw[3] = {{0, k, 0, k, 3 * k * k}, {0, k, k, k, 4 * k * k}, {k, k, k, k, 5 * k * k}};
     for (int r0 = x.m0; r0 < x.m1; r0 += tr) {
         const int nr = min(tr, x.m1 - r0);
@@ -461,7 +501,7 @@ static __device__ __noinline__ bool w_phase_C(WCtx& x) {
         const double* Sm = sm->S;
         row_mm<4>(nr, k, k, T, ldT, [&](int l, int j) { return Sm[j * KA + l]; },
                   [&](int r, int j, double v) { T[r * ldT + k + j] = v; });
-        row_mm<4>(nr, 4 * k, k, F, ldF, [&](int l, int j) { return ST[l * k + j]; },
+        row_mm<4>(nr, NOPS_W * k, k, F, ldF, [&](int l, int j) { return ST[l * k + j]; },
                   [&](int r, int j, double v) { T[r * ldT + k + j] = T[r * ldT + k + j] - dE * v; });
         __syncthreads();
         wstore(x.st.L, RA, 0, T, ldT, k, r0, nr, k);
@@ -1723,21 +1763,27 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 double* acc = sm->work;
                 const int mm = m * m;
                 // operators per chunk: as many as fit with at least 16 feature rows
-                const int opc = (8 * mm + 16 * 5 * m <= WORKD) ? 4 : ((4 * mm + 16 * 5 * m <= WORKD) ? 2 : 1);
+                int opc;
+                if constexpr (kThreeD) {
+                    const int fr = 16 * (NOPS_W + 1) * m;
+                    opc = (12 * mm + fr <= WORKD) ? 6 : (6 * mm + fr <= WORKD) ? 3 : (4 * mm + fr <= WORKD) ? 2 : 1;
+                } else {
+                    opc = (8 * mm + 16 * 5 * m <= WORKD) ? 4 : ((4 * mm + 16 * 5 * m <= WORKD) ? 2 : 1);
+                }
                 double* F = sm->work + 2 * opc * mm;
                 if (x.mixed && m >= kTcMinWidth) {
                     if (!w_grams_tc(x, x.st.X, x.st.W, m)) { aborted = true; break; }
                 } else {
-                    for (int d = 0; d < 4; d += opc) {
+                    for (int d = 0; d < NOPS_W; d += opc) {
                         w_acc_zero(acc, 2 * opc * mm);
-                        w_grams_pass(x, x.st.X, x.st.W, m, d, d + opc, 0, acc, F, 5 * m,
-                                     rows_fit(WORKD - 2 * opc * mm, 5 * m));
-                        wpublish_chunk(x, acc, d * mm, opc * mm);                   // X side G_d
-                        wpublish_chunk(x, acc + opc * mm, (4 + d) * mm, opc * mm);  // W side C_d
+                        w_grams_pass(x, x.st.X, x.st.W, m, d, d + opc, 0, acc, F, (NOPS_W + 1) * m,
+                                     rows_fit(WORKD - 2 * opc * mm, (NOPS_W + 1) * m));
+                        wpublish_chunk(x, acc, d * mm, opc * mm);                        // X side G_d
+                        wpublish_chunk(x, acc + opc * mm, (NOPS_W + d) * mm, opc * mm);  // W side C_d
                         __syncthreads();
                     }
                 }
-                if (!wreduce(x, 8 * mm)) { aborted = true; break; }
+                if (!wreduce(x, 2 * NOPS_W * mm)) { aborted = true; break; }
                 // Sup = S2 - dE sum_d G_d S2 C_d ; eta from the [k:, k:] block
                 ProfScope ps_sup(x.prof, PF_SMALL);
                 double* Gd = x.scr + SO_TMP;
@@ -1748,9 +1794,9 @@ static __device__ __noinline__ void energy_loop(WCtx& x, int n_begin, int n_end,
                 g_copy(Sup, KA, sm->S, KA, m, m);
                 double* E = sm->work + 2 * KA * KA;    // k x k eta accumulator
                 g_zero(E, RA, k, k);
-                for (int d = 0; d < 4; ++d) {
+                for (int d = 0; d < NOPS_W; ++d) {
                     load_red(x, d * mm, m, m, Gd, KA);
-                    load_red(x, (4 + d) * mm, m, m, Cd, KA);
+                    load_red(x, (NOPS_W + d) * mm, m, m, Cd, KA);
                     g_mm(Tm, KA, sm->S, KA, false, Cd, KA, false, m, m, m);
                     g_mm(Um, KA, Gd, KA, false, Tm, KA, false, m, m, m);
                     for (int e = threadIdx.x; e < m * m; e += NT) {
@@ -2182,5 +2228,5 @@ adaptive_batched_kernel(DevProblem P0, WideState* states, int G, int T, const Sp
     tc_teardown(x);
 }
 
-}  // namespace wide
+}  // namespace TITUS_WIDE_NS
 }  // namespace titus

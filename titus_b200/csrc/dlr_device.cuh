@@ -47,7 +47,7 @@ struct DevProblem {
     const double* omega;      // q x 3
     const double* mred;       // N x q
     const int32_t* lof;       // N: Legendre order l of moment m
-    Csr op[NOPS];
+    Csr op[6];                // Ax, Az, |Ax|, |Az|; 3D problems also Ay, |Ay| (z streaming)
     const int32_t* xcomp; int nxcomp;
     const int32_t* wcomp; int nwcomp;
     const uint8_t* restore;   // n: 1 if ordinate-0 value is restored after the sweep
@@ -56,6 +56,8 @@ struct DevProblem {
     long long spin_limit;     // polls before a team barrier gives up (0 = default, about a second)
     int fault_barrier;        // test hook: CTA 1 does not arrive at this barrier generation (<= 0: off)
     int precision;            // 0: FP64; 1: MIXED (tensor-core operator Grams, adaptive integrators)
+    int nz;                   // 3D problems: z layers (cell (i, j, k) at row (k nx + i) ny + j); 0 in 2D
+    double dz;                // 3D problems: z spacing
 };
 
 // Phase-timer categories (titus_profile reports them in this order).

@@ -13,8 +13,13 @@
 #include "titus_handle.h"
 #include "dlr_adaptive.cuh"
 
+// Host entry names: the 3D compilation (titus_adaptive3d.cu) appends _3d.
+#ifndef TITUS_WIDE_HOST
+#define TITUS_WIDE_HOST(name) name
+#endif
+
 using namespace titus;
-using namespace titus::wide;
+using namespace titus::TITUS_WIDE_NS;
 using titus_host::fail;
 
 namespace {
@@ -41,12 +46,14 @@ int ensure_state(titus_solver* s) {
         return rc;
     if ((rc = s->walloc(&s->d_wst, 1))) return rc;
     CK(cudaMemcpy(s->d_wst, &w, sizeof(WideState), cudaMemcpyHostToDevice));
-    CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sizeof(WSmem)));
     CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_BUG_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sizeof(WSmem)));
-    CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_REJECTION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sizeof(WSmem)));
+    if constexpr (!kThreeD) {   // 3D problems run the BUG integrator only
+        CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(WSmem)));
+        CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_REJECTION>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WSmem)));
+    }
     return TITUS_OK;
 }
 
@@ -57,7 +64,8 @@ __global__ void wide_init_kernel(WideState* states, int n, int N, int nx, int ny
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < r0; j += gridDim.x * blockDim.x) {
         if (j < n) {
             const int i = j / ny, jj = j % ny;
-            const bool bnd = (i == 0 || jj == 0 || i == nx - 1 || jj == ny - 1);
+            // 3D: the first r0 < nx ny rows lie in the z = 0 face
+            const bool bnd = kThreeD || (i == 0 || jj == 0 || i == nx - 1 || jj == ny - 1);
             st.X[(size_t)j * KA + j] = bnd ? 0.0 : 1.0;
         }
         if (j < N) st.W[(size_t)j * KA + j] = 1.0;
@@ -106,12 +114,13 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : std::min(s->num_sms, 64);
     G = std::max(1, std::min(G, s->num_sms));
     int per_sm = 0;
-    void (*kfun)(DevProblem, WideState*, int, int, int, int) =
-        method == TITUS_PARALLEL_ADAPTIVE    ? adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>
-        : method == TITUS_PARALLEL_REJECTION ? adaptive_kernel<TITUS_PARALLEL_REJECTION>
-                                             : adaptive_kernel<TITUS_BUG_ADAPTIVE>;
+    void (*kfun)(DevProblem, WideState*, int, int, int, int) = adaptive_kernel<TITUS_BUG_ADAPTIVE>;
+    if constexpr (!kThreeD) {
+        if (method == TITUS_PARALLEL_ADAPTIVE) kfun = adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>;
+        if (method == TITUS_PARALLEL_REJECTION) kfun = adaptive_kernel<TITUS_PARALLEL_REJECTION>;
+    }
     auto kern = (void*)kfun;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, wide::NT, sizeof(WSmem)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, TITUS_WIDE_NS::NT, sizeof(WSmem)));
     if (per_sm < 1) return fail(TITUS_ERR_CUDA, "adaptive kernel does not fit on an SM (smem %zu)", sizeof(WSmem));
     G = std::min(G, per_sm * s->num_sms);
     DevProblem P = s->P;
@@ -130,7 +139,7 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     CK(cudaMemsetAsync(w.diag, 0, 16 * sizeof(double), stream));
     WideState* dst = s->d_wst;
     void* args[] = {&P, &dst, &G, &n_begin, &n_end, &max_iters};
-    CK(cudaLaunchCooperativeKernel(kern, dim3(G), dim3(wide::NT), args, sizeof(WSmem), stream));
+    CK(cudaLaunchCooperativeKernel(kern, dim3(G), dim3(TITUS_WIDE_NS::NT), args, sizeof(WSmem), stream));
     s->last_G = G;
     s->wide_state_valid = 1;
     return TITUS_OK;
@@ -194,7 +203,7 @@ int check_status(titus_solver* s) {
 
 }  // namespace
 
-int titus_host::wide_solve_device(titus_solver* s, int method, const titus_options_t* opt, cudaStream_t stream) {
+int titus_host::TITUS_WIDE_HOST(wide_solve_device)(titus_solver* s, int method, const titus_options_t* opt, cudaStream_t stream) {
     int rc = ensure_state(s);
     if (rc) return rc;
     const int r0 = s->r / 2;
@@ -211,7 +220,7 @@ int titus_host::wide_solve_device(titus_solver* s, int method, const titus_optio
     return launch(s, method, opt, 2, n_end, max_iters, stream);
 }
 
-int titus_host::wide_solve_from(titus_solver* s, int method, const titus_options_t* opt, int n_stop) {
+int titus_host::TITUS_WIDE_HOST(wide_solve_from)(titus_solver* s, int method, const titus_options_t* opt, int n_stop) {
     if (!s->d_wst || !s->wide_state_valid) return fail(TITUS_ERR_ARG, "no adaptive state to resume (call titus_set_state)");
     int info[8];
     CK(cudaMemcpy(info, s->wst.info, sizeof(info), cudaMemcpyDeviceToHost));
@@ -226,7 +235,7 @@ int titus_host::wide_solve_from(titus_solver* s, int method, const titus_options
     return launch(s, method, opt, n_begin, n_end, max_iters, nullptr);
 }
 
-int titus_host::wide_fetch(titus_solver* s, titus_result_t* res) {
+int titus_host::TITUS_WIDE_HOST(wide_fetch)(titus_solver* s, titus_result_t* res) {
     int rc = check_status(s);
     if (rc) return rc;
     WideState& w = s->wst;
@@ -261,7 +270,7 @@ int titus_host::wide_fetch(titus_solver* s, titus_result_t* res) {
     return TITUS_OK;
 }
 
-int titus_host::wide_set_state(titus_solver* s, int rank, const double* X, const double* S, const double* W,
+int titus_host::TITUS_WIDE_HOST(wide_set_state)(titus_solver* s, int rank, const double* X, const double* S, const double* W,
                                const double* psi, const double* dose, int n_next) {
     int rc = ensure_state(s);
     if (rc) return rc;
@@ -290,6 +299,7 @@ int titus_host::wide_set_state(titus_solver* s, int rank, const double* X, const
 }
 
 
+#if TITUS_WIDE_NOPS == 4   // batched pencil beams: 2D problems
 namespace {
 
 struct DevTemps {
@@ -452,7 +462,7 @@ int titus_host::batch_launch(titus_batch* b, int method, const titus_options_t* 
     auto kfun = method == TITUS_PARALLEL_ADAPTIVE ? adaptive_batched_kernel<TITUS_PARALLEL_ADAPTIVE>
                                                   : adaptive_batched_kernel<TITUS_BUG_ADAPTIVE>;
     CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WSmem)));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, wide::NT, sizeof(WSmem)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, TITUS_WIDE_NS::NT, sizeof(WSmem)));
     if (per_sm < 1) return fail(TITUS_ERR_CUDA, "batched kernel does not fit on an SM");
     const int T = std::max(1, std::min(b->nspots, per_sm * s->num_sms / G));
     int rc = ensure_batch_states(s, T, G);
@@ -481,7 +491,7 @@ int titus_host::batch_launch(titus_batch* b, int method, const titus_options_t* 
     int* queue = b->d_queue;
     const int* order = b->d_order;
     void* args[] = {&P, &dst, &Gl, &Tl, &d_sd, &ns, &r0l, &max_iters, &msl, &queue, &order};
-    CK(cudaLaunchCooperativeKernel((void*)kfun, dim3(T * G), dim3(wide::NT), args, sizeof(WSmem), stream));
+    CK(cudaLaunchCooperativeKernel((void*)kfun, dim3(T * G), dim3(TITUS_WIDE_NS::NT), args, sizeof(WSmem), stream));
     b->last_T = T;
     b->last_G = G;
     b->launched = true;
@@ -536,8 +546,9 @@ int titus_host::wide_solve_batched(titus_solver* s, int method, const titus_opti
     batch_free(b);
     return rc;
 }
+#endif
 
-void titus_host::wide_free(titus_solver* s) {
+void titus_host::TITUS_WIDE_HOST(wide_free)(titus_solver* s) {
     for (void* p : s->wide_allocs) cudaFree(p);
     s->wide_allocs.clear();
     s->d_wst = nullptr;

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "titus_handle.h"
+#include "wide_common.cuh"
 #include "dlr_fixed.cuh"
 
 using namespace titus;
@@ -299,14 +300,21 @@ extern "C" int titus_create_3d(const titus_problem_t* pb, const titus_problem_3d
     }
     s->nz = ext->nz;
     s->dz = ext->dz;
+    s->P.nz = ext->nz;
+    s->P.dz = ext->dz;
+    s->P.op[4] = s->op3[0];
+    s->P.op[5] = s->op3[1];
     *out = s;
     return TITUS_OK;
 }
 
-// The DLR integrators, their batched and resumed forms run the reference's 2D
-// problems; a 3D handle (titus_create_3d) runs the full-rank P_N solver.
-static int reject_3d(const titus_solver* s, const char* what) {
-    return s->nz ? fail(TITUS_ERR_ARG, "%s: 3D problems run with titus_pn_full_solve", what) : TITUS_OK;
+// A 3D handle (titus_create_3d) runs the full-rank P_N solver and the BUG
+// integrator (plain and resumed); the other DLR integrators and the batched
+// form run the reference's 2D problems.
+static int reject_3d(const titus_solver* s, const char* what, int method = -1) {
+    if (!s->nz || method == TITUS_BUG_ADAPTIVE) return TITUS_OK;
+    return fail(TITUS_ERR_ARG, "%s: 3D problems run with titus_pn_full_solve or the BUG integrator (method %d)", what,
+                TITUS_BUG_ADAPTIVE);
 }
 
 // Initial factors of SolverCSD.jl:931-955: X = first r identity columns with
@@ -430,11 +438,14 @@ static int check_precision(int method, const titus_options_t* opt) {
 
 extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus_options_t* opt, void* stream_) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
-    if (int rc = reject_3d(s, "titus_solve")) return rc;
+    if (int rc = reject_3d(s, "titus_solve", method)) return rc;
     if (int rc = check_precision(method, opt)) return rc;
+    if (s->nz && opt && opt->precision != TITUS_PRECISION_FP64)
+        return fail(TITUS_ERR_ARG, "3D problems run in FP64 (precision %d)", opt->precision);
     cudaStream_t stream = (cudaStream_t)stream_;
     if (is_wide_family(method)) {
         s->last_method = method;
+        if (s->nz) return titus_host::wide_solve_device_3d(s, method, opt, stream);
         return titus_host::wide_solve_device(s, method, opt, stream);
     }
     if (!is_fixed_family(method)) return fail(TITUS_ERR_ARG, "unknown method %d", method);
@@ -446,7 +457,8 @@ extern "C" int titus_solve_device(titus_solver_t* s, int32_t method, const titus
 extern "C" int titus_fetch(titus_solver_t* s, titus_result_t* res) {
     if (!s || !res) return fail(TITUS_ERR_ARG, "NULL argument");
     if (is_wide_family(s->last_method))
-        return titus_host::wide_fetch(s, res);
+        return s->nz ? titus_host::wide_fetch_3d(s, res) : titus_host::wide_fetch(s, res);
+    if (s->nz) return fail(TITUS_ERR_ARG, "titus_fetch: no DLR solve has run on this 3D handle");
     int rc = check_status(s);
     if (rc) return rc;
     int info[4];
@@ -497,9 +509,9 @@ extern "C" int titus_solve_problem(const titus_problem_t* pb, int32_t method, co
 extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X, const double* S, const double* W,
                                const double* psi, const double* dose, int32_t n_next) {
     if (!s || !X || !S || !W || !psi || !dose) return fail(TITUS_ERR_ARG, "NULL argument");
-    if (int rc = reject_3d(s, "titus_set_state")) return rc;
     if (rank < 1 || rank > wide::RA) return fail(TITUS_ERR_LIMIT, "rank %d outside [1, %d]", rank, wide::RA);
     if (n_next < 2 || n_next > s->nE + 1) return fail(TITUS_ERR_ARG, "n_next %d outside [2, nE+1]", n_next);
+    if (s->nz) return titus_host::wide_set_state_3d(s, rank, X, S, W, psi, dose, n_next);
     // the adaptive integrators' state always; the fixed-rank state when the rank fits
     int rcw = titus_host::wide_set_state(s, rank, X, S, W, psi, dose, n_next);
     if (rcw) return rcw;
@@ -527,10 +539,14 @@ extern "C" int titus_set_state(titus_solver_t* s, int32_t rank, const double* X,
 extern "C" int titus_solve_from(titus_solver_t* s, int32_t method, const titus_options_t* opt, int32_t n_stop,
                                 titus_result_t* res) {
     if (!s) return fail(TITUS_ERR_ARG, "solver is NULL");
-    if (int rc = reject_3d(s, "titus_solve_from")) return rc;
+    if (int rc = reject_3d(s, "titus_solve_from", method)) return rc;
     if (int rc = check_precision(method, opt)) return rc;
     if (is_wide_family(method)) {
         s->last_method = method;
+        if (s->nz) {
+            int rc = titus_host::wide_solve_from_3d(s, method, opt, n_stop);
+            return rc ? rc : titus_host::wide_fetch_3d(s, res);
+        }
         int rc = titus_host::wide_solve_from(s, method, opt, n_stop);
         if (rc) return rc;
         return titus_host::wide_fetch(s, res);

@@ -5,7 +5,8 @@
 #include <vector>
 
 #include "../../include/titus.h"
-#include "wide_common.cuh"
+#include "dlr_device.cuh"
+#include "wide_state.h"
 
 struct titus_solver;
 struct titus_batch;
@@ -46,6 +47,13 @@ int wide_fetch(titus_solver* s, titus_result_t* res);
 int wide_set_state(titus_solver* s, int rank, const double* X, const double* S, const double* W, const double* psi,
                    const double* dose, int n_next);
 void wide_free(titus_solver* s);
+// the BUG integrator on 3D problems (titus_adaptive3d.cu: the same source with six streaming pairs)
+int wide_solve_device_3d(titus_solver* s, int method, const titus_options_t* opt, cudaStream_t stream);
+int wide_solve_from_3d(titus_solver* s, int method, const titus_options_t* opt, int n_stop);
+int wide_fetch_3d(titus_solver* s, titus_result_t* res);
+int wide_set_state_3d(titus_solver* s, int rank, const double* X, const double* S, const double* W,
+                      const double* psi, const double* dose, int n_next);
+void wide_free_3d(titus_solver* s);
 int batch_upload(titus_solver* s, int nspots, const titus_spot_t* spots, titus_batch** out);
 int batch_launch(titus_batch* b, int method, const titus_options_t* opt, cudaStream_t stream);
 int batch_fetch(titus_batch* b, double* dose_out, int32_t* rank_out, int32_t* iters_out);
@@ -77,12 +85,12 @@ struct titus_solver {
     unsigned long long* prof = nullptr;
     int clock_khz = 0;
     // rank-adaptive state (allocated on first use)
-    titus::wide::WideState wst{};
-    titus::wide::WideState* d_wst = nullptr;
+    titus::WideState wst{};
+    titus::WideState* d_wst = nullptr;
     std::vector<void*> wide_allocs;
     // batched teams (allocated on first batched solve, grown on demand)
-    std::vector<titus::wide::WideState> bst;
-    titus::wide::WideState* d_bst = nullptr;
+    std::vector<titus::WideState> bst;
+    titus::WideState* d_bst = nullptr;
     int b_teams = 0, b_G = 0;
     std::vector<void*> batch_allocs;
     int wide_state_valid = 0;   // 1 after an adaptive solve or titus_set_state

@@ -12,22 +12,39 @@
 #pragma once
 #include "dlr_device.cuh"
 #include "umma.cuh"
+#include "wide_state.h"
+
+// The rank-adaptive kernels are compiled twice: for the reference's 2D
+// problems (four streaming pairs, namespace titus::wide) and for 3D problems
+// (six pairs, the z pair appended; namespace titus::wide3, titus_adaptive3d.cu).
+#ifndef TITUS_WIDE_NOPS
+#define TITUS_WIDE_NOPS 4
+#endif
+#ifndef TITUS_WIDE_NS
+#define TITUS_WIDE_NS wide
+#endif
 
 namespace titus {
-namespace wide {
+namespace TITUS_WIDE_NS {
+
+// streaming pairs (stencil L_d, P_N matrix A_d): (L2x, Ax), (L2y, Az), (L1x, |Ax|),
+// (L1y, |Az|) and, for 3D problems, (L2z, Ay), (L1z, |Ay|)
+constexpr int NOPS_W = TITUS_WIDE_NOPS;
+constexpr bool kThreeD = NOPS_W == 6;
+static_assert(NOPS_W == 4 || NOPS_W == 6, "four (2D) or six (3D) streaming pairs");
 
 constexpr int NT = titus::NT;   // threads per CTA
-constexpr int RA = 40;          // max rank entering a step
+constexpr int RA = titus::WIDE_RA;   // max rank entering a step
 constexpr int KA = 2 * RA;      // max augmented width
 constexpr int LDS = KA + 1;     // row stride of the truncation SVD's column arrays (odd: no bank conflicts)
 constexpr int QW = titus::QM;   // psi leading dimension (reduced ordinates <= QW)
 constexpr int TRW = 8;          // rows per staged tile (minimum layout)
 constexpr int TRMAX = 512;      // rows per staged tile when the phase's free shared memory allows
-constexpr int PMAXW = 8 * KA * KA;   // largest reduction (BUG S-step Grams): 51200 doubles
+constexpr int PMAXW = 2 * NOPS_W * KA * KA;   // largest reduction (BUG S-step Grams): 51200 doubles in 2D
 constexpr int WORKD = 20480;    // shared work area (doubles)
 constexpr int ACCW = 16384;     // accumulator chunk (doubles), inside the work area
 constexpr int FLD = 10 * RA;    // feature-tile leading dimension (doubles)
-constexpr int SCRW = 81920;     // per-CTA scratch (doubles, global)
+constexpr int SCRW = kThreeD ? 90112 : 81920;   // per-CTA scratch (doubles, global)
 constexpr int WCS = 3 * RA;     // row stride of the W-side completion coefficients
 
 // extra device status codes (titus::ST_* holds 1..4)
@@ -36,41 +53,13 @@ constexpr int ST_UNSUPPORTED = 6;  // angular basis lost orthonormality (cannot 
 constexpr int ST_SVD = 7;          // Jacobi SVD did not converge
 constexpr int ST_REF_SHAPE = 8;    // the reference's next step raises DimensionMismatch (parallel-rejection loop)
 
-struct WideState {
-    double* X;      // n x KA
-    double* W;      // N x KA
-    double* K;      // n x RA
-    double* KP;     // n x RA  projected K
-    double* CX;     // n x RA  range-finder C (X side)
-    double* L;      // N x RA
-    double* LP;     // N x RA
-    double* CW;     // N x RA
-    double* psi0;   // n x QW
-    double* psi1;
-    double* dose;   // n
-    double* S;      // KA x KA (state S, written back at exit)
-    double* part;   // 2 x G x PMAXW
-    double* red;    // 2 x PMAXW (double-buffered with the partials)
-    double* scr;    // G x SCRW per-CTA scratch
-    unsigned* bar;  // G + 1 barrier flags
-    int* status;
-    int* info;      // [0] rank, [1] iterations, [2] psi index, [3] next n, [4] eta count
-    double* diag;   // 16
-    double* tvar;   // [0] pseudo-time t (BUG / parallel)
-    int* rank_hist; // hist_cap
-    double* time_hist;
-    double* eta_hist;
-    double* bound_hist;
-    double* X0;     // n x RA: X entering the energy, boundary rows zeroed (parallel-rejection loop)
-    double* W0;     // N x RA: W entering the energy (parallel-rejection loop)
-    int hist_cap;
-};
+using WideState = titus::WideState;
 
 // Per-CTA scratch layout (offsets in doubles). r x r matrices use ld RA.
 enum : int {
-    SO_SC = 0,                       // 4 stacked S C_d        (4 RA x RA)
-    SO_SG = SO_SC + 4 * RA * RA,     // 4 stacked S^T G_d^T    (4 RA x RA)
-    SO_SBAR = SO_SG + 4 * RA * RA,   // S after the streaming / in-scattering S update (RA x RA)
+    SO_SC = 0,                            // stacked S C_d          (NOPS_W RA x RA)
+    SO_SG = SO_SC + NOPS_W * RA * RA,     // stacked S^T G_d^T      (NOPS_W RA x RA)
+    SO_SBAR = SO_SG + NOPS_W * RA * RA,   // S after the streaming / in-scattering S update (RA x RA)
     SO_SIDE = SO_SBAR + RA * RA,     // per-side blocks, SIDE_STRIDE each
 };
 // per-side block offsets (relative to SO_SIDE + side * SIDE_STRIDE)
@@ -148,8 +137,16 @@ __device__ __forceinline__ int rows_fit(int avail, int per_row) {
 }
 
 __device__ __forceinline__ bool is_bnd_w(const DevProblem& P, int c) {
-    int i = c / P.ny, j = c - (c / P.ny) * P.ny;
-    return i == 0 || j == 0 || i == P.nx - 1 || j == P.ny - 1;
+    if constexpr (kThreeD) {
+        // 3D: cell (i, j, k) at row (k nx + i) ny + j; boundary on any of the six faces
+        const int nxy = P.nx * P.ny;
+        const int k = c / nxy, rr = c - k * nxy;
+        const int i = rr / P.ny, j = rr - i * P.ny;
+        return k == 0 || k == P.nz - 1 || i == 0 || j == 0 || i == P.nx - 1 || j == P.ny - 1;
+    } else {
+        int i = c / P.ny, j = c - (c / P.ny) * P.ny;
+        return i == 0 || j == 0 || i == P.nx - 1 || j == P.ny - 1;
+    }
 }
 
 __device__ __forceinline__ bool wsync(WCtx& x) {
@@ -422,5 +419,5 @@ __device__ inline void gram_blocks(double* acc, const double* F, int ldf, int nr
     }
 }
 
-}  // namespace wide
+}  // namespace TITUS_WIDE_NS
 }  // namespace titus

@@ -9,7 +9,7 @@
 #include "wide_common.cuh"
 
 namespace titus {
-namespace wide {
+namespace TITUS_WIDE_NS {
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -486,5 +486,5 @@ static __device__ __noinline__ int w_svd_complete(double* At, double* Vt, int ld
     return rho;
 }
 
-}  // namespace wide
+}  // namespace TITUS_WIDE_NS
 }  // namespace titus

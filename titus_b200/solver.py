@@ -323,8 +323,7 @@ class SolverCSD:
         U, sig, Vt = np.linalg.svd(out["S"])
         V = Vt.T
         X, W = out["X"], out["W"]
-        nx, ny = self.settings.NCellsX, self.settings.NCellsY
-        psi = out["psi"].reshape(nx, ny, self.q)
+        psi = out["psi"].reshape(self.psi_shape)
         return X @ U, 0.5 * math.sqrt(self.gamma[0]) * sig, self.O @ (W @ V), W @ V, out["dose"], psi
 
 
@@ -388,7 +387,9 @@ class SolverCSD3D(SolverCSD):
     exp(-sigmaZInv (z - z0)^2), applied on every face cell. The sweep's
     boundary-slab quirk (``SolverCSD.jl:1002,1005``) is applied in every z
     layer. A 3D handle runs the full-rank P_N solver
-    (``SolveFirstCollisionSource``).
+    (``SolveFirstCollisionSource``) and the rank-adaptive BUG integrator
+    (``SolveFirstCollisionSourceDLRBUGRejection``, plain and resumed with
+    ``run_from``); the other DLR integrators raise.
     """
 
     def __init__(self, settings, team_ctas: int = 0, precision: int = _lib.TITUS_PRECISION_FP64):
