@@ -916,7 +916,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    w = WORKLOADS.get(args.method, WORKLOADS["bug"])
+    w = three_d_workload(WORKLOADS.get(args.method, WORKLOADS["bug"]), args.size)
     if args.dry_run:
         run_dry(args, rank, world)
     elif args.impl == "reference":

@@ -62,14 +62,15 @@ def test_repeat_is_bitwise_identical():
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
-def test_dlr_entry_points_reject_3d():
+def test_other_entry_points_reject_3d():
     s, _ = _pair(8, 3, 1.0, 0.15, 0.1)
     sv = SolverCSD3D(s)
     lib = _lib.load()
     h = sv.handle()
     opt = sv.options(5)
     res = _lib.Result()
-    assert lib.titus_solve(h, _lib.TITUS_BUG_ADAPTIVE, C.byref(opt), C.byref(res)) == _lib.TITUS_ERR_ARG
+    # the 3D build offers the BUG integrator and the full-rank sweep; the others raise
+    assert lib.titus_solve(h, _lib.TITUS_PARALLEL_ADAPTIVE, C.byref(opt), C.byref(res)) == _lib.TITUS_ERR_ARG
     assert "3D" in _lib.last_error()
     z = np.zeros(sv.n)
     assert lib.titus_dose_adjoint(h, 0, C.byref(opt), _lib.as_dp(z), _lib.as_dp(z), None, 0, None, None, None,

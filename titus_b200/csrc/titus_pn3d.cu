@@ -36,6 +36,7 @@ namespace {
 
 constexpr int P3_NT = 256;
 constexpr int P3_NOP = 6;
+constexpr int P3_CBM = 8;   // most cells per CTA of pn3_stream_kernel
 constexpr size_t P3_SMEM_MAX = 100 * 1024;   // stencil images per CTA (two CTAs per SM)
 
 struct Pn3Args {
@@ -126,35 +127,52 @@ __global__ void __launch_bounds__(P3_NT) pn3_stream_kernel(Pn3Args a, int n, con
     __syncthreads();
     const double dE = a.dE;
     const double* sg = a.sigma + (size_t)(n - 1) * (a.npn + 1);
-    for (int e = threadIdx.x; e < nc * N; e += blockDim.x) {
-        const int cl = e / N, m = e - (e / N) * N;
-        const int c = c0 + cl;
-        const size_t ix = (size_t)c * N + m;
-        if (p3_bnd(a, c)) {
-            u_out[ix] = 0.0;
-            continue;
-        }
-        double ut = u[ix];
+    // a thread owns moment m for all of the CTA's cells: each nonzero of row m
+    // of A_d^T is loaded once and applied to the cb cells' images (independent
+    // FMAs), as in the moment-product kernel of the 2D solver
+    for (int m = threadIdx.x; m < N; m += blockDim.x) {
+        double ut[P3_CBM];
+#pragma unroll
+        for (int cl = 0; cl < P3_CBM; ++cl) ut[cl] = cl < nc ? u[(size_t)(c0 + cl) * N + m] : 0.0;
 #pragma unroll
         for (int d = 0; d < P3_NOP; ++d) {
-            const double* im = img + ((size_t)d * cb + cl) * N;
+            const double* im = img + (size_t)d * cb * N;
+            double sd[P3_CBM];
+#pragma unroll
+            for (int cl = 0; cl < P3_CBM; ++cl) sd[cl] = 0.0;
             const int q1 = __ldg(a.tp[d] + m + 1);
-            double s = 0.0;
-            for (int qq = __ldg(a.tp[d] + m); qq < q1; ++qq) s = fma(__ldg(a.tv[d] + qq), im[__ldg(a.ti[d] + qq)], s);
-            ut = ut - dE * s;
+            for (int qq = __ldg(a.tp[d] + m); qq < q1; ++qq) {
+                const double v = __ldg(a.tv[d] + qq);
+                const double* col = im + __ldg(a.ti[d] + qq);
+#pragma unroll
+                for (int cl = 0; cl < P3_CBM; ++cl)
+                    if (cl < cb) sd[cl] = fma(v, col[(size_t)cl * N], sd[cl]);
+            }
+#pragma unroll
+            for (int cl = 0; cl < P3_CBM; ++cl) ut[cl] = ut[cl] - dE * sd[cl];
         }
         const double dv = sg[a.lof[m]];
         const double D = sg[0] - dv;
-        const double* pr = psi + (size_t)c * QM;
-        double src = 0.0;
-        for (int k = 0; k < a.q; ++k) src = fma(a.mred[(size_t)m * a.q + k], pr[k], src);
-        const double un = (ut + dE * dv * src) / (1.0 + dE * D);
-        u_out[ix] = un;
-        if (m == 0) {
-            double unc = 0.0;
-            for (int k = 0; k < a.q; ++k) unc = fma(pr[k], a.mred[k], unc);
-            const double half = (n == 2 || n == a.nE) ? 2.0 : 1.0;
-            dose[c] += dE * (un + unc) * a.smid[n - 2] * a.rinv[c] / half;
+#pragma unroll
+        for (int cl = 0; cl < P3_CBM; ++cl) {
+            if (cl >= nc) continue;
+            const int c = c0 + cl;
+            const size_t ix = (size_t)c * N + m;
+            if (p3_bnd(a, c)) {
+                u_out[ix] = 0.0;
+                continue;
+            }
+            const double* pr = psi + (size_t)c * QM;
+            double src = 0.0;
+            for (int k = 0; k < a.q; ++k) src = fma(a.mred[(size_t)m * a.q + k], pr[k], src);
+            const double un = (ut[cl] + dE * dv * src) / (1.0 + dE * D);
+            u_out[ix] = un;
+            if (m == 0) {
+                double unc = 0.0;
+                for (int k = 0; k < a.q; ++k) unc = fma(pr[k], a.mred[k], unc);
+                const double half = (n == 2 || n == a.nE) ? 2.0 : 1.0;
+                dose[c] += dE * (un + unc) * a.smid[n - 2] * a.rinv[c] / half;
+            }
         }
     }
 }
@@ -238,8 +256,8 @@ int pn3_ensure(titus_solver* s) {
             delete st;
             return rc;
         }
-    // cells per CTA: as many (up to 8) as keep the six stencil images within the budget
-    st->cb = 8;
+    // cells per CTA: as many (up to P3_CBM) as keep the six stencil images within the budget
+    st->cb = P3_CBM;
     while (st->cb > 1 && (size_t)P3_NOP * st->cb * s->N * sizeof(double) > P3_SMEM_MAX) st->cb /= 2;
     st->smem = (size_t)P3_NOP * st->cb * s->N * sizeof(double);
     if (st->smem > 200 * 1024) {
