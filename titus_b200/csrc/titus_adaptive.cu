@@ -24,6 +24,21 @@ using titus_host::fail;
 
 namespace {
 
+using KernelFn = void (*)(DevProblem, WideState*, int, int, int, int);
+
+// The energy-loop kernel of `method`. A template, so that the 3D build (BUG
+// only) never instantiates the other integrators' kernels.
+template <bool ThreeD>
+KernelFn kernel_for(int method) {
+    if constexpr (ThreeD) {
+        return adaptive_kernel<TITUS_BUG_ADAPTIVE>;
+    } else {
+        if (method == TITUS_PARALLEL_ADAPTIVE) return adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>;
+        if (method == TITUS_PARALLEL_REJECTION) return adaptive_kernel<TITUS_PARALLEL_REJECTION>;
+        return adaptive_kernel<TITUS_BUG_ADAPTIVE>;
+    }
+}
+
 int ensure_state(titus_solver* s) {
     if (s->d_wst) return TITUS_OK;
     WideState& w = s->wst;
@@ -46,14 +61,9 @@ int ensure_state(titus_solver* s) {
         return rc;
     if ((rc = s->walloc(&s->d_wst, 1))) return rc;
     CK(cudaMemcpy(s->d_wst, &w, sizeof(WideState), cudaMemcpyHostToDevice));
-    CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_BUG_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sizeof(WSmem)));
-    if constexpr (!kThreeD) {   // 3D problems run the BUG integrator only
-        CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    for (int method : {TITUS_PARALLEL_ADAPTIVE, TITUS_BUG_ADAPTIVE, TITUS_PARALLEL_REJECTION})
+        CK(cudaFuncSetAttribute(kernel_for<kThreeD>(method), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(WSmem)));
-        CK(cudaFuncSetAttribute(adaptive_kernel<TITUS_PARALLEL_REJECTION>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WSmem)));
-    }
     return TITUS_OK;
 }
 
@@ -114,11 +124,7 @@ int launch(titus_solver* s, int method, const titus_options_t* opt, int n_begin,
     int G = (opt && opt->team_ctas > 0) ? opt->team_ctas : std::min(s->num_sms, 64);
     G = std::max(1, std::min(G, s->num_sms));
     int per_sm = 0;
-    void (*kfun)(DevProblem, WideState*, int, int, int, int) = adaptive_kernel<TITUS_BUG_ADAPTIVE>;
-    if constexpr (!kThreeD) {
-        if (method == TITUS_PARALLEL_ADAPTIVE) kfun = adaptive_kernel<TITUS_PARALLEL_ADAPTIVE>;
-        if (method == TITUS_PARALLEL_REJECTION) kfun = adaptive_kernel<TITUS_PARALLEL_REJECTION>;
-    }
+    const KernelFn kfun = kernel_for<kThreeD>(method);
     auto kern = (void*)kfun;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, TITUS_WIDE_NS::NT, sizeof(WSmem)));
     if (per_sm < 1) return fail(TITUS_ERR_CUDA, "adaptive kernel does not fit on an SM (smem %zu)", sizeof(WSmem));
