@@ -5,5 +5,5 @@ from .solver import (DoseAdjoint, PencilBeamBatch, SolveBatchedPencilBeams, Solv
                      SolveFirstCollisionSourceDLR, SolveFirstCollisionSourceDLRHighOrder,
                      SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel,
                      SolveFirstCollisionSourceDLRParallelRejection, scalar_flux)
-from .spots import partition, plan_dose, plan_objective  # noqa: F401
+from .spots import partition, plan_adjoint, plan_dose, plan_objective  # noqa: F401
 from .output import write_dlm, write_dose_vtk, write_vtr  # noqa: F401

@@ -11,8 +11,11 @@ spot). Per-spot doses never leave their rank.
 For the plan objective J(w) = sum_c mask_c (sum_s w_s D_s[c] - P[c])^2 the
 spot-weight gradient dJ/dw_s = 2 sum_c mask_c (D[c] - P[c]) D_s[c] needs only
 the reduced total dose and the rank's own spot doses, so it is computed where
-the spots were solved. The gradient with respect to the density (an adjoint
-transport solve) is not provided.
+the spots were solved. ``plan_adjoint`` adds the gradient with respect to the
+voxel densities through the discrete adjoint of the full-rank sweep
+(``DoseAdjoint``): spots of one energy share one solve whose inflow profile is
+their weighted sum (the sweep is linear in the inflow), the energy groups are
+sharded over the ranks, and dJ/drho and dJ/dw are summed by all-reduce.
 """
 from __future__ import annotations
 
@@ -104,3 +107,82 @@ def plan_objective(solver, spots, weights, prescription, mask=None, method: str 
     if idx.size:
         g[idx] = 2.0 * (local @ res)
     return J, _allreduce_sum(g, device), D
+
+
+def _full_rank_forward(solver, profile):
+    from .solver import SolveFirstCollisionSource
+
+    solver.set_beam_profile(profile)
+    return SolveFirstCollisionSource(solver)[1]
+
+
+def _full_rank_adjoint(solver, profile, dj_ddose, checkpoint_every):
+    from .solver import DoseAdjoint
+
+    solver.set_beam_profile(profile)
+    _, dose, grho, gprof = DoseAdjoint(solver, dj_ddose=dj_ddose, checkpoint_every=checkpoint_every)
+    return dose, grho, gprof
+
+
+def plan_adjoint(make_solver, spots, weights, prescription, mask=None, checkpoint_every: int = 0, device=None,
+                 forward=None, adjoint=None):
+    """J(w, rho) = sum_c mask_c (D[c] - P[c])^2 of a plan solved with the
+    full-rank sweep, and its gradients with respect to the spot weights and the
+    voxel densities (the adjoint-optimisation objective of a treatment plan).
+
+    ``spots`` = [(energy, y0), ...]; ``make_solver(energy)`` returns a solver
+    (``SolverCSD``) of the phantom for beams of that energy; ``beam_profile(y0=...)``
+    of that solver gives a spot's inflow profile. Spots of equal energy share
+    one solve with inflow sum_s w_s p_s. Groups are sharded round robin over
+    the default process group: each rank solves its groups forward, the total
+    dose D is summed by all-reduce, each rank then runs the adjoint of its groups
+    with dJ/dD = 2 mask (D - P) (``titus_dose_adjoint`` checkpointing every
+    ``checkpoint_every`` steps), and dJ/drho and dJ/dw = p_s . dJ/dprofile are
+    summed by all-reduce. ``forward(solver, profile) -> dose`` and
+    ``adjoint(solver, profile, dj_ddose, checkpoint_every) -> (dose, dJ/drho,
+    dJ/dprofile)`` replace the GPU calls (tests). Returns (J, dJ/dw (nspots),
+    dJ/drho (n), D).
+    """
+    forward = forward or _full_rank_forward
+    adjoint = adjoint or _full_rank_adjoint
+    spots = list(spots)
+    ns = len(spots)
+    w = np.asarray(weights, dtype=np.float64)
+    if w.shape != (ns,):
+        raise ValueError(f"{w.shape[0] if w.ndim else 0} weights for {ns} spots")
+    energies = sorted({float(e) for e, _ in spots})
+    world, rank = _world()
+    mine = partition(len(energies), world, rank)
+    groups = []
+    for gi in mine:
+        e = energies[gi]
+        members = [i for i, (ei, _) in enumerate(spots) if float(ei) == e]
+        sv = make_solver(e)
+        profs = [np.asarray(sv.beam_profile(y0=spots[i][1]), dtype=np.float64) for i in members]
+        profile = sum(w[i] * p for i, p in zip(members, profs))
+        groups.append((sv, members, profs, profile))
+    n = None
+    part = None
+    for sv, _, _, profile in groups:
+        d = np.asarray(forward(sv, profile), dtype=np.float64)
+        part = d if part is None else part + d
+        n = d.size
+    P = np.asarray(prescription, dtype=np.float64)
+    if n is None:
+        n = P.size
+        part = np.zeros(n)
+    D = _allreduce_sum(part, device)
+    m = np.ones_like(D) if mask is None else np.asarray(mask, dtype=np.float64)
+    if P.shape != D.shape or m.shape != D.shape:
+        raise ValueError("prescription and mask must have one entry per cell")
+    res = m * (D - P)
+    J = float(res @ (D - P))
+    djdd = 2.0 * res
+    grho = np.zeros(n)
+    gw = np.zeros(ns)
+    for sv, members, profs, profile in groups:
+        _, gr, gp = adjoint(sv, profile, djdd, checkpoint_every)
+        grho += np.asarray(gr, dtype=np.float64)
+        for i, p in zip(members, profs):
+            gw[i] = float(p @ np.asarray(gp, dtype=np.float64))
+    return J, _allreduce_sum(gw, device), _allreduce_sum(grho, device), D
