@@ -251,8 +251,8 @@ int titus_profile(titus_solver_t* solver, double* ns, int32_t n);
  * TITUS_ERR_LIMIT. All calls on a device share that array, so calls that
  * overlap on the GPU race: issue them one at a time per device. Each call
  * clears what must start at zero and looks the array's address up for the
- * current device. The call is synchronous (it reads e_trafo[0..1] and the status
- * words back and waits for `stream`), so it cannot run inside a stream capture.
+ * current device. The call is synchronous: it reads e_trafo[0..1] and the status
+ * words back and waits for `stream`.
  * Error text (if any) is written to err[0..err_len). */
 int titus_solve_noalloc(const titus_problem_t* problem, const titus_options_t* options, double* dose,
                         double* X, double* S, double* W, double* psi, int32_t* rank_out, void* stream,

@@ -21,8 +21,7 @@
 //    current (cudaGetSymbolAddress; nothing is cached, so concurrent first calls
 //    from several host threads and a cudaDeviceReset between calls are safe);
 //  * the call is synchronous: it reads e_trafo[0..1] back to the host before the
-//    launch and the status words after it, then waits for `stream`, so it cannot
-//    be recorded into a CUDA graph by stream capture;
+//    launch and the status words after it, then waits for `stream`;
 //  * a problem fits when 913 n + 580 N + 4 nE + 73 728 G + 48 KiB <= 16 MiB
 //    bytes (n cells, N moments, nE energies, G CTAs; 256-byte alignment of each
 //    piece included in the constant): about 16 700 cells at P21 with G = 16.
