@@ -51,3 +51,35 @@ def test_dlm_round_trip(tmp_path):
     p2 = write_dlm(str(tmp_path / "v"), v)
     assert np.array_equal(np.loadtxt(p2, delimiter="\t"), v)
     assert open(p).readline().count("\t") == 3
+
+
+def test_vtr_3d_round_trip(tmp_path):
+    from titus_b200.output import write_dose_vtk_3d
+    from titus_b200.settings import Settings3D
+
+    s = Settings3D(Nx=6, Ny=5, Nz=4, nPN=1, L=1.0)
+    n = s.NCellsX * s.NCellsY * s.NCellsZ
+    rng = np.random.default_rng(3)
+    dose = np.abs(rng.standard_normal(n))
+    u = rng.standard_normal(n)
+    p = write_dose_vtk_3d(s, dose, u, 2.0, outdir=str(tmp_path))
+    assert p.endswith(f"dose_csd_nx{s.NCellsX}ny{s.NCellsY}nz{s.NCellsZ}.vtr")
+    x, y, z, d = read_vtr(p, with_z=True)
+    assert np.array_equal(x, s.xMid) and np.array_equal(y, s.yMid) and np.array_equal(z, s.zMid)
+    assert f'WholeExtent="0 {s.NCellsX - 1} 0 {s.NCellsY - 1} 0 {s.NCellsZ - 1}"' in open(p).read(300)
+    # VTK order: x fastest; the solver's row of cell (i, j, k) is (k nx + i) ny + j
+    i, j, k = 3, 2, 1
+    vtk = i + s.NCellsX * (j + s.NCellsY * k)
+    row = (k * s.NCellsX + i) * s.NCellsY + j
+    assert d["dose"][vtk] == dose[row]
+    assert np.array_equal(np.sort(d["dose"]), np.sort(dose))
+    assert d["u"][vtk] == u[row] / 0.5 / math.sqrt(2.0)
+
+
+def test_vtr_2d_file_unchanged_by_3d_support(tmp_path):
+    x = np.linspace(0.0, 1.0, 3)
+    y = np.linspace(0.0, 2.0, 2)
+    p = write_vtr(str(tmp_path / "p"), x, y, {"a": np.arange(6.0)})
+    txt = open(p).read()
+    assert '<DataArray type="Float64" Name="z" format="ascii">0.0</DataArray>' in txt
+    assert 'WholeExtent="0 2 0 1 0 0"' in txt

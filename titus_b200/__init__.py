@@ -6,4 +6,4 @@ from .solver import (DoseAdjoint, PencilBeamBatch, SolveBatchedPencilBeams, Solv
                      SolveFirstCollisionSourceDLRBUGRejection, SolveFirstCollisionSourceDLRParallel,
                      SolveFirstCollisionSourceDLRParallelRejection, scalar_flux)
 from .spots import partition, plan_adjoint, plan_dose, plan_objective  # noqa: F401
-from .output import write_dlm, write_dose_vtk, write_vtr  # noqa: F401
+from .output import write_dlm, write_dose_vtk, write_dose_vtk_3d, write_vtr  # noqa: F401

@@ -8,6 +8,9 @@
   fastest, and so does any VTK reader of this file.
 * Delimited text (``code/SolverCSD.jl:878``, ``writedlm(file, W*V)``): one matrix
   row per line, tab-separated.
+* 3D problems (no counterpart in the reference): the same rectilinear grid with
+  z coordinates, the point arrays in VTK's own order (x fastest, then y, then
+  z), converted from the solver's row order (k nx + i) ny + j.
 
 Data are written inline as ASCII with 17 significant digits, which every VTK
 reader accepts and which round-trips FP64 exactly.
@@ -24,15 +27,18 @@ def _ascii(a) -> str:
     return " ".join(repr(float(v)) for v in np.asarray(a, dtype=np.float64).ravel())
 
 
-def write_vtr(path: str, x, y, point_data: dict) -> str:
-    """Rectilinear grid with coordinates x (nx), y (ny), z = [0] and point
-    arrays of nx*ny values each. Returns the file name (``.vtr`` appended)."""
+def write_vtr(path: str, x, y, point_data: dict, z=None) -> str:
+    """Rectilinear grid with coordinates x (nx), y (ny), z (nz; None = the
+    plane z = [0]) and point arrays of nx*ny*nz values each, passed in the
+    order the file stores them. Returns the file name (``.vtr`` appended)."""
     x = np.asarray(x, dtype=np.float64).ravel()
     y = np.asarray(y, dtype=np.float64).ravel()
-    npts = x.size * y.size
+    zc = None if z is None else np.asarray(z, dtype=np.float64).ravel()
+    nz = 1 if zc is None else zc.size
+    npts = x.size * y.size * nz
     if not path.endswith(".vtr"):
         path = path + ".vtr"
-    ext = f"0 {x.size - 1} 0 {y.size - 1} 0 0"
+    ext = f"0 {x.size - 1} 0 {y.size - 1} 0 {nz - 1}"
     lines = ['<?xml version="1.0"?>',
              '<VTKFile type="RectilinearGrid" version="1.0" byte_order="LittleEndian" header_type="UInt64">',
              f'  <RectilinearGrid WholeExtent="{ext}">', f'    <Piece Extent="{ext}">', "      <PointData>"]
@@ -44,7 +50,8 @@ def write_vtr(path: str, x, y, point_data: dict) -> str:
     lines += ["      </PointData>", "      <CellData>", "      </CellData>", "      <Coordinates>",
               f'        <DataArray type="Float64" Name="x" format="ascii">{_ascii(x)}</DataArray>',
               f'        <DataArray type="Float64" Name="y" format="ascii">{_ascii(y)}</DataArray>',
-              '        <DataArray type="Float64" Name="z" format="ascii">0.0</DataArray>',
+              ('        <DataArray type="Float64" Name="z" format="ascii">0.0</DataArray>' if zc is None else
+               f'        <DataArray type="Float64" Name="z" format="ascii">{_ascii(zc)}</DataArray>'),
               "      </Coordinates>", "    </Piece>", "  </RectilinearGrid>", "</VTKFile>"]
     d = os.path.dirname(path)
     if d:
@@ -67,6 +74,26 @@ def write_dose_vtk(settings, dose, u, gamma0: float, name: str | None = None, ou
     })
 
 
+def write_dose_vtk_3d(settings, dose, u, gamma0: float, name: str | None = None, outdir: str = "output") -> str:
+    """Dose of a 3D problem (``Settings3D``): ``output/dose_csd_nx{NX}ny{NY}nz{NZ}.vtr``
+    with dose, dose_normalized and u / 0.5 / sqrt(gamma[1]) on the cell
+    centres, in VTK's x-fastest order."""
+    s = settings
+    shape = (s.NCellsZ, s.NCellsX, s.NCellsY)
+
+    def vtk_order(a):
+        return np.asarray(a, dtype=np.float64).reshape(shape).transpose(0, 2, 1).ravel()
+
+    dose = np.asarray(dose, dtype=np.float64)
+    if name is None:
+        name = f"dose_csd_nx{s.NCellsX}ny{s.NCellsY}nz{s.NCellsZ}"
+    return write_vtr(os.path.join(outdir, name), s.xMid, s.yMid, {
+        "dose": vtk_order(dose),
+        "dose_normalized": vtk_order(dose / dose.max()),
+        "u": vtk_order(np.asarray(u, dtype=np.float64) / 0.5 / math.sqrt(gamma0)),
+    }, z=s.zMid)
+
+
 def write_dlm(path: str, a) -> str:
     """``writedlm(path, a)``: rows of a 2-D array (a vector is one column),
     tab-separated, shortest round-trip float text."""
@@ -82,12 +109,15 @@ def write_dlm(path: str, a) -> str:
     return path
 
 
-def read_vtr(path: str):
-    """(x, y, {name: array}) of a file written by ``write_vtr``."""
+def read_vtr(path: str, with_z: bool = False):
+    """(x, y, {name: array}) of a file written by ``write_vtr``; with
+    ``with_z``, (x, y, z, {name: array})."""
     import xml.etree.ElementTree as ET
 
     root = ET.parse(path).getroot()
     piece = root.find("RectilinearGrid/Piece")
     coords = [np.array(e.text.split(), dtype=np.float64) for e in piece.find("Coordinates")]
     data = {e.get("Name"): np.array(e.text.split(), dtype=np.float64) for e in piece.find("PointData")}
+    if with_z:
+        return coords[0], coords[1], coords[2], data
     return coords[0], coords[1], data
