@@ -205,17 +205,38 @@ class _IterClock:
 
 def _cost_of_history(by_rank, ranks):
     """Sum over the history of the mean measured time at each rank; ranks not
-    measured take the linear interpolation between the nearest measured ranks
-    (the nearest one outside their range). Returns (seconds, share of the
-    history's iterations at a directly measured rank)."""
+    measured take the linear interpolation between the nearest ranks measured
+    at least twice (the nearest one outside their range). A rank met once --
+    the first iteration, which also pays the loop's set-up -- is used where it
+    occurs, never as an interpolation node: it would inflate every rank between
+    it and the steady rank. Returns (seconds, share of the history's iterations
+    at a directly measured rank)."""
     import numpy as np
 
-    rs = np.array(sorted(by_rank))
+    nodes = [r for r in sorted(by_rank) if len(by_rank[r]) >= 2] or sorted(by_rank)
+    rs = np.array(nodes)
     cs = np.array([float(np.mean(by_rank[r])) for r in rs])
     vals, cnt = np.unique(np.asarray(ranks, dtype=np.int64), return_counts=True)
-    total = float(np.sum(np.interp(vals, rs, cs) * cnt))
+    per = np.interp(vals, rs, cs)
+    for k, v in enumerate(vals):
+        if int(v) in by_rank:
+            per[k] = float(np.mean(by_rank[int(v)]))
+    total = float(np.sum(per * cnt))
     direct = float(np.sum(cnt[np.isin(vals, rs)]) / max(1, np.sum(cnt)))
     return total, direct
+
+
+def _warm_oracle(w, mk):
+    """A few untimed oracle iterations of the same problem, so that the timed
+    windows do not pay first-call costs (thread pools, caches, lazy imports)."""
+    if w["method"] in ("pn3d", "bug3d"):
+        return
+    from oracle.full_rank import solve_pn_full
+    from oracle.solver import solve_dlr_bug, solve_dlr_fixed, solve_dlr_parallel
+
+    fn = {"pn_full": solve_pn_full, "bug": solve_dlr_bug, "parallel": solve_dlr_parallel,
+          "fixed": solve_dlr_fixed}[w["method"]]
+    fn(mk(), max_steps=3)
 
 
 def cpu_cost_model(w, ranks, state200=None, head=40, tail=20):
@@ -235,6 +256,7 @@ def cpu_cost_model(w, ranks, state200=None, head=40, tail=20):
     from oracle.solver import solve_dlr_bug, solve_dlr_fixed, solve_dlr_parallel
 
     mk = _oracle_setup(w)
+    _warm_oracle(w, mk)
     if w["method"] == "pn_full":
         from oracle.full_rank import solve_pn_full
 
