@@ -222,7 +222,7 @@ def _cost_of_history(by_rank, ranks):
         if int(v) in by_rank:
             per[k] = float(np.mean(by_rank[int(v)]))
     total = float(np.sum(per * cnt))
-    direct = float(np.sum(cnt[np.isin(vals, rs)]) / max(1, np.sum(cnt)))
+    direct = float(np.sum(cnt[np.isin(vals, np.array(sorted(by_rank)))]) / max(1, np.sum(cnt)))
     return total, direct
 
 
